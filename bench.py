@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""QEM force evaluations per second at N = 1e5 on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one force evaluation of the whole system): the N = 1e5
+slab of the benchmark configuration -- +-1 charges, Lx = Ly = 1000, Lz = 10,
+gamma_up = gamma_down = 0.95, alpha = 0.1, r_c = 10, 30-node Gauss-Legendre
+quadrature, P = 500 random-batch k-vectors (seeded), Julia-reference
+semantics -- evaluated by the FP32+FP64-fix path (short + self + long range).
+The plain FP64 GPU path is timed in the same run and reported beside it, with
+the FP32 path's force error against it.
+
+Multi-GPU (torchrun): one independent system per rank (seeded per rank), no
+data-path collective; value = total evaluations/s over all ranks ("weak").
+
+--impl reference times the FP64 CPU restatement of the reference algorithm
+(oracle/, OpenMP on all host cores) on a bounded sample of the same workload
+and extrapolates to evaluations/s of the full system.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QEM force evals/s at N=1e5: FP32+FP64-fix vs FP64 GPU at ≤1e-5 force err"
+UNIT = "evals/s"
+FLOPS_PER_PAIR_NODE = 100   # op model per short-range quadrature node (FP32 flops)
+SFU_PER_PAIR_NODE = 6       # MUFU ops per node in the same model
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=100_000)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampler (200 ms) running across the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------- ranks
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(v: float, world: int, device):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_sample(cfg, pairs, seconds_target=15.0, n_pairs=None, n_self=None, P_s=None):
+    """FP64 oracle (OpenMP, all host cores) on a bounded sample of one evaluation; returns
+    (evals/s extrapolated to the full system, cores, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+
+    p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"],
+                 accuracy=cfg["accuracy"], N_t=cfg["N_t"])
+    cores = O.max_threads()
+    xyz, q, N = cfg["xyz"], cfg["q"], cfg["N"]
+    Np = len(pairs)
+    # size the sample from a short calibration so the whole sample takes ~seconds_target
+    t0 = time.perf_counter()
+    O.pairs_eval(p, xyz, q, pairs[:2000])
+    t_pair = (time.perf_counter() - t0) / 2000
+    if n_pairs is None:
+        n_pairs = int(min(Np, max(2000, 0.6 * seconds_target / max(t_pair, 1e-9))))
+    if n_self is None:
+        n_self = min(N, max(1000, n_pairs // 10))
+    if P_s is None:
+        P_s = 4
+    t0 = time.perf_counter()
+    O.pairs_eval(p, xyz, q, pairs[:n_pairs])
+    t_pairs = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.self_eval(p, xyz, q, n_self)
+    t_self = time.perf_counter() - t0
+    rng = np.random.default_rng(1)
+    k3 = np.zeros((P_s, 3))
+    for i in range(P_s):
+        mx, my = rng.integers(-40, 41, 2)
+        mx = mx if (mx or my) else 1
+        k3[i] = [2 * np.pi * mx / cfg["L"][0], 2 * np.pi * my / cfg["L"][1], 0]
+        k3[i, 2] = np.hypot(k3[i, 0], k3[i, 1])
+    t0 = time.perf_counter()
+    O.F_long(p, xyz, q, k3, 1.0)
+    t_long = time.perf_counter() - t0
+    t_full = t_pairs * (Np / n_pairs) + t_self * (N / n_self) + t_long * (cfg["P"] / P_s)
+    desc = (f"oracle FP64 on {cores} threads: {n_pairs} of {Np} pairs, {n_self} of {N} self terms, "
+            f"{P_s} of {cfg['P']} k-vectors over all N; extrapolated to one full evaluation "
+            f"({t_pairs + t_self + t_long:.1f} s measured, {t_full:.1f} s per evaluation)")
+    return 1.0 / t_full, cores, desc
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from qem4molly_b200 import _lib as L
+    from qem4molly_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    lib = L.load()
+    fp32_peak, mufu_peak = C.c_double(0), C.c_double(0)
+    lib.qem_measure_peaks(local, C.byref(fp32_peak), C.byref(mufu_peak))
+
+    cfg = W.config2(N=args.N, seed=None if rank == 0 else W.SEED0 + 2 + 1000 * rank)
+    e32 = W.engine_for(cfg, "fp32", device=local)
+    e64 = W.engine_for(cfg, "fp64", device=local)  # same seeded k-set
+    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
+    q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
+    F = torch.empty_like(x)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    terms = L.QEM_TERM_ALL
+
+    def timed(e, K):
+        per, kt = [], {}
+        for _ in range(K):
+            flush.zero_()  # evict the 126 MB L2 between steps (outside the event window)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e.forces_device(x, q, F, terms=terms)
+            b.record(stream)
+            b.synchronize()
+            per.append(a.elapsed_time(b))
+            for k, v in e.timings().items():
+                kt.setdefault(k, []).append(v)
+        return per, {k: float(np.mean(v)) for k, v in kt.items()}
+
+    for _ in range(max(args.warmup, 3)):
+        e32.forces_device(x, q, F, terms=terms)
+        e64.forces_device(x, q, F, terms=terms)
+    e32.set_profiling(True)
+    e64.set_profiling(True)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = Clocks(local)
+    torch.cuda.synchronize()
+    barrier(world)
+    per32, kt32 = timed(e32, args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms32 = max_over_ranks(float(np.sum(per32)) / args.steps, world, dev)
+    K64 = max(3, args.steps // 4)
+    per64, kt64 = timed(e64, K64)
+    ms64 = max_over_ranks(float(np.sum(per64)) / K64, world, dev)
+    counts = e32.counts()
+
+    # accuracy of the FP32+fix path against the plain FP64 path (parity-tested against the oracle)
+    e32.forces_device(x, q, F, terms=terms)
+    F32 = F.cpu().numpy().copy()
+    e64.forces_device(x, q, F, terms=terms)
+    F64 = F.cpu().numpy().copy()
+    err, err_max = W.rel_err(F32, F64)
+
+    # end to end through the public API with pinned host buffers (H2D + D2H inside the timed region)
+    xh = torch.tensor(cfg["xyz"], dtype=torch.float64).pin_memory()
+    qh = torch.tensor(cfg["q"], dtype=torch.float64).pin_memory()
+    Fh = torch.empty_like(xh).pin_memory()
+    for _ in range(2):
+        e32.forces(xh.numpy(), qh.numpy(), terms=terms, out=Fh.numpy())
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e32.forces(xh.numpy(), qh.numpy(), terms=terms, out=Fh.numpy())
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e = {"value": world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(xh.numel() * 8 + qh.numel() * 8),
+           "d2h_bytes_per_step": int(Fh.numel() * 8)}
+
+    # roofline of the dominant kernel (short-range pair quadrature, FP32)
+    Np = counts["pairs"]
+    nodes = Np * 8 * cfg["N_t"]
+    t_pair = kt32.get("short_pair", float("nan")) * 1e-3
+    achieved = nodes * FLOPS_PER_PAIR_NODE / t_pair / 1e12
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get("short_pair_fp32_bytes_per_launch")
+    roofline = {"bound": "fp32", "kernel": "k_short_pair<FP32>", "achieved": achieved, "peak": fp32_peak.value,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak.value if fp32_peak.value else None,
+                "traffic": traffic,
+                "peak_source": "measured in this run (qem_measure_peaks FMA chain); MEASURED_PEAKS.json has no FP32 figure",
+                "work_model": f"{FLOPS_PER_PAIR_NODE} FP32 flops + {SFU_PER_PAIR_NODE} MUFU ops per pair-node; "
+                              f"{Np} pairs x 8 x {cfg['N_t']} nodes per launch",
+                "mufu": {"achieved": nodes * SFU_PER_PAIR_NODE / t_pair / 1e12, "peak": mufu_peak.value,
+                         "unit": "Tops/s"}}
+
+    out = {"metric": METRIC, "value": world * 1000.0 / ms32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64fix", "data": "synthetic (seeded, per-rank system)",
+           "config": {"workload": f"QEM slab N={cfg['N']} Lx=Ly={cfg['L'][0]:g} Lz=10 gamma=0.95/0.95 alpha=0.1 "
+                                  f"r_c=10 N_t=30 P={cfg['P']} (short+self+long), Julia-reference semantics",
+                      "N": cfg["N"], "pairs": Np, "P": cfg["P"], "precision": "FP32+FP64-fix",
+                      "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
+                      "parallelism": f"{world} independent systems (one per GPU)"},
+           "e2e": e2e, "gpu_launches": int(counts["launches"]) * args.steps, "roofline": roofline,
+           "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64, "steps": K64},
+           "speedup_vs_fp64": ms64 / ms32, "force_rel_err_vs_fp64": err, "force_max_err_vs_fp64_rms": err_max,
+           "kernel_ms": {"fp32": kt32, "fp64": kt64}, "clocks": clk}
+    if rank == 0 and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
+        pairs = O.pairs(p, cfg["xyz"], method="cells")
+        v, cores, desc = cpu_sample(cfg, pairs)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    e32.close()
+    e64.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from qem4molly_b200 import workloads as W
+
+    cfg = W.config2(N=args.N)
+    p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
+    pairs = O.pairs(p, cfg["xyz"], method="cells")
+    per_step = max(2.0, min(10.0, 150.0 / (args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(cfg, pairs, seconds_target=per_step / 4)
+    vals, desc, cores = [], "", 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, cores, desc = cpu_sample(cfg, pairs, seconds_target=per_step)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = len(vals) / sum(1.0 / v for v in vals)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": f"QEM slab N={cfg['N']} (same system as the GPU arm), FP64 CPU restatement of "
+                                  "the reference algorithm, bounded samples extrapolated per evaluation"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "sample_wall_s": wall}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * qem.h -- C-ABI of the B200-native QEM (Quasi-Ewald Method) force/energy
+ * library, libqem.so.  Plain C types only: pointers, sizes, a POD parameter
+ * struct and an opaque handle.  Julia binds it with ccall, Python with ctypes;
+ * the torch.autograd.Function in qem4molly_b200 is a thin layer over it.
+ *
+ * Reference interfaces replaced (paths inside ArrogantGao/QEM4Molly):
+ *   QEM_short(L, r_cutoff, alpha; iter_period, gamma_1, gamma_2, eps_0,
+ *             accuracy, N_t)                        src/QEM_short.jl:19-25
+ *   QEM_long(L; k_cutoff, z_list, gamma_1, gamma_2, eps_0, accuracy, alpha,
+ *            rbe_mode, rbe_p)                       src/QEM_long.jl:19-30
+ *   QEM_inter(n_atoms, L; s, accuracy, rbe_mode, rbe_p, eps_0, gamma_1,
+ *             gamma_2, N_t, iter_period)            src/Quasi_Ewald_Method.jl:3-24
+ *   Substrate_LJ(; cutoff, sigma, eps, sub_pos, direction)
+ *                                                   src/Substrate_LJ.jl:15-17
+ *   Molly.forces(inter::QEM_short, sys, nb)         src/QEM_short.jl:27-59
+ *   Molly.forces(inter::QEM_long, sys, nb)          src/QEM_long.jl:32-44
+ *   Molly.forces(inter::Substrate_LJ, sys, nb)      src/Substrate_LJ.jl:24-46
+ *   K_set_generator(L_x, L_y, alpha, accuracy) + StatsBase.sample
+ *                                                   src/K_set_generator.jl:5-45,
+ *                                                   src/Force_long.jl:235
+ *   Energy_short / Energy_long (python_lib; the Julia package has no energy)
+ *                                                   src/python_lib/Energy_short_range_njit.py:84-99,
+ *                                                   src/python_lib/Energy_long_range_njit.py:10-44
+ *
+ * Conventions
+ *   - Coordinates are 3N doubles, particle-major (x0 y0 z0 x1 ...), which is
+ *     exactly reinterpret(Float64, sys.coords) for Molly's SVector{3,Float64}.
+ *   - Charges are N doubles; forces are written as 3N doubles (overwritten).
+ *   - gamma_down is the reference's gamma_1 (image across z = 0),
+ *     gamma_up is gamma_2 (image across z = L_z).
+ *   - mem == QEM_MEM_HOST: pointers are host memory; the call copies, computes
+ *     and synchronises before returning.  mem == QEM_MEM_DEVICE: pointers are
+ *     device memory on the handle's device; work is ordered on `stream`
+ *     (a cudaStream_t, NULL = legacy default stream) and the call also
+ *     synchronises that stream before returning, so the status is final.
+ *   - A handle is not thread-safe; use one handle per host thread / stream.
+ *   - The caller owns every buffer it passes.  The handle owns its device
+ *     scratch (cell arrays, pair list, k-set, partial sums) and grows it on
+ *     demand.
+ *   - Every entry point returns a qem_status; details of the last failure are
+ *     in qem_last_error().  No entry point traps, asserts or aborts.
+ */
+#ifndef QEM_H
+#define QEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t qem_status;
+#define QEM_OK 0
+#define QEM_ERR_ARG 1          /* invalid parameter or size                         */
+#define QEM_ERR_OUT_OF_SLAB 2  /* Substrate_LJ.jl:37 @assert direction*dz > 0       */
+#define QEM_ERR_NONFINITE 3    /* NaN/Inf in coordinates or charges                 */
+#define QEM_ERR_NB_OVERFLOW 4  /* neighbour data exceeded a fixed capacity          */
+#define QEM_ERR_TIMEOUT 5      /* a bounded device-side wait ran out                */
+#define QEM_ERR_CUDA 6         /* CUDA runtime error (message in qem_last_error)    */
+#define QEM_ERR_NO_KSET 7      /* long range requested before a k-set exists        */
+#define QEM_ERR_RANGE 8        /* exponent range of the FP32 k-space path exceeded  */
+
+/* mode_flags: one bit per parity quirk of the reference (0 = reference Julia) */
+#define QEM_CUTOFF_PYTHON 0x1u   /* python_lib quadrature limits (Force_short_range_njit.py:51-52)
+                                    instead of Julia's per-image limits (Force_short.jl:48-67)     */
+#define QEM_DIR_MINIMAGE 0x2u    /* minimum-image x/y direction instead of the raw coordinate
+                                    difference of Force_short.jl:57-58                            */
+#define QEM_PAIR_PHYSICAL 0x4u   /* F[j] += F_short_ij(j, i) instead of F[j] -= F_ij
+                                    (QEM_short.jl:46-47)                                          */
+#define QEM_STALE_NEIGHBORS 0x8u /* rebuild the pair list only on calls 1, 1+iter_period, ...
+                                    (QEM_short.jl:32-36); default rebuilds every call             */
+#define QEM_RESAMPLE_KSET 0x10u  /* draw a fresh random batch of k-vectors on every long-range
+                                    call (Force_long.jl:235); default reuses the current batch    */
+#define QEM_PYTHON_MODE (QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL)
+
+/* precision */
+#define QEM_FP64 0      /* plain FP64 everywhere                                           */
+#define QEM_FP32_FIX 1  /* FP32 quadrature and structure sums (compensated), FP64 k-space
+                           denominators and phases, cancellation-free short-range
+                           denominators, FP64 final force/energy reductions              */
+
+/* terms (bit mask) */
+#define QEM_TERM_SHORT 0x1u
+#define QEM_TERM_LONG 0x2u
+#define QEM_TERM_LJ 0x4u
+#define QEM_TERM_ALL 0x7u
+
+/* memory kind of the pointers passed to a call */
+#define QEM_MEM_HOST 0
+#define QEM_MEM_DEVICE 1
+
+/* Substrate_LJ(; cutoff, sigma, eps, sub_pos, direction)  Substrate_LJ.jl:7-17 */
+typedef struct {
+    double cutoff;
+    double sigma;
+    double eps;
+    double sub_pos;
+    double direction; /* +1 or -1 */
+} qem_lj_wall;
+
+typedef struct {
+    double Lx, Ly, Lz;  /* QEM_short.L / QEM_long.L                                    */
+    double alpha;       /* Ewald splitting parameter                                    */
+    double r_cutoff;    /* short-range cutoff (must be < min(Lx, Ly) / 2)               */
+    double gamma_down;  /* reference gamma_1                                            */
+    double gamma_up;    /* reference gamma_2                                            */
+    double eps_0;       /* default 1                                                    */
+    double accuracy;    /* default 1e-6                                                 */
+    int32_t N_t;        /* Gauss-Legendre order, 1..64 (default 30)                     */
+    int32_t rbe_p;      /* random-batch size P (default 30)                             */
+    int32_t iter_period;/* neighbour refresh period for QEM_STALE_NEIGHBORS (default 100) */
+    int32_t n_walls;    /* 0..2 Substrate_LJ walls fused into the short-range pass      */
+    qem_lj_wall walls[2];
+    uint32_t mode_flags;/* QEM_CUTOFF_PYTHON | ...                                      */
+    int32_t precision;  /* QEM_FP64 or QEM_FP32_FIX                                     */
+    int32_t device;     /* CUDA device ordinal                                          */
+    int32_t reserved[5];/* must be zero                                                 */
+} qem_params;
+
+typedef struct qem_handle qem_handle;
+
+/* Fills p with the reference defaults (QEM_short.jl:19, QEM_long.jl:19):
+ * gamma 0, eps_0 1, accuracy 1e-6, N_t 30, rbe_p 30, iter_period 100, no walls. */
+void qem_default_params(qem_params *p);
+
+/* QEM_inter factory (Quasi_Ewald_Method.jl:3-24): alpha = n_atoms / (Lx Ly)
+ * (rbe_mode != 0) or sqrt(n_atoms) / (Lx Ly), r_cutoff = s / sqrt(alpha).
+ * Writes alpha, r_cutoff and rbe_p into p. */
+qem_status qem_inter_params(qem_params *p, int64_t n_atoms, double s, int32_t rbe_mode, int32_t rbe_p);
+
+/* Creates a handle (QEM_short + QEM_long + Substrate_LJ state on one device). */
+qem_status qem_create(const qem_params *p, qem_handle **out);
+void qem_destroy(qem_handle *h);
+const char *qem_last_error(const qem_handle *h);
+const char *qem_status_string(qem_status s);
+
+/* Random-batch k-set.  qem_set_kset feeds P rows of (kx, ky, k) and the
+ * normaliser sum_K (K_set_generator.jl:28) -- the way parity runs feed the
+ * same batch to the library and to the oracle.  qem_sample_kset draws P
+ * vectors from exp(-k^2 / 4 alpha) on the 2 pi (m / Lx, n / Ly) lattice
+ * (k != 0, |m| <= ceil(k_c Lx / 2 pi) + 1, K_set_generator.jl:7-9) with the
+ * library's own seeded separable sampler. */
+qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K);
+qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P);
+qem_status qem_get_kset(const qem_handle *h, double *k3_out, int32_t cap, int32_t *P, double *sum_K);
+
+/* Fused evaluation: short range (+ self terms) + long range + walls.
+ * F: 3N doubles (overwritten).  energy: NULL or one double receiving the QEM
+ * short + long energy (Substrate_LJ has no energy in the reference). */
+qem_status qem_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, double *energy,
+                      uint32_t terms, int32_t mem, void *stream);
+
+/* Molly.forces(inter::QEM_short, sys)   QEM_short.jl:27-59 (plus walls if configured) */
+qem_status qem_short_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, int32_t mem,
+                            void *stream);
+/* Molly.forces(inter::QEM_long, sys)    QEM_long.jl:32-44, Force_long.jl:201-242 */
+qem_status qem_long_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, int32_t mem,
+                           void *stream);
+/* Molly.forces(inter::Substrate_LJ, sys) Substrate_LJ.jl:24-46 for the handle's walls */
+qem_status qem_lj_forces(qem_handle *h, int32_t N, const double *xyz, double *F, int32_t mem, void *stream);
+/* Molly.potential_energy for the QEM terms (python_lib energies; see above) */
+qem_status qem_potential_energy(qem_handle *h, int32_t N, const double *xyz, const double *q, double *energy,
+                                uint32_t terms, int32_t mem, void *stream);
+
+/* Neighbour data of the last short-range build, for bit-exact checks.
+ * qem_pair_list: (i, j) pairs with i < j, min-image rho <= r_cutoff
+ * (CellListMap.neighborlist set, QEM_short.jl:35); writes min(cap, npairs)
+ * pairs, always sets *npairs.  qem_cell_index: per particle cell id
+ * (cx * ncy + cy) of the 2-D binning and the per-cell start offsets. */
+qem_status qem_pair_list(qem_handle *h, int32_t N, const double *xyz, int32_t *pairs, int64_t cap, int64_t *npairs);
+qem_status qem_cell_index(qem_handle *h, int32_t N, const double *xyz, int32_t *cell, int32_t *cell_start,
+                          int32_t cap_cells, int32_t *ncx, int32_t *ncy);
+/* z order: zlist[m] = index of the m-th lowest z (sortperm, QEM_long.jl:39-40). */
+qem_status qem_z_order(qem_handle *h, int32_t N, const double *xyz, int32_t *zlist);
+
+/* Per-kernel device times (ms) of the last call, measured with CUDA events on
+ * the call's stream when profiling is enabled (0 = off).  names: a
+ * comma-separated list written into buf. */
+qem_status qem_set_profiling(qem_handle *h, int32_t on);
+qem_status qem_get_timings(const qem_handle *h, double *ms, int32_t cap, int32_t *n, char *names, int32_t names_cap);
+/* Counts of the last call: [0] pairs evaluated, [1] particles, [2] k-vectors,
+ * [3] kernel launches. */
+qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
+
+/* Library identity (version string and the compiled CUDA architecture). */
+const char *qem_version(void);
+
+/* Measured FP32 FMA throughput (TFLOP/s, 2 flops per FMA) and MUFU ex2
+ * throughput (Tops/s) of `device`: the roofline denominators of the QEM
+ * kernels, which are bound by those two pipes.  Diagnostic; no reference
+ * counterpart. */
+qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, double *mufu_tops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QEM_H */

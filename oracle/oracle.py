@@ -91,6 +91,9 @@ def lib():
             "qo_sigma_ns": (C.c_double, [dp, C.c_int, dp, dp, ip]),
             "qo_energy_k0": (C.c_double, [P, C.c_int, dp, dp, ip]),
             "qo_energy_long": (C.c_double, [P, C.c_int, dp, dp, ip, C.c_int, dp, C.c_double]),
+            "qo_pairs_eval": (None, [P, dp, dp, C.c_long, ip, dp, C.c_int]),
+            "qo_self_eval": (None, [P, C.c_int, dp, dp, dp, C.c_int]),
+            "qo_max_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -307,3 +310,23 @@ def lj_two_walls(xyz, walls):
         F, b = lj_forces(xyz, w["cutoff"], w["sigma"], w["eps"], w["sub_pos"], w["direction"], F)
         bad += b
     return F, bad
+
+
+def pairs_eval(p, xyz, q, pair_list, nthreads=0):
+    """F_short_ij rows (fx, fy, fz_i, fz_j) for the given pairs (timed CPU-baseline sample)."""
+    xyz, px = _d(xyz)
+    pl, pp = _i(pair_list)
+    out = np.zeros((pl.shape[0], 4))
+    lib().qo_pairs_eval(C.byref(p), px, _d(q)[1], pl.shape[0], pp, _d(out)[1], nthreads)
+    return out
+
+
+def self_eval(p, xyz, q, n, nthreads=0):
+    xyz, px = _d(xyz)
+    out = np.zeros(n)
+    lib().qo_self_eval(C.byref(p), n, px, _d(q)[1], _d(out)[1], nthreads)
+    return out
+
+
+def max_threads():
+    return lib().qo_max_threads()

@@ -803,3 +803,41 @@ double qo_energy_long(const qo_params *p, int N, const double *xyz, const double
     free(zlist);
     return E;
 }
+
+/* ------------------------------------------------------------------ */
+/* Bounded-sample drivers for the timed CPU baseline (bench.py).        */
+/* ------------------------------------------------------------------ */
+/* F_short_ij for npairs pairs (4 doubles per pair, see qo_F_short_ij). */
+void qo_pairs_eval(const qo_params *p, const double *xyz, const double *q, long npairs, const int *pairs,
+                   double *out, int nthreads)
+{
+    (void)nthreads;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (long t = 0; t < npairs; t++) {
+        int i = pairs[2 * t], j = pairs[2 * t + 1];
+        qo_F_short_ij(p, q[i], q[j], xyz + 3 * i, xyz + 3 * j, 0, out + 4 * t);
+    }
+}
+
+/* F_short_i for the first n particles. */
+void qo_self_eval(const qo_params *p, int n, const double *xyz, const double *q, double *out, int nthreads)
+{
+    (void)nthreads;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (int i = 0; i < n; i++) out[i] = qo_F_short_i(p, q[i], xyz + 3 * i, 0);
+}
+
+int qo_max_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,295 @@
+"""Python mirror of QEM4Molly's interaction API, backed by libqem.so.
+
+Names, keyword defaults and argument meaning follow the Julia package:
+
+    QEM_short(L, r_cutoff, alpha; iter_period=100, gamma_1=0, gamma_2=0,
+              eps_0=1, accuracy=1e-6, N_t=30)            src/QEM_short.jl:19-25
+    QEM_long(L; k_cutoff=1.0, z_list=[], gamma_1=0, gamma_2=0, eps_0=1,
+             accuracy=1e-6, alpha=1, rbe_mode=true, rbe_p=30) src/QEM_long.jl:19-30
+    QEM_inter(n_atoms, L; s=1.0, accuracy=1e-6, rbe_mode=true, rbe_p=30,
+              eps_0=1.0, gamma_1=0.0, gamma_2=0.0, N_t=30, iter_period=100)
+                                                          src/Quasi_Ewald_Method.jl:3-24
+    Substrate_LJ(; cutoff=1.0, sigma=0.5, eps=1.0, sub_pos=0.0, direction=+1)
+                                                          src/Substrate_LJ.jl:15-17
+    forces(inter, sys)  ==  Molly.forces(inter, sys, neighbors)
+
+`sys` is any object with `coords` (N x 3) and `charges` (N) -- the fields the
+reference reads from Molly's System (sys.coords, sys.atoms[i].charge).  The
+gamma_1 / gamma_2 names are the reference's: gamma_1 is the lower (z = 0)
+dielectric jump, gamma_2 the upper one.
+
+Extra keywords (not in the reference): `precision` ("fp64" or "fp32"),
+`mode` ("julia" = reference semantics, "python" = python_lib conventions),
+`seed` for the random-batch sampler, `device`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _mode_flags(mode: str) -> int:
+    if mode == "julia":
+        return 0
+    if mode == "python":
+        return L.QEM_PYTHON_MODE
+    raise ValueError("mode must be 'julia' or 'python'")
+
+
+def _precision(precision: str) -> int:
+    return {"fp64": L.QEM_FP64, "fp32": L.QEM_FP32_FIX}[precision]
+
+
+class Engine:
+    """One libqem handle: a configured QEM short + long + wall evaluator."""
+
+    def __init__(self, *, L_box, alpha, r_cutoff, gamma_1=0.0, gamma_2=0.0, eps_0=1.0, accuracy=1e-6,
+                 N_t=30, rbe_p=30, iter_period=100, walls=(), mode_flags=0, precision=L.QEM_FP64, device=0):
+        lib = L.load()
+        p = L.default_params()
+        p.Lx, p.Ly, p.Lz = (float(v) for v in L_box)
+        p.alpha, p.r_cutoff = float(alpha), float(r_cutoff)
+        p.gamma_down, p.gamma_up = float(gamma_1), float(gamma_2)
+        p.eps_0, p.accuracy = float(eps_0), float(accuracy)
+        p.N_t, p.rbe_p, p.iter_period = int(N_t), int(rbe_p), int(iter_period)
+        p.n_walls = len(walls)
+        for i, w in enumerate(walls):
+            p.walls[i] = L.LJWall(float(w.cutoff), float(w.sigma), float(w.eps), float(w.sub_pos),
+                                  float(w.direction))
+        p.mode_flags = int(mode_flags)
+        p.precision = int(precision)
+        p.device = int(device)
+        self.params = p
+        h = C.c_void_p()
+        st = lib.qem_create(C.byref(p), C.byref(h))
+        if st != 0:
+            raise L.QemError(st, "qem_create failed (see stderr for the parameter that was rejected)")
+        self._h = h
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.qem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise L.QemError(st, self._lib.qem_last_error(self._h).decode())
+
+    # -- k-set -----------------------------------------------------------------
+    def set_kset(self, k3, sum_K):
+        k3 = np.ascontiguousarray(k3, dtype=np.float64).reshape(-1, 3)
+        self._check(self._lib.qem_set_kset(self._h, k3.ctypes.data_as(C.POINTER(C.c_double)), k3.shape[0],
+                                           float(sum_K)))
+
+    def sample_kset(self, seed, P):
+        self._check(self._lib.qem_sample_kset(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(P)))
+
+    def get_kset(self):
+        P = C.c_int32()
+        s = C.c_double()
+        self._check(self._lib.qem_get_kset(self._h, None, 0, C.byref(P), C.byref(s)))
+        out = np.zeros((max(P.value, 1), 3))
+        self._check(self._lib.qem_get_kset(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), P.value, None,
+                                           None))
+        return out[:P.value], s.value
+
+    # -- evaluation ------------------------------------------------------------
+    def forces(self, xyz, q, terms=L.QEM_TERM_ALL, energy=False, out=None):
+        """Host arrays in, host arrays out.  Returns F (N x 3) or (F, E); `out` may be a
+        preallocated (e.g. pinned) float64 N x 3 array that receives the forces."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+        if q.shape[0] != xyz.shape[0]:
+            raise ValueError("coords and charges differ in length")
+        if out is not None:
+            if out.shape != xyz.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous float64 array shaped like xyz")
+            F = out
+        else:
+            F = np.zeros_like(xyz)
+        E = C.c_double(0.0)
+        st = self._lib.qem_forces(self._h, xyz.shape[0], xyz.ctypes.data, q.ctypes.data, F.ctypes.data,
+                                  C.byref(E) if energy else None, int(terms), L.QEM_MEM_HOST, None)
+        self._check(st)
+        return (F, E.value) if energy else F
+
+    def forces_device(self, xyz, q, F, terms=L.QEM_TERM_ALL, energy=False, stream=None):
+        """torch CUDA tensors (float64, contiguous) in place; returns the energy or None."""
+        import torch
+
+        for t in (xyz, q, F):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("device tensors must be contiguous float64 CUDA tensors")
+        s = stream if stream is not None else torch.cuda.current_stream(xyz.device).cuda_stream
+        E = C.c_double(0.0)
+        st = self._lib.qem_forces(self._h, q.shape[0], C.c_void_p(xyz.data_ptr()), C.c_void_p(q.data_ptr()),
+                                  C.c_void_p(F.data_ptr()), C.byref(E) if energy else None, int(terms),
+                                  L.QEM_MEM_DEVICE, C.c_void_p(s))
+        self._check(st)
+        return E.value if energy else None
+
+    def energy(self, xyz, q, terms=L.QEM_TERM_SHORT | L.QEM_TERM_LONG):
+        return self.forces(xyz, q, terms=terms, energy=True)[1]
+
+    def pair_list(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        n = C.c_int64()
+        dp = xyz.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self._lib.qem_pair_list(self._h, xyz.shape[0], dp, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 2), dtype=np.int32)
+        self._check(self._lib.qem_pair_list(self._h, xyz.shape[0], dp, out.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            n.value, C.byref(n)))
+        return out[:n.value]
+
+    def cell_index(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        ncx, ncy = C.c_int32(), C.c_int32()
+        self._check(self._lib.qem_cell_index(self._h, 0, xyz.ctypes.data_as(C.POINTER(C.c_double)), None, None, 0,
+                                             C.byref(ncx), C.byref(ncy)))
+        cell = np.zeros(xyz.shape[0], dtype=np.int32)
+        start = np.zeros(ncx.value * ncy.value + 1, dtype=np.int32)
+        ip = C.POINTER(C.c_int32)
+        self._check(self._lib.qem_cell_index(self._h, xyz.shape[0], xyz.ctypes.data_as(C.POINTER(C.c_double)),
+                                             cell.ctypes.data_as(ip), start.ctypes.data_as(ip), start.shape[0],
+                                             C.byref(ncx), C.byref(ncy)))
+        return cell, start, (ncx.value, ncy.value)
+
+    def z_order(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        z = np.zeros(xyz.shape[0], dtype=np.int32)
+        self._check(self._lib.qem_z_order(self._h, xyz.shape[0], xyz.ctypes.data_as(C.POINTER(C.c_double)),
+                                          z.ctypes.data_as(C.POINTER(C.c_int32))))
+        return z
+
+    def set_profiling(self, on=True):
+        self._check(self._lib.qem_set_profiling(self._h, 1 if on else 0))
+
+    def timings(self):
+        ms = (C.c_double * 32)()
+        n = C.c_int32()
+        names = C.create_string_buffer(1024)
+        self._check(self._lib.qem_get_timings(self._h, ms, 32, C.byref(n), names, 1024))
+        keys = names.value.decode().split(",") if n.value else []
+        return dict(zip(keys, list(ms)[: n.value]))
+
+    def counts(self):
+        c = (C.c_int64 * 4)()
+        self._check(self._lib.qem_get_counts(self._h, c, 4))
+        return dict(pairs=c[0], particles=c[1], kvectors=c[2], launches=c[3])
+
+
+@dataclass
+class Substrate_LJ:
+    """Substrate_LJ(; cutoff=1.0, sigma=0.5, eps=1.0, sub_pos=0.0, direction=+1)  (Substrate_LJ.jl:15)"""
+
+    cutoff: float = 1.0
+    sigma: float = 0.5
+    eps: float = 1.0
+    sub_pos: float = 0.0
+    direction: int = +1
+
+
+class QEM_short:
+    """QEM_short(L, r_cutoff, alpha; ...)  (QEM_short.jl:19-25).  Mutable n_steps as in the reference."""
+
+    def __init__(self, L, r_cutoff, alpha, *, iter_period=100, gamma_1=0, gamma_2=0, eps_0=1, accuracy=1e-6,
+                 N_t=30, precision="fp64", mode="julia", stale_neighbors=False, device=0):
+        self.L, self.r_cutoff, self.alpha = tuple(L), r_cutoff, alpha
+        self.iter_period, self.gamma_1, self.gamma_2 = iter_period, gamma_1, gamma_2
+        self.eps_0, self.accuracy, self.N_t = eps_0, accuracy, N_t
+        self.n_steps = 0
+        flags = _mode_flags(mode) | (L.QEM_STALE_NEIGHBORS if stale_neighbors else 0)
+        self.engine = Engine(L_box=self.L, alpha=alpha, r_cutoff=r_cutoff, gamma_1=gamma_1, gamma_2=gamma_2,
+                             eps_0=eps_0, accuracy=accuracy, N_t=N_t, rbe_p=0, iter_period=iter_period,
+                             mode_flags=flags, precision=_precision(precision), device=device)
+
+
+class QEM_long:
+    """QEM_long(L; k_cutoff, z_list, gamma_1, gamma_2, eps_0, accuracy, alpha, rbe_mode, rbe_p)
+    (QEM_long.jl:19-30).  A fresh random batch of rbe_p k-vectors is drawn on every forces call,
+    as Force_long.jl:235 does; pass `resample=False` to keep one batch."""
+
+    def __init__(self, L, *, k_cutoff=1.0, z_list=(), gamma_1=0, gamma_2=0, eps_0=1, accuracy=1e-6, alpha=1,
+                 rbe_mode=True, rbe_p=30, precision="fp64", mode="julia", seed=0, resample=True, device=0):
+        if not rbe_mode:
+            raise NotImplementedError("rbe_mode=false: the exact k-sum branch of Force_long.jl:220-233 is not "
+                                      "provided (it is broken in the reference)")
+        self.L, self.k_cutoff, self.z_list = tuple(L), k_cutoff, list(z_list)
+        self.gamma_1, self.gamma_2, self.eps_0, self.accuracy = gamma_1, gamma_2, eps_0, accuracy
+        self.alpha, self.rbe_mode, self.rbe_p = alpha, rbe_mode, rbe_p
+        flags = _mode_flags(mode) | (L.QEM_RESAMPLE_KSET if resample else 0)
+        # the short-range cutoff is irrelevant for the long range; any value < L/2 is valid
+        self.engine = Engine(L_box=self.L, alpha=alpha, r_cutoff=0.25 * min(self.L[0], self.L[1]),
+                             gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0, accuracy=accuracy, rbe_p=rbe_p,
+                             mode_flags=flags, precision=_precision(precision), device=device)
+        self.engine.sample_kset(seed, rbe_p)
+
+
+def QEM_inter(n_atoms, L, *, s=1.0, accuracy=1e-6, rbe_mode=True, rbe_p=30, eps_0=1.0, gamma_1=0.0, gamma_2=0.0,
+              N_t=30, iter_period=100, **kw):
+    """Quasi_Ewald_Method.jl:3-24: alpha = N / (Lx Ly), r_c = s / sqrt(alpha), k_c = 2 s sqrt(alpha)."""
+    Lx, Ly, _ = L
+    alpha = n_atoms / (Lx * Ly) if rbe_mode else np.sqrt(n_atoms) / (Lx * Ly)
+    r_cutoff = s / np.sqrt(alpha)
+    k_cutoff = 2 * s * np.sqrt(alpha)
+    short = QEM_short(L, r_cutoff, alpha, iter_period=iter_period, gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0,
+                      accuracy=accuracy, N_t=N_t, **{k: v for k, v in kw.items() if k != "seed"})
+    long = QEM_long(L, k_cutoff=k_cutoff, gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0, accuracy=accuracy,
+                    alpha=alpha, rbe_mode=rbe_mode, rbe_p=rbe_p if rbe_mode else 0, **kw)
+    return short, long
+
+
+@dataclass
+class System:
+    """Minimal stand-in for the parts of Molly's System the interactions read."""
+
+    coords: np.ndarray
+    charges: np.ndarray
+
+
+def forces(inter, sys, neighbors=None):
+    """Molly.forces(inter, sys, neighbors) for QEM_short / QEM_long / Substrate_LJ (N x 3)."""
+    xyz, q = np.asarray(sys.coords, dtype=np.float64), np.asarray(sys.charges, dtype=np.float64)
+    if isinstance(inter, QEM_short):
+        inter.n_steps += 1
+        return inter.engine.forces(xyz, q, terms=L.QEM_TERM_SHORT)
+    if isinstance(inter, QEM_long):
+        return inter.engine.forces(xyz, q, terms=L.QEM_TERM_LONG)
+    if isinstance(inter, Substrate_LJ):
+        e = _wall_engine(inter, xyz)
+        return e.forces(xyz, np.zeros(len(xyz)), terms=L.QEM_TERM_LJ)
+    raise TypeError(f"no forces for {type(inter).__name__}")
+
+
+def potential_energy(inter, sys, neighbors=None):
+    """Molly.potential_energy for the QEM interactions (python_lib energy formulas)."""
+    xyz, q = np.asarray(sys.coords, dtype=np.float64), np.asarray(sys.charges, dtype=np.float64)
+    if isinstance(inter, QEM_short):
+        return inter.engine.energy(xyz, q, terms=L.QEM_TERM_SHORT)
+    if isinstance(inter, QEM_long):
+        return inter.engine.energy(xyz, q, terms=L.QEM_TERM_LONG)
+    raise TypeError(f"no potential energy for {type(inter).__name__} (the reference defines none)")
+
+
+_WALL_ENGINES: dict = {}
+
+
+def _wall_engine(w: Substrate_LJ, xyz):
+    key = (w.cutoff, w.sigma, w.eps, w.sub_pos, w.direction)
+    e = _WALL_ENGINES.get(key)
+    if e is None:
+        # the box does not enter the wall force (Substrate_LJ.jl:34-43); any valid box works
+        e = Engine(L_box=(100.0, 100.0, 1.0), alpha=1.0, r_cutoff=1.0, walls=[w], rbe_p=0)
+        _WALL_ENGINES[key] = e
+    return e

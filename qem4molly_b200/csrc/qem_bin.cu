@@ -1,0 +1,482 @@
+// qem_bin.cu -- in-plane cell binning, pair list and z order.
+//
+// Replaces the neighbour machinery of the reference:
+//   CellListMap.neighborlist(xy, r_cutoff; unitcell)   QEM_short.jl:34-35
+//   Q2d_neighbor / update_neighbor                     Q2d_neighbor.jl:10-30
+//   sortperm(z) / bulket_sorting                       QEM_long.jl:39-40, bulket_sorting.jl:4-10
+//
+// Everything here is integer/byte work bound by memory latency and bandwidth;
+// the outputs are deterministic: cells list their particles in ascending
+// index, pairs are emitted in (cell order of i, stencil order, cell order of
+// j), the incoming lists are sorted by pair index, and the z order is the
+// stable ascending order of (z, index) -- identical to Julia's sortperm.
+#include "qem_internal.cuh"
+
+namespace {
+
+constexpr int SCAN_BLOCK = 1024;
+
+// ---------------------------------------------------------------------------
+// pack: AoS coordinates + charges -> double4, 2-D cell index, finiteness check
+// ---------------------------------------------------------------------------
+__global__ void k_pack(int N, const double *__restrict__ xyz, const double *__restrict__ q, double4 *__restrict__ pos,
+                       int *__restrict__ cell, CellGeom g, unsigned *status)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2], qq = q[i];
+    bool ok = isfinite(x) && isfinite(y) && isfinite(z) && isfinite(qq);
+    if (!ok) {
+        atomicOr(status, QEM_ST_NONFINITE);
+        x = 0; y = 0; z = 0; qq = 0;
+    }
+    pos[i] = make_double4(x, y, z, qq);
+    double xw = x - g.Lx * floor(x * g.invLx);
+    double yw = y - g.Ly * floor(y * g.invLy);
+    int cx = (int)(xw * g.inv_lcx), cy = (int)(yw * g.inv_lcy);
+    cx = min(max(cx, 0), g.ncx - 1);
+    cy = min(max(cy, 0), g.ncy - 1);
+    cell[i] = cx * g.ncy + cy;
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scans (block scan + scan of block sums + add); out[n] = total
+// ---------------------------------------------------------------------------
+template <typename TI, typename TO>
+__global__ void k_scan_block(const TI *__restrict__ in, TO *__restrict__ out, int n, TO *__restrict__ bsum)
+{
+    __shared__ TO warp_tot[SCAN_BLOCK / 32];
+    int i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+    TO v = (i < n) ? (TO)in[i] : (TO)0;
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    TO x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        TO t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        TO y = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            TO t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        warp_tot[lane] = y;  // inclusive over warps
+    }
+    __syncthreads();
+    TO incl = x + (w > 0 ? warp_tot[w - 1] : (TO)0);
+    if (i < n) out[i] = incl - v;  // exact for integers; for doubles see k_scan_block_excl
+    if (threadIdx.x == SCAN_BLOCK - 1) bsum[blockIdx.x] = incl;
+}
+
+// exclusive scan of doubles without the "inclusive minus own" subtraction
+__global__ void k_scan_block_excl_f64(const double *__restrict__ in, double *__restrict__ out, int n,
+                                      double *__restrict__ bsum)
+{
+    __shared__ double warp_tot[SCAN_BLOCK / 32];
+    int i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+    double v = (i < n) ? in[i] : 0.0;
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        double t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    double ex = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) ex = 0.0;
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        double y = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            double t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        double e = __shfl_up_sync(0xffffffffu, y, 1);
+        if (lane == 0) e = 0.0;
+        warp_tot[lane] = e;  // exclusive over warps
+        if (lane == 31) bsum[blockIdx.x] = y;
+    }
+    __syncthreads();
+    if (i < n) out[i] = warp_tot[w] + ex;
+}
+
+template <typename T>
+__global__ void k_scan_top(T *bsum, int nb)
+{
+    // one block: exclusive scan of nb block sums in place, chunks of SCAN_BLOCK with a carry
+    __shared__ T warp_tot[SCAN_BLOCK / 32];
+    __shared__ T carry;
+    if (threadIdx.x == 0) carry = (T)0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < nb; base += SCAN_BLOCK) {
+        int i = base + threadIdx.x;
+        T v = (i < nb) ? bsum[i] : (T)0;
+        T x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            T t = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += t;
+        }
+        T ex = __shfl_up_sync(0xffffffffu, x, 1);
+        if (lane == 0) ex = (T)0;
+        if (lane == 31) warp_tot[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            T y = warp_tot[lane];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                T t = __shfl_up_sync(0xffffffffu, y, d);
+                if (lane >= d) y += t;
+            }
+            T e = __shfl_up_sync(0xffffffffu, y, 1);
+            if (lane == 0) e = (T)0;
+            warp_tot[lane] = e;
+        }
+        __syncthreads();
+        T c = carry;
+        if (i < nb) bsum[i] = c + warp_tot[w] + ex;
+        __syncthreads();
+        if (threadIdx.x == SCAN_BLOCK - 1) carry = c + warp_tot[w] + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;  // grand total
+}
+
+template <typename T>
+__global__ void k_scan_add(T *__restrict__ out, int n, const T *__restrict__ bsum)
+{
+    int i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+    if (i < n) out[i] = bsum[blockIdx.x] + out[i];
+    if (i == 0) out[n] = bsum[(n + SCAN_BLOCK - 1) / SCAN_BLOCK];
+}
+
+// ---------------------------------------------------------------------------
+// cell counting sort
+// ---------------------------------------------------------------------------
+__global__ void k_cell_count(int N, const int *__restrict__ cell, int *cnt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) atomicAdd(&cnt[cell[i]], 1);
+}
+
+__global__ void k_cell_scatter(int N, const int *__restrict__ cell, int *fill, int *__restrict__ list)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) list[atomicAdd(&fill[cell[i]], 1)] = i;
+}
+
+// ascending particle index inside every cell (makes the slot order of the
+// atomic scatter irrelevant), and the inverse map particle -> sorted slot
+__global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__restrict__ list, int *__restrict__ pos_of)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int b = start[c], e = start[c + 1];
+    for (int s = b + 1; s < e; s++) {
+        int v = list[s], t = s - 1;
+        while (t >= b && list[t] > v) {
+            list[t + 1] = list[t];
+            t--;
+        }
+        list[t + 1] = v;
+    }
+    for (int s = b; s < e; s++) pos_of[list[s]] = s;
+}
+
+// ---------------------------------------------------------------------------
+// pair list (j > i, minimum-image rho^2 <= r_c^2)
+// ---------------------------------------------------------------------------
+// rho^2 with explicitly rounded operations so that the in/out decision is
+// bit-identical to an unfused CPU evaluation of the same expression.
+__device__ __forceinline__ double rho2_exact(double4 a, double4 b, const CellGeom &g)
+{
+    double dx = __dsub_rn(a.x, b.x), dy = __dsub_rn(a.y, b.y);
+    dx = __dsub_rn(dx, __dmul_rn(g.Lx, rint(dx / g.Lx)));
+    dy = __dsub_rn(dy, __dmul_rn(g.Ly, rint(dy / g.Ly)));
+    return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+__device__ __forceinline__ void stencil_range(int n, int &lo, int &hi)
+{
+    if (n >= 3) { lo = -1; hi = 1; }
+    else if (n == 2) { lo = 0; hi = 1; }
+    else { lo = 0; hi = 0; }
+}
+
+template <bool FILL>
+__global__ void k_pairs(int N, const double4 *__restrict__ pos, const int *__restrict__ cell,
+                        const int *__restrict__ cstart, const int *__restrict__ clist, CellGeom g, double rc2,
+                        int *__restrict__ pcount, const int64_t *__restrict__ poff, int2 *__restrict__ pairs)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    int i = clist[t];
+    double4 pi = pos[i];
+    int c = cell[i];
+    int cx = c / g.ncy, cy = c - cx * g.ncy;
+    int xlo, xhi, ylo, yhi;
+    stencil_range(g.ncx, xlo, xhi);
+    stencil_range(g.ncy, ylo, yhi);
+    int cnt = 0;
+    int64_t o = FILL ? poff[t] : 0;
+    for (int ox = xlo; ox <= xhi; ox++) {
+        int nx = cx + ox;
+        nx = nx < 0 ? nx + g.ncx : (nx >= g.ncx ? nx - g.ncx : nx);
+        for (int oy = ylo; oy <= yhi; oy++) {
+            int ny = cy + oy;
+            ny = ny < 0 ? ny + g.ncy : (ny >= g.ncy ? ny - g.ncy : ny);
+            int cc = nx * g.ncy + ny;
+            int b = cstart[cc], e = cstart[cc + 1];
+            for (int s = b; s < e; s++) {
+                int j = clist[s];
+                if (j <= i) continue;
+                if (rho2_exact(pi, pos[j], g) <= rc2) {
+                    if (FILL) pairs[o + cnt] = make_int2(i, j);
+                    cnt++;
+                }
+            }
+        }
+    }
+    if (!FILL) pcount[t] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// incoming pairs per particle (CSR over the second index), sorted by pair id
+// ---------------------------------------------------------------------------
+__global__ void k_in_count(int64_t Np, const int2 *__restrict__ pairs, int *cnt)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < Np) atomicAdd(&cnt[pairs[p].y], 1);
+}
+
+__global__ void k_in_fill(int64_t Np, const int2 *__restrict__ pairs, const int64_t *__restrict__ off, int *fill,
+                          int64_t *__restrict__ list)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= Np) return;
+    int j = pairs[p].y;
+    list[off[j] + atomicAdd(&fill[j], 1)] = p;
+}
+
+__global__ void k_in_sort(int N, const int64_t *__restrict__ off, int64_t *__restrict__ list)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int64_t b = off[i], e = off[i + 1];
+    for (int64_t s = b + 1; s < e; s++) {
+        int64_t v = list[s], t = s - 1;
+        while (t >= b && list[t] > v) {
+            list[t + 1] = list[t];
+            t--;
+        }
+        list[t + 1] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z order: bitonic sort of 1024-element tiles in shared memory, then merge
+// passes by co-ranking.  Keys are (z, index): a total order, so the result is
+// the stable ascending order of z.  Non-finite z was zeroed by k_pack.
+// ---------------------------------------------------------------------------
+constexpr int ZTILE = 1024;
+
+__device__ __forceinline__ bool zless(double za, int ia, double zb, int ib)
+{
+    return (za < zb) || (za == zb && ia < ib);
+}
+
+__global__ void k_ztile(int N, const double4 *__restrict__ pos, double *__restrict__ key, int *__restrict__ idx)
+{
+    __shared__ double sk[ZTILE];
+    __shared__ int si[ZTILE];
+    int base = blockIdx.x * ZTILE;
+    for (int t = threadIdx.x; t < ZTILE; t += blockDim.x) {
+        int i = base + t;
+        if (i < N) {
+            sk[t] = pos[i].z;
+            si[t] = i;
+        } else {
+            sk[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+            si[t] = 0x7fffffff;
+        }
+    }
+    __syncthreads();
+    for (int size = 2; size <= ZTILE; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < ZTILE / 2; t += blockDim.x) {
+                int lo = 2 * t - (t & (stride - 1));
+                int hi = lo + stride;
+                bool up = ((lo & size) == 0);
+                double ka = sk[lo], kb = sk[hi];
+                int ia = si[lo], ib = si[hi];
+                bool swap = up ? zless(kb, ib, ka, ia) : zless(ka, ia, kb, ib);
+                if (swap) {
+                    sk[lo] = kb; sk[hi] = ka;
+                    si[lo] = ib; si[hi] = ia;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int t = threadIdx.x; t < ZTILE; t += blockDim.x) {
+        int i = base + t;
+        if (i < N) {
+            key[i] = sk[t];
+            idx[i] = si[t];
+        }
+    }
+}
+
+__global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
+                         double *__restrict__ key_out, int *__restrict__ idx_out)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    int run = p / width;
+    int lstart = (run & ~1) * width;
+    int rstart = lstart + width;
+    int lend = min(rstart, N), rend = min(rstart + width, N);
+    double kz = key[p];
+    int ki = idx[p];
+    int pos_out;
+    if ((run & 1) == 0) {
+        // left element: count right-run elements strictly before it
+        int lo = rstart, hi = rend;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (zless(key[mid], idx[mid], kz, ki)) lo = mid + 1;
+            else hi = mid;
+        }
+        pos_out = lstart + (p - lstart) + (lo - rstart);
+    } else {
+        int lo = lstart, hi = lend;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (zless(key[mid], idx[mid], kz, ki)) lo = mid + 1;
+            else hi = mid;
+        }
+        pos_out = lstart + (p - rstart) + (lo - lstart);
+    }
+    key_out[pos_out] = kz;
+    idx_out[pos_out] = ki;
+}
+
+inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
+
+template <typename TI, typename TO>
+cudaError_t scan_impl(const TI *in, TO *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
+{
+    int nb = nblk(n, SCAN_BLOCK);
+    if (nb < 1) nb = 1;
+    if (tmp_bytes < sizeof(TO) * (size_t)(nb + 1)) return cudaErrorInvalidValue;
+    TO *bsum = (TO *)tmp;
+    k_scan_block<TI, TO><<<nb, SCAN_BLOCK, 0, s>>>(in, out, n, bsum);
+    k_scan_top<TO><<<1, SCAN_BLOCK, 0, s>>>(bsum, nb);
+    k_scan_add<TO><<<nb, SCAN_BLOCK, 0, s>>>(out, n, bsum);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t qem_scan_tmp_bytes(int n) { return sizeof(double) * (size_t)(nblk(n, SCAN_BLOCK) + 2); }
+
+cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
+{
+    return scan_impl<int, int64_t>(in, out, n, tmp, tmp_bytes, s);
+}
+
+cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
+{
+    int nb = nblk(n, SCAN_BLOCK);
+    if (nb < 1) nb = 1;
+    if (tmp_bytes < sizeof(double) * (size_t)(nb + 1)) return cudaErrorInvalidValue;
+    double *bsum = (double *)tmp;
+    k_scan_block_excl_f64<<<nb, SCAN_BLOCK, 0, s>>>(in, out, n, bsum);
+    k_scan_top<double><<<1, SCAN_BLOCK, 0, s>>>(bsum, nb);
+    k_scan_add<double><<<nb, SCAN_BLOCK, 0, s>>>(out, n, bsum);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *pos, int *cell, CellGeom g,
+                            unsigned *status, cudaStream_t s)
+{
+    if (N <= 0) return cudaSuccess;
+    k_pack<<<nblk(N, 256), 256, 0, s>>>(N, xyz, q, pos, cell, g, status);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_cells(int N, int ncell, const int *cell, int *cell_cnt, int *cell_start, int *cell_fill,
+                             int *cell_list, int *pos_of, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(cell_cnt, 0, sizeof(int) * ncell, s);
+    if (e != cudaSuccess) return e;
+    k_cell_count<<<nblk(N, 256), 256, 0, s>>>(N, cell, cell_cnt);
+    e = scan_impl<int, int>(cell_cnt, cell_start, ncell, scan_tmp, scan_tmp_bytes, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(cell_fill, cell_start, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    k_cell_scatter<<<nblk(N, 256), 256, 0, s>>>(N, cell, cell_fill, cell_list);
+    k_cell_sort<<<nblk(ncell, 128), 128, 0, s>>>(ncell, cell_start, cell_list, pos_of);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_pair_count(int N, const double4 *pos, const int *cell, const int *cell_start,
+                                  const int *cell_list, CellGeom g, double rc2, int *pcount, cudaStream_t s)
+{
+    k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
+                                                 nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_pair_fill(int N, const double4 *pos, const int *cell, const int *cell_start,
+                                 const int *cell_list, CellGeom g, double rc2, const int64_t *poff, int2 *pairs,
+                                 cudaStream_t s)
+{
+    k_pairs<true><<<nblk(N, 128), 128, 0, s>>>(N, pos, cell, cell_start, cell_list, g, rc2, nullptr, poff, pairs);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_incoming(int N, int64_t Np, const int2 *pairs, int *in_cnt, int64_t *in_off, int *in_fill,
+                                int64_t *in_list, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(in_cnt, 0, sizeof(int) * N, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(in_fill, 0, sizeof(int) * N, s);
+    if (e != cudaSuccess) return e;
+    if (Np > 0) k_in_count<<<nblk(Np, 256), 256, 0, s>>>(Np, pairs, in_cnt);
+    e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s);
+    if (e != cudaSuccess) return e;
+    if (Np > 0) k_in_fill<<<nblk(Np, 256), 256, 0, s>>>(Np, pairs, in_off, in_fill, in_list);
+    k_in_sort<<<nblk(N, 128), 128, 0, s>>>(N, in_off, in_list);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
+                             cudaStream_t s)
+{
+    if (N <= 0) return cudaSuccess;
+    k_ztile<<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
+    double *ka = zkey, *kb = zkey_tmp;
+    int *ia = zperm, *ib = ztmp;
+    int passes = 0;
+    for (int w = ZTILE; w < N; w <<= 1) {
+        k_zmerge<<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
+        double *tk = ka; ka = kb; kb = tk;
+        int *ti = ia; ia = ib; ib = ti;
+        passes++;
+    }
+    if (passes & 1) {
+        cudaError_t e = cudaMemcpyAsync(zperm, ia, sizeof(int) * N, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(zkey, ka, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}

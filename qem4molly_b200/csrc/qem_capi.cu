@@ -1,0 +1,766 @@
+// qem_capi.cu -- the C-ABI of libqem.so (include/qem.h): handle, parameter
+// validation, device scratch, k-set sampling and the per-call orchestration of
+// the binning, short-range and long-range kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qem_internal.cuh"
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+cudaError_t grow(DevBuf &b, size_t bytes)
+{
+    if (bytes <= b.cap && b.p) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t nb = std::max<size_t>(bytes + bytes / 4, 256);
+    cudaError_t e = cudaMalloc(&b.p, nb);
+    if (e == cudaSuccess) b.cap = nb;
+    return e;
+}
+
+template <typename T>
+T *ptr(DevBuf &b) { return (T *)b.p; }
+
+// Gauss-Legendre nodes on [-1, 1] (ascending) by Newton iteration on P_n
+void gauss_legendre(int n, double *x, double *w)
+{
+    for (int i = 0; i < (n + 1) / 2; i++) {
+        double z = cos(QEM_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; k++) {
+                double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (n == 1) { p0 = 1.0; p1 = z; }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (fabs(dz) < 1e-16) {
+                p0 = 1.0; p1 = z;
+                for (int k = 2; k <= n; k++) {
+                    double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                    p0 = p1;
+                    p1 = p2;
+                }
+                if (n == 1) { p0 = 1.0; p1 = z; }
+                dp = n * (z * p1 - p0) / (z * z - 1.0);
+                break;
+            }
+        }
+        double wi = 2.0 / ((1.0 - z * z) * dp * dp);
+        x[n - 1 - i] = z;
+        x[i] = -z;
+        w[i] = wi;
+        w[n - 1 - i] = wi;
+    }
+    if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+// splitmix64 (Steele, Lea, Flood 2014): seeded stream of 64-bit words
+inline uint64_t splitmix64(uint64_t &s)
+{
+    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+inline double uniform01(uint64_t &s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    int used = 0;
+    std::vector<std::string> names;
+    std::vector<std::pair<int, int>> spans;
+    std::vector<double> ms;
+    void begin() { used = 0; names.clear(); spans.clear(); }
+    int mark(cudaStream_t s)
+    {
+        if (!on) return -1;
+        if (used == (int)pool.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            pool.push_back(e);
+        }
+        cudaEventRecord(pool[used], s);
+        return used++;
+    }
+    void span(const char *n, int a, int b)
+    {
+        if (a >= 0 && b >= 0) { names.push_back(n); spans.push_back({a, b}); }
+    }
+    void finish()
+    {
+        ms.assign(spans.size(), 0.0);
+        for (size_t i = 0; i < spans.size(); i++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, pool[spans[i].first], pool[spans[i].second]);
+            ms[i] = t;
+        }
+    }
+};
+
+}  // namespace
+
+struct qem_handle {
+    qem_params p;
+    std::string err;
+    // k-set (host master copy)
+    std::vector<double> kset;
+    double sum_K = 0;
+    int P = 0;
+    bool has_kset = false, kset_dirty = true;
+    uint64_t rng = 0x51ed5eedULL;
+    std::vector<double> cdfx, cdfy;
+    long mxmax = 0, mymax = 0;
+    double sampler_sumK = 0;
+    double kmax = 0;
+    // geometry / constants
+    CellGeom geom;
+    int ncell = 0;
+    ShortConsts sc;
+    // device scratch
+    DevBuf xyz, q, F, pos, cell, cell_cnt, cell_start, cell_fill, cell_list, pos_of, pcount, poff, pairs, R, Upair,
+        in_cnt, in_off, in_fill, in_list, scan_tmp;
+    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, tot, off, Utot, Epart, status,
+        Eout;
+    unsigned *h_status = nullptr;
+    double *h_E = nullptr;
+    int64_t *h_np = nullptr;
+    // neighbour-list state (QEM_short.jl:32-36)
+    int64_t Np = 0;
+    int pairs_N = -1;
+    bool pairs_valid = false;
+    int64_t short_calls = 0;
+    Prof prof;
+    int64_t counts[4] = {0, 0, 0, 0};
+};
+
+static const char *status_str(qem_status s)
+{
+    switch (s) {
+    case QEM_OK: return "ok";
+    case QEM_ERR_ARG: return "invalid argument";
+    case QEM_ERR_OUT_OF_SLAB: return "particle run out of the box (Substrate_LJ wall)";
+    case QEM_ERR_NONFINITE: return "non-finite coordinate or charge";
+    case QEM_ERR_NB_OVERFLOW: return "neighbour capacity exceeded";
+    case QEM_ERR_TIMEOUT: return "device wait timed out";
+    case QEM_ERR_CUDA: return "CUDA error";
+    case QEM_ERR_NO_KSET: return "no k-set";
+    case QEM_ERR_RANGE: return "exponent range of the FP32 k-space path exceeded";
+    }
+    return "unknown status";
+}
+
+static qem_status fail(qem_handle *h, qem_status s, const std::string &msg)
+{
+    if (h) h->err = std::string(status_str(s)) + ": " + msg;
+    return s;
+}
+
+#define CU(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(h, QEM_ERR_CUDA, std::string(#call) + " -> " + cudaGetErrorString(e_));      \
+    } while (0)
+
+static bool finite_pos(double v) { return std::isfinite(v) && v > 0; }
+
+static qem_status validate(const qem_params *p, std::string &why)
+{
+    if (!p) { why = "params is NULL"; return QEM_ERR_ARG; }
+    if (!finite_pos(p->Lx) || !finite_pos(p->Ly) || !finite_pos(p->Lz)) { why = "box lengths must be > 0"; return QEM_ERR_ARG; }
+    if (!finite_pos(p->alpha)) { why = "alpha must be > 0"; return QEM_ERR_ARG; }
+    if (!finite_pos(p->r_cutoff) || !(p->r_cutoff < 0.5 * std::min(p->Lx, p->Ly))) {
+        why = "r_cutoff must be in (0, min(Lx, Ly) / 2)";
+        return QEM_ERR_ARG;
+    }
+    if (!(p->accuracy > 0 && p->accuracy < 1)) { why = "accuracy must be in (0, 1)"; return QEM_ERR_ARG; }
+    if (!finite_pos(p->eps_0)) { why = "eps_0 must be > 0"; return QEM_ERR_ARG; }
+    if (p->N_t < 1 || p->N_t > QEM_MAX_NT) { why = "N_t must be in 1..64"; return QEM_ERR_ARG; }
+    if (p->rbe_p < 0) { why = "rbe_p must be >= 0"; return QEM_ERR_ARG; }
+    if (p->iter_period < 1) { why = "iter_period must be >= 1"; return QEM_ERR_ARG; }
+    if (!std::isfinite(p->gamma_up) || !std::isfinite(p->gamma_down) || !(fabs(p->gamma_up * p->gamma_down) < 1.0)) {
+        why = "|gamma_up * gamma_down| must be < 1 (the regularised gamma >= 1 path is not provided)";
+        return QEM_ERR_ARG;
+    }
+    if (p->n_walls < 0 || p->n_walls > 2) { why = "n_walls must be 0..2"; return QEM_ERR_ARG; }
+    for (int w = 0; w < p->n_walls; w++) {
+        const qem_lj_wall &W = p->walls[w];
+        if (!(W.direction == 1.0 || W.direction == -1.0) || !std::isfinite(W.cutoff) || !std::isfinite(W.sigma) ||
+            !std::isfinite(W.eps) || !std::isfinite(W.sub_pos)) {
+            why = "wall parameters must be finite and direction +-1";
+            return QEM_ERR_ARG;
+        }
+    }
+    const uint32_t known = QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL | QEM_STALE_NEIGHBORS |
+                           QEM_RESAMPLE_KSET;
+    if (p->mode_flags & ~known) { why = "unknown mode flag"; return QEM_ERR_ARG; }
+    if (p->precision != QEM_FP64 && p->precision != QEM_FP32_FIX) { why = "precision must be QEM_FP64 or QEM_FP32_FIX"; return QEM_ERR_ARG; }
+    for (int i = 0; i < 5; i++)
+        if (p->reserved[i] != 0) { why = "reserved fields must be zero"; return QEM_ERR_ARG; }
+    return QEM_OK;
+}
+
+static void build_consts(qem_handle *h)
+{
+    const qem_params &p = h->p;
+    ShortConsts &c = h->sc;
+    memset(&c, 0, sizeof(c));
+    c.Lx = p.Lx; c.Ly = p.Ly; c.invLx = 1.0 / p.Lx; c.invLy = 1.0 / p.Ly;
+    c.Lz = p.Lz; c.twoLz = 2.0 * p.Lz;
+    c.alpha = p.alpha; c.inv4alpha = 1.0 / (4.0 * p.alpha);
+    c.rc2 = p.r_cutoff * p.r_cutoff;
+    c.g1 = p.gamma_down; c.g2 = p.gamma_up; c.g12 = p.gamma_down * p.gamma_up;
+    c.one_minus_g12 = 1.0 - c.g12;
+    c.neg_lnacc = -log(p.accuracy);
+    c.pref = 1.0 / (2.0 * QEM_PI * p.eps_0);
+    c.kf_gauss_py = sqrt(-4.0 * p.alpha * log(p.accuracy));
+    c.kf_point_py = -log(p.accuracy) / (2.0 * p.Lz);
+    c.Nt = p.N_t;
+    c.flags = p.mode_flags;
+    c.n_walls = p.n_walls;
+    for (int w = 0; w < p.n_walls; w++) {
+        c.wall_cut[w] = p.walls[w].cutoff;
+        c.wall_sig2[w] = p.walls[w].sigma * p.walls[w].sigma;
+        c.wall_eps[w] = p.walls[w].eps;
+        c.wall_pos[w] = p.walls[w].sub_pos;
+        c.wall_dir[w] = p.walls[w].direction;
+    }
+    double x[QEM_MAX_NT], w[QEM_MAX_NT];
+    gauss_legendre(p.N_t, x, w);
+    for (int i = 0; i < p.N_t; i++) {
+        c.xd[i] = x[i]; c.wd[i] = w[i];
+        c.xf[i] = (float)x[i]; c.wf[i] = (float)w[i];
+    }
+    // in-plane cells of side >= r_cutoff
+    CellGeom &g = h->geom;
+    int ncx = std::max(1, (int)floor(p.Lx / p.r_cutoff)), ncy = std::max(1, (int)floor(p.Ly / p.r_cutoff));
+    while ((int64_t)ncx * ncy > (1 << 24)) {
+        ncx = std::max(1, ncx / 2);
+        ncy = std::max(1, ncy / 2);
+    }
+    g.Lx = p.Lx; g.Ly = p.Ly; g.invLx = 1.0 / p.Lx; g.invLy = 1.0 / p.Ly;
+    g.ncx = ncx; g.ncy = ncy;
+    g.inv_lcx = ncx / p.Lx; g.inv_lcy = ncy / p.Ly;
+    h->ncell = ncx * ncy;
+    // separable k sampler: p(m) ~ exp(-(2 pi m / L)^2 / (4 alpha)), |m| <= ceil(k_c L / 2 pi) + 1
+    const double k_c = 2.0 * sqrt(-4.0 * p.alpha * log(p.accuracy));  // K_set_generator.jl:7
+    h->mxmax = (long)ceil(k_c * p.Lx / (2.0 * QEM_PI)) + 1;
+    h->mymax = (long)ceil(k_c * p.Ly / (2.0 * QEM_PI)) + 1;
+    auto cdf = [&](long mmax, double L, std::vector<double> &out) {
+        out.resize(2 * mmax + 1);
+        double s = 0;
+        for (long m = -mmax; m <= mmax; m++) {
+            const double k = 2.0 * QEM_PI * m / L;
+            s += exp(-k * k / (4.0 * p.alpha));
+            out[m + mmax] = s;
+        }
+        return s;
+    };
+    const double Sx = cdf(h->mxmax, p.Lx, h->cdfx), Sy = cdf(h->mymax, p.Ly, h->cdfy);
+    h->sampler_sumK = Sx * Sy - 1.0;  // = S_x + S_y + S_x S_y with m = 0 excluded (K_set_generator.jl:28)
+}
+
+static void sample_kset(qem_handle *h, int P)
+{
+    const qem_params &p = h->p;
+    h->kset.resize(3 * (size_t)P);
+    double kmax = 0;
+    for (int i = 0; i < P;) {
+        const double ux = uniform01(h->rng) * h->cdfx.back(), uy = uniform01(h->rng) * h->cdfy.back();
+        const long mx = (long)(std::upper_bound(h->cdfx.begin(), h->cdfx.end(), ux) - h->cdfx.begin()) - h->mxmax;
+        const long my = (long)(std::upper_bound(h->cdfy.begin(), h->cdfy.end(), uy) - h->cdfy.begin()) - h->mymax;
+        if (mx == 0 && my == 0) continue;
+        if (mx < -h->mxmax || mx > h->mxmax || my < -h->mymax || my > h->mymax) continue;
+        const double kx = 2.0 * QEM_PI * mx / p.Lx, ky = 2.0 * QEM_PI * my / p.Ly;
+        const double k = sqrt(kx * kx + ky * ky);
+        h->kset[3 * i] = kx;
+        h->kset[3 * i + 1] = ky;
+        h->kset[3 * i + 2] = k;
+        kmax = std::max(kmax, k);
+        i++;
+    }
+    h->P = P;
+    h->sum_K = h->sampler_sumK;
+    h->kmax = kmax;
+    h->has_kset = true;
+    h->kset_dirty = true;
+}
+
+// ---------------------------------------------------------------------------
+// one evaluation
+// ---------------------------------------------------------------------------
+static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
+                      uint32_t terms, int mem, cudaStream_t s)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (N < 0) return fail(h, QEM_ERR_ARG, "N < 0");
+    if (terms & ~QEM_TERM_ALL) return fail(h, QEM_ERR_ARG, "unknown term bit");
+    if (mem != QEM_MEM_HOST && mem != QEM_MEM_DEVICE) return fail(h, QEM_ERR_ARG, "mem must be HOST or DEVICE");
+    const bool do_short = terms & QEM_TERM_SHORT;
+    const bool do_long = terms & QEM_TERM_LONG;
+    const bool do_lj = (terms & QEM_TERM_LJ) && h->p.n_walls > 0;
+    const bool want_E = energy != nullptr;
+    if (N == 0) {
+        if (energy) *energy = 0;
+        return QEM_OK;
+    }
+    if (!xyz || !q || !F) return fail(h, QEM_ERR_ARG, "NULL coordinate, charge or force pointer");
+    CU(cudaSetDevice(h->p.device));
+    const int prec = h->p.precision;
+    h->prof.begin();
+    int launches = 0;
+    const int mk0 = h->prof.mark(s);
+
+    CU(grow(h->pos, sizeof(double4) * N));
+    CU(grow(h->cell, sizeof(int) * N));
+    CU(grow(h->status, 64));
+    CU(grow(h->Eout, 64));
+    const double *xyz_d = xyz, *q_d = q;
+    double *F_d = F;
+    if (mem == QEM_MEM_HOST) {
+        CU(grow(h->xyz, sizeof(double) * 3 * N));
+        CU(grow(h->q, sizeof(double) * N));
+        CU(grow(h->F, sizeof(double) * 3 * N));
+        CU(cudaMemcpyAsync(h->xyz.p, xyz, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(h->q.p, q, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+        xyz_d = ptr<double>(h->xyz);
+        q_d = ptr<double>(h->q);
+        F_d = ptr<double>(h->F);
+    }
+    unsigned *st = ptr<unsigned>(h->status);
+    CU(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+    const int mk_in = h->prof.mark(s);
+    CU(qem_launch_pack(N, xyz_d, q_d, ptr<double4>(h->pos), ptr<int>(h->cell), h->geom, st, s));
+    launches++;
+
+    // energy partials: [short blocks | long chunks | k0 blocks | P split terms]
+    const int LCH = qem_long_chunk();
+    const int nbS = (N + 255) / 256, nch = (N + LCH - 1) / LCH, nb0 = (N + 255) / 256;
+    const int P = do_long ? (h->has_kset ? h->P : 0) : 0;
+    CU(grow(h->Epart, sizeof(double) * (size_t)(nbS + nch + nb0 + std::max(P, h->p.rbe_p) + 8)));
+    double *Ep = ptr<double>(h->Epart);
+    if (want_E) CU(cudaMemsetAsync(Ep, 0, sizeof(double) * (size_t)(nbS + nch + nb0 + std::max(P, h->p.rbe_p) + 8), s));
+    CU(grow(h->scan_tmp, qem_scan_tmp_bytes(std::max(std::max(N, h->ncell), 1)) + 64));
+
+    int mk_bin = -1, mk_pair = -1, mk_gather = -1;
+    if (do_short) {
+        const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
+        const bool rebuild = !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
+        if (rebuild) {
+            CU(grow(h->cell_cnt, sizeof(int) * h->ncell));
+            CU(grow(h->cell_start, sizeof(int) * (h->ncell + 1)));
+            CU(grow(h->cell_fill, sizeof(int) * h->ncell));
+            CU(grow(h->cell_list, sizeof(int) * N));
+            CU(grow(h->pos_of, sizeof(int) * N));
+            CU(grow(h->pcount, sizeof(int) * N));
+            CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
+            CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<int>(h->cell_cnt), ptr<int>(h->cell_start),
+                                ptr<int>(h->cell_fill), ptr<int>(h->cell_list), ptr<int>(h->pos_of), h->scan_tmp.p,
+                                h->scan_tmp.cap, s));
+            CU(qem_launch_pair_count(N, ptr<double4>(h->pos), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                                     ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), s));
+            CU(qem_scan_i32_to_i64(ptr<int>(h->pcount), ptr<int64_t>(h->poff), N, h->scan_tmp.p, h->scan_tmp.cap, s));
+            CU(cudaMemcpyAsync(h->h_np, ptr<int64_t>(h->poff) + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            const int64_t Np = *h->h_np;
+            CU(grow(h->pairs, sizeof(int2) * std::max<int64_t>(Np, 1)));
+            CU(grow(h->R, sizeof(double4) * std::max<int64_t>(Np, 1)));
+            CU(grow(h->Upair, sizeof(double) * std::max<int64_t>(Np, 1)));
+            CU(grow(h->in_cnt, sizeof(int) * N));
+            CU(grow(h->in_fill, sizeof(int) * N));
+            CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
+            CU(grow(h->in_list, sizeof(int64_t) * std::max<int64_t>(Np, 1)));
+            CU(qem_launch_pair_fill(N, ptr<double4>(h->pos), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                                    ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
+                                    ptr<int2>(h->pairs), s));
+            CU(qem_launch_incoming(N, Np, ptr<int2>(h->pairs), ptr<int>(h->in_cnt), ptr<int64_t>(h->in_off),
+                                   ptr<int>(h->in_fill), ptr<int64_t>(h->in_list), h->scan_tmp.p, h->scan_tmp.cap, s));
+            launches += 16;
+            h->Np = Np;
+            h->pairs_N = N;
+            h->pairs_valid = true;
+        }
+        h->short_calls++;
+        mk_bin = h->prof.mark(s);
+        CU(qem_launch_short_pairs(prec, want_E, h->Np, ptr<int2>(h->pairs), ptr<double4>(h->pos), ptr<double4>(h->R),
+                                  ptr<double>(h->Upair), h->sc, s));
+        launches += h->Np > 0;
+        mk_pair = h->prof.mark(s);
+    }
+    if (do_short || do_lj) {
+        CU(qem_launch_short_gather(prec, want_E, do_short, do_lj, N, ptr<double4>(h->pos), ptr<int>(h->pos_of),
+                                   ptr<int64_t>(h->poff), ptr<double4>(h->R), ptr<double>(h->Upair),
+                                   ptr<int64_t>(h->in_off), ptr<int64_t>(h->in_list), h->sc, F_d, Ep, st, s));
+        launches++;
+    } else {
+        CU(cudaMemsetAsync(F_d, 0, sizeof(double) * 3 * N, s));
+    }
+    mk_gather = h->prof.mark(s);
+
+    int mk_lprep = -1, mk_lforce = -1;
+    if (do_long) {
+        if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+        else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+        const int Pk = h->has_kset ? h->P : 0;
+        if (prec == QEM_FP32_FIX && Pk > 0 && h->kmax * h->p.Lz > 120.0)
+            return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
+        CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
+        if (h->kset_dirty && Pk > 0) {
+            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
+            h->kset_dirty = false;
+        }
+        CU(grow(h->zperm, sizeof(int) * N));
+        CU(grow(h->ztmp, sizeof(int) * N));
+        CU(grow(h->zkey, sizeof(double) * N));
+        CU(grow(h->zkey2, sizeof(double) * N));
+        CU(grow(h->zx, sizeof(double) * N));
+        CU(grow(h->zy, sizeof(double) * N));
+        CU(grow(h->zhf, sizeof(float) * N));
+        CU(grow(h->zhd, sizeof(double) * N));
+        CU(grow(h->qf, sizeof(float) * N));
+        CU(grow(h->qd, sizeof(double) * N));
+        CU(grow(h->k0, sizeof(double) * N));
+        CU(grow(h->qscan, sizeof(double) * (N + 1)));
+        CU(grow(h->kc, sizeof(KConst) * std::max(Pk, 1)));
+        CU(grow(h->tot, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
+        CU(grow(h->off, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
+        CU(grow(h->Utot, sizeof(double) * 4 * std::max(Pk, 1)));
+        CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
+                            ptr<double>(h->zkey2), s));
+        LongBuffers b;
+        b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
+        b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
+        b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
+        b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
+        b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
+        b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
+        b.Epart = Ep + nbS;
+        b.Eks = Ep + nbS + nch + nb0;
+        b.stmp = h->scan_tmp.p; b.stmp_bytes = h->scan_tmp.cap;
+        CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, F_d, nch, st, s, 0));
+        mk_lprep = h->prof.mark(s);
+        CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, F_d, nch, st, s, 1));
+        mk_lforce = h->prof.mark(s);
+        launches += 8;
+        h->counts[2] = Pk;
+    } else {
+        h->counts[2] = 0;
+    }
+    if (want_E) {
+        const int nE = nbS + nch + nb0 + (do_long ? (h->has_kset ? h->P : 0) : 0);
+        CU(qem_launch_reduce_sum(Ep, nE, ptr<double>(h->Eout), s));
+        launches++;
+        CU(cudaMemcpyAsync(h->h_E, h->Eout.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    if (mem == QEM_MEM_HOST) CU(cudaMemcpyAsync(F, F_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    const int mk_end = h->prof.mark(s);
+    CU(cudaStreamSynchronize(s));
+    CU(cudaGetLastError());
+    h->prof.span("upload", mk0, mk_in);
+    h->prof.span("bin_pairs", mk_in, mk_bin);
+    h->prof.span("short_pair", mk_bin, mk_pair);
+    h->prof.span("short_gather", mk_pair >= 0 ? mk_pair : mk_in, mk_gather);
+    h->prof.span("long_prep", mk_gather, mk_lprep);
+    h->prof.span("long_force", mk_lprep, mk_lforce);
+    h->prof.span("total", mk0, mk_end);
+    if (h->prof.on) h->prof.finish();
+    h->counts[0] = do_short ? h->Np : 0;
+    h->counts[1] = N;
+    h->counts[3] = launches;
+    const unsigned stv = *h->h_status;
+    if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
+    if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    if (want_E) *energy = *h->h_E;
+    h->err.clear();
+    return QEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// exported C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void qem_default_params(qem_params *p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->Lx = p->Ly = p->Lz = 1.0;
+    p->alpha = 1.0;
+    p->r_cutoff = 0.25;
+    p->eps_0 = 1.0;
+    p->accuracy = 1e-6;
+    p->N_t = 30;
+    p->rbe_p = 30;
+    p->iter_period = 100;
+    p->precision = QEM_FP64;
+}
+
+qem_status qem_inter_params(qem_params *p, int64_t n_atoms, double s, int32_t rbe_mode, int32_t rbe_p)
+{
+    if (!p || n_atoms <= 0 || !(s > 0) || !(p->Lx > 0) || !(p->Ly > 0)) return QEM_ERR_ARG;
+    const double area = p->Lx * p->Ly;
+    p->alpha = rbe_mode ? (double)n_atoms / area : sqrt((double)n_atoms) / area;  // Quasi_Ewald_Method.jl:6, 14
+    p->r_cutoff = s / sqrt(p->alpha);                                             // Quasi_Ewald_Method.jl:7, 15
+    p->rbe_p = rbe_mode ? rbe_p : 0;
+    return QEM_OK;
+}
+
+qem_status qem_create(const qem_params *p, qem_handle **out)
+{
+    if (!out) return QEM_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    qem_status st = validate(p, why);
+    if (st != QEM_OK) {
+        fprintf(stderr, "qem_create: %s\n", why.c_str());
+        return st;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || p->device < 0 || p->device >= ndev) return QEM_ERR_CUDA;
+    if (cudaSetDevice(p->device) != cudaSuccess) return QEM_ERR_CUDA;
+    qem_handle *h = new qem_handle();
+    h->p = *p;
+    build_consts(h);
+    if (cudaMallocHost(&h->h_status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMallocHost(&h->h_E, sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&h->h_np, sizeof(int64_t)) != cudaSuccess) {
+        qem_destroy(h);
+        return QEM_ERR_CUDA;
+    }
+    *out = h;
+    return QEM_OK;
+}
+
+void qem_destroy(qem_handle *h)
+{
+    if (!h) return;
+    cudaSetDevice(h->p.device);
+    DevBuf *bufs[] = {&h->xyz, &h->q, &h->F, &h->pos, &h->cell, &h->cell_cnt, &h->cell_start, &h->cell_fill,
+                      &h->cell_list, &h->pos_of, &h->pcount, &h->poff, &h->pairs, &h->R, &h->Upair, &h->in_cnt,
+                      &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
+                      &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin,
+                      &h->tot, &h->off, &h->Utot, &h->Epart, &h->status, &h->Eout};
+    for (DevBuf *b : bufs)
+        if (b->p) cudaFree(b->p);
+    for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
+    if (h->h_status) cudaFreeHost(h->h_status);
+    if (h->h_E) cudaFreeHost(h->h_E);
+    if (h->h_np) cudaFreeHost(h->h_np);
+    delete h;
+}
+
+const char *qem_last_error(const qem_handle *h) { return h ? h->err.c_str() : "NULL handle"; }
+const char *qem_status_string(qem_status s) { return status_str(s); }
+
+qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (P < 0 || (P > 0 && !k3) || !std::isfinite(sum_K)) return fail(h, QEM_ERR_ARG, "bad k-set arguments");
+    double kmax = 0;
+    for (int i = 0; i < P; i++) {
+        const double kx = k3[3 * i], ky = k3[3 * i + 1], k = k3[3 * i + 2];
+        if (!std::isfinite(kx) || !std::isfinite(ky) || !(k > 0) || fabs(kx * kx + ky * ky - k * k) > 1e-9 * k * k)
+            return fail(h, QEM_ERR_ARG, "k-set rows must be (kx, ky, |k|) with |k| > 0 (Force_long.jl:7)");
+        kmax = std::max(kmax, k);
+    }
+    h->kset.assign(k3, k3 + 3 * (size_t)P);
+    h->P = P;
+    h->sum_K = sum_K;
+    h->kmax = kmax;
+    h->has_kset = true;
+    h->kset_dirty = true;
+    return QEM_OK;
+}
+
+qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (P < 0) return fail(h, QEM_ERR_ARG, "P < 0");
+    h->rng = seed;
+    sample_kset(h, P);
+    return QEM_OK;
+}
+
+qem_status qem_get_kset(const qem_handle *h, double *k3_out, int32_t cap, int32_t *P, double *sum_K)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (P) *P = h->P;
+    if (sum_K) *sum_K = h->sum_K;
+    if (k3_out && cap > 0) memcpy(k3_out, h->kset.data(), sizeof(double) * 3 * (size_t)std::min(cap, h->P));
+    return QEM_OK;
+}
+
+qem_status qem_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, double *energy,
+                      uint32_t terms, int32_t mem, void *stream)
+{
+    return run(h, N, xyz, q, F, energy, terms, mem, (cudaStream_t)stream);
+}
+
+qem_status qem_short_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, int32_t mem,
+                            void *stream)
+{
+    return run(h, N, xyz, q, F, nullptr, QEM_TERM_SHORT, mem, (cudaStream_t)stream);
+}
+
+qem_status qem_long_forces(qem_handle *h, int32_t N, const double *xyz, const double *q, double *F, int32_t mem,
+                           void *stream)
+{
+    return run(h, N, xyz, q, F, nullptr, QEM_TERM_LONG, mem, (cudaStream_t)stream);
+}
+
+qem_status qem_lj_forces(qem_handle *h, int32_t N, const double *xyz, double *F, int32_t mem, void *stream)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (N < 0) return fail(h, QEM_ERR_ARG, "N < 0");
+    if (N == 0) return QEM_OK;
+    if (!xyz || !F) return fail(h, QEM_ERR_ARG, "NULL pointer");
+    // charges are not used by the walls; feed zeros of the right memory kind
+    std::vector<double> qz;
+    const double *q = nullptr;
+    DevBuf tmp;
+    if (mem == QEM_MEM_HOST) {
+        qz.assign(N, 0.0);
+        q = qz.data();
+    } else {
+        CU(cudaSetDevice(h->p.device));
+        CU(grow(tmp, sizeof(double) * N));
+        CU(cudaMemsetAsync(tmp.p, 0, sizeof(double) * N, (cudaStream_t)stream));
+        q = ptr<double>(tmp);
+    }
+    qem_status st = run(h, N, xyz, q, F, nullptr, QEM_TERM_LJ, mem, (cudaStream_t)stream);
+    if (tmp.p) cudaFree(tmp.p);
+    return st;
+}
+
+qem_status qem_potential_energy(qem_handle *h, int32_t N, const double *xyz, const double *q, double *energy,
+                                uint32_t terms, int32_t mem, void *stream)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (!energy) return fail(h, QEM_ERR_ARG, "energy is NULL");
+    if (N <= 0) return run(h, N, xyz, q, nullptr, energy, terms, mem, (cudaStream_t)stream);
+    DevBuf tmp;
+    double *F = nullptr;
+    std::vector<double> Fh;
+    if (mem == QEM_MEM_HOST) {
+        Fh.resize(3 * (size_t)N);
+        F = Fh.data();
+    } else {
+        CU(cudaSetDevice(h->p.device));
+        CU(grow(tmp, sizeof(double) * 3 * N));
+        F = ptr<double>(tmp);
+    }
+    qem_status st = run(h, N, xyz, q, F, energy, terms, mem, (cudaStream_t)stream);
+    if (tmp.p) cudaFree(tmp.p);
+    return st;
+}
+
+qem_status qem_pair_list(qem_handle *h, int32_t N, const double *xyz, int32_t *pairs, int64_t cap, int64_t *npairs)
+{
+    if (!h || !npairs || N < 0 || (N > 0 && !xyz)) return QEM_ERR_ARG;
+    *npairs = 0;
+    if (N == 0) return QEM_OK;
+    std::vector<double> q(N, 0.0), F(3 * (size_t)N);
+    const uint32_t saved = h->p.mode_flags;
+    h->p.mode_flags &= ~QEM_STALE_NEIGHBORS;  // always a fresh list
+    qem_status st = run(h, N, xyz, q.data(), F.data(), nullptr, QEM_TERM_SHORT, QEM_MEM_HOST, 0);
+    h->p.mode_flags = saved;
+    if (st != QEM_OK) return st;
+    *npairs = h->Np;
+    if (pairs && cap > 0 && h->Np > 0) {
+        const int64_t n = std::min(cap, h->Np);
+        CU(cudaMemcpy(pairs, h->pairs.p, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+    }
+    return QEM_OK;
+}
+
+qem_status qem_cell_index(qem_handle *h, int32_t N, const double *xyz, int32_t *cell, int32_t *cell_start,
+                          int32_t cap_cells, int32_t *ncx, int32_t *ncy)
+{
+    if (!h || N < 0 || (N > 0 && !xyz)) return QEM_ERR_ARG;
+    if (ncx) *ncx = h->geom.ncx;
+    if (ncy) *ncy = h->geom.ncy;
+    if (N == 0) return QEM_OK;
+    int64_t np = 0;
+    qem_status st = qem_pair_list(h, N, xyz, nullptr, 0, &np);
+    if (st != QEM_OK) return st;
+    if (cell) CU(cudaMemcpy(cell, h->cell.p, sizeof(int) * N, cudaMemcpyDeviceToHost));
+    if (cell_start && cap_cells > 0)
+        CU(cudaMemcpy(cell_start, h->cell_start.p, sizeof(int) * std::min(cap_cells, h->ncell + 1),
+                      cudaMemcpyDeviceToHost));
+    return QEM_OK;
+}
+
+qem_status qem_z_order(qem_handle *h, int32_t N, const double *xyz, int32_t *zlist)
+{
+    if (!h || N < 0 || (N > 0 && (!xyz || !zlist))) return QEM_ERR_ARG;
+    if (N == 0) return QEM_OK;
+    std::vector<double> q(N, 0.0), F(3 * (size_t)N);
+    const int P = h->P;
+    const bool had = h->has_kset;
+    h->P = 0;  // k = 0 term only: runs the z sort without k-space work
+    h->has_kset = true;
+    const int32_t saved_rbe = h->p.rbe_p;
+    h->p.rbe_p = 0;
+    qem_status st = run(h, N, xyz, q.data(), F.data(), nullptr, QEM_TERM_LONG, QEM_MEM_HOST, 0);
+    h->P = P;
+    h->has_kset = had;
+    h->p.rbe_p = saved_rbe;
+    if (st != QEM_OK) return st;
+    CU(cudaMemcpy(zlist, h->zperm.p, sizeof(int) * N, cudaMemcpyDeviceToHost));
+    return QEM_OK;
+}
+
+qem_status qem_set_profiling(qem_handle *h, int32_t on)
+{
+    if (!h) return QEM_ERR_ARG;
+    h->prof.on = on != 0;
+    return QEM_OK;
+}
+
+qem_status qem_get_timings(const qem_handle *h, double *ms, int32_t cap, int32_t *n, char *names, int32_t names_cap)
+{
+    if (!h) return QEM_ERR_ARG;
+    const int cnt = (int)h->prof.ms.size();
+    if (n) *n = cnt;
+    if (ms)
+        for (int i = 0; i < std::min(cap, cnt); i++) ms[i] = h->prof.ms[i];
+    if (names && names_cap > 0) {
+        std::string s;
+        for (int i = 0; i < (int)h->prof.names.size(); i++) {
+            if (i) s += ",";
+            s += h->prof.names[i];
+        }
+        snprintf(names, names_cap, "%s", s.c_str());
+    }
+    return QEM_OK;
+}
+
+qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap)
+{
+    if (!h || !counts) return QEM_ERR_ARG;
+    for (int i = 0; i < std::min(cap, 4); i++) counts[i] = h->counts[i];
+    return QEM_OK;
+}
+
+const char *qem_version(void) { return "qem4molly_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// qem_diag.cu -- measured throughput peaks used as roofline denominators.
+//
+// The QEM kernels are bound by the FP32 FMA pipe and the MUFU (SFU) pipe, not
+// by HBM or tensor cores, so their roofline needs the device's own FP32 FMA
+// and MUFU rates: these kernels measure them with CUDA events (dependent-free
+// chains of 8 independent accumulators per thread, enough warps to fill every
+// SM).
+#include <algorithm>
+
+#include "qem_internal.cuh"
+
+namespace {
+
+__global__ void k_fma_peak(int iters, float seed, float *out)
+{
+    float a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+          a7 = a0 + 7;
+    const float m = 0.9999999f, c = 1e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 1234.5f) out[0] = s;  // keeps the chain alive
+}
+
+__global__ void k_mufu_peak(int iters, float seed, float *out)
+{
+    float a0 = seed * threadIdx.x * 1e-6f, a1 = a0 + 0.1f, a2 = a0 + 0.2f, a3 = a0 + 0.3f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            asm volatile("ex2.approx.ftz.f32 %0, %0;" : "+f"(a0));
+            asm volatile("ex2.approx.ftz.f32 %0, %0;" : "+f"(a1));
+            asm volatile("ex2.approx.ftz.f32 %0, %0;" : "+f"(a2));
+            asm volatile("ex2.approx.ftz.f32 %0, %0;" : "+f"(a3));
+        }
+    }
+    const float s = a0 + a1 + a2 + a3;
+    if (s == 1234.5f) out[0] = s;
+}
+
+}  // namespace
+
+extern "C" qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, double *mufu_tops)
+{
+    if (cudaSetDevice(device) != cudaSuccess) return QEM_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return QEM_ERR_CUDA;
+    float *d = nullptr;
+    if (cudaMalloc(&d, 64) != cudaSuccess) return QEM_ERR_CUDA;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = prop.multiProcessorCount * 8, threads = 256;
+    const int it_fma = 4096, it_mufu = 1024;
+    float best_f = 1e30f, best_m = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        float t = 0;
+        cudaEventRecord(a);
+        k_fma_peak<<<blocks, threads>>>(it_fma, 1.0f, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t, a, b);
+        if (rep > 0) best_f = std::min(best_f, t);
+        cudaEventRecord(a);
+        k_mufu_peak<<<blocks, threads>>>(it_mufu, 1.0f, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t, a, b);
+        if (rep > 0) best_m = std::min(best_m, t);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return QEM_ERR_CUDA;
+    const double nthr = (double)blocks * threads;
+    if (fp32_tflops) *fp32_tflops = 2.0 * nthr * it_fma * 16 * 8 / (best_f * 1e-3) * 1e-12;
+    if (mufu_tops) *mufu_tops = nthr * it_mufu * 16 * 4 / (best_m * 1e-3) * 1e-12;
+    return QEM_OK;
+}

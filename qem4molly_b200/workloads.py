@@ -1,0 +1,103 @@
+"""Seeded synthetic slab systems with the shapes of the benchmark configurations.
+
+Each generator returns a dict with coordinates (N x 3), charges (N), box L,
+and the QEM parameters.  Charges are exactly neutral.  Seeds are fixed
+(20261203 + config index) so every run sees the same systems.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SEED0 = 20261203
+
+
+def _slab(rng, N, Lx, Ly, zlo, zhi):
+    return np.stack([rng.random(N) * Lx, rng.random(N) * Ly, zlo + rng.random(N) * (zhi - zlo)], axis=1)
+
+
+def _pm_charges(N):
+    q = np.ones(N)
+    q[N // 2:] = -1.0
+    if N % 2:
+        q[-1] = 0.0
+    return q
+
+
+def config1(seed=None):
+    """N=100 (50 +1, 50 -1), Lx=Ly=100, Lz=10, gamma_up=0.95, gamma_down=-0.95, alpha=0.1, r_c=10,
+    N_t=30, P=100, LJ walls at z=0 (+1) and z=10 (-1) with eps=1, sigma=1, cutoff=1."""
+    rng = np.random.default_rng(SEED0 + 1 if seed is None else seed)
+    N = 100
+    return dict(name="config1_N100_slab", N=N, L=(100.0, 100.0, 10.0), xyz=_slab(rng, N, 100.0, 100.0, 0.5, 9.5),
+                q=_pm_charges(N), alpha=0.1, r_cutoff=10.0, gamma_up=0.95, gamma_down=-0.95, N_t=30,
+                accuracy=1e-6, P=100,
+                walls=[dict(cutoff=1.0, sigma=1.0, eps=1.0, sub_pos=0.0, direction=+1),
+                       dict(cutoff=1.0, sigma=1.0, eps=1.0, sub_pos=10.0, direction=-1)])
+
+
+def config2(seed=None, N=100_000):
+    """N=1e5 (+-1, neutral), Lx=Ly=1000, Lz=10, z in [0.5, 9.5], gamma_up=gamma_down=0.95,
+    alpha=0.1, r_c=10, P=500 (about 31 neighbours within r_c)."""
+    rng = np.random.default_rng(SEED0 + 2 if seed is None else seed)
+    L = 1000.0 * np.sqrt(N / 100_000)
+    return dict(name=f"config2_N{N}_slab", N=N, L=(L, L, 10.0), xyz=_slab(rng, N, L, L, 0.5, 9.5),
+                q=_pm_charges(N), alpha=0.1, r_cutoff=10.0, gamma_up=0.95, gamma_down=0.95, N_t=30,
+                accuracy=1e-6, P=500, walls=[])
+
+
+def config3(seed=None, N=20_000):
+    """N=2e4, |q| ~ U[0.5, 1.5] with random sign, re-neutralised; Lx=Ly=450, Lz=10,
+    gamma_up=0.8, gamma_down=-0.6."""
+    rng = np.random.default_rng(SEED0 + 3 if seed is None else seed)
+    L = 450.0 * np.sqrt(N / 20_000)
+    q = rng.uniform(0.5, 1.5, N) * rng.choice([-1.0, 1.0], N)
+    q[-1] -= q.sum()
+    return dict(name=f"config3_N{N}_slab", N=N, L=(L, L, 10.0), xyz=_slab(rng, N, L, L, 0.5, 9.5), q=q,
+                alpha=0.1, r_cutoff=10.0, gamma_up=0.8, gamma_down=-0.6, N_t=30, accuracy=1e-6, P=500, walls=[])
+
+
+def config4(seed=None, n_systems=256):
+    """256 independent slabs, N ~ U[200, 5000], Lz ~ U[5, 20], Lx=Ly from density 0.01,
+    gamma pairs ~ U(-0.95, 0.95)^2, alpha=0.1, r_c=10, P=200."""
+    rng = np.random.default_rng(SEED0 + 4 if seed is None else seed)
+    out = []
+    for s in range(n_systems):
+        N = int(rng.integers(200, 5001))
+        Lz = float(rng.uniform(5, 20))
+        L = float(np.sqrt(N / 0.01))
+        gu, gd = rng.uniform(-0.95, 0.95, 2)
+        out.append(dict(name=f"config4_sys{s}", N=N, L=(L, L, Lz), xyz=_slab(rng, N, L, L, 0.5, Lz - 0.5),
+                        q=_pm_charges(N), alpha=0.1, r_cutoff=10.0, gamma_up=float(gu), gamma_down=float(gd),
+                        N_t=30, accuracy=1e-6, P=200, walls=[]))
+    return out
+
+
+def config5(seed=None, N=1_000_000):
+    """N=1e6 (+-1), Lx=Ly=3162, Lz=10, gamma_up=gamma_down=0.99, alpha=0.1, r_c=10, P=2000."""
+    rng = np.random.default_rng(SEED0 + 5 if seed is None else seed)
+    L = 3162.0 * np.sqrt(N / 1_000_000)
+    return dict(name=f"config5_N{N}_slab", N=N, L=(L, L, 10.0), xyz=_slab(rng, N, L, L, 0.5, 9.5),
+                q=_pm_charges(N), alpha=0.1, r_cutoff=10.0, gamma_up=0.99, gamma_down=0.99, N_t=30,
+                accuracy=1e-6, P=2000, walls=[])
+
+
+def engine_for(cfg, precision="fp64", mode_flags=0, seed=7, device=0):
+    """A libqem Engine configured for cfg, with a seeded k-set of cfg['P'] vectors."""
+    from . import _lib as L
+    from .api import Engine, Substrate_LJ
+
+    walls = [Substrate_LJ(**w) for w in cfg.get("walls", [])]
+    e = Engine(L_box=cfg["L"], alpha=cfg["alpha"], r_cutoff=cfg["r_cutoff"], gamma_1=cfg["gamma_down"],
+               gamma_2=cfg["gamma_up"], accuracy=cfg["accuracy"], N_t=cfg["N_t"], rbe_p=cfg["P"], walls=walls,
+               mode_flags=mode_flags, precision={"fp64": L.QEM_FP64, "fp32": L.QEM_FP32_FIX}[precision],
+               device=device)
+    e.sample_kset(seed, cfg["P"])
+    return e
+
+
+def rel_err(F, Fref):
+    """(||F - Fref||_2 / ||Fref||_2, max_i |F_i - Fref_i| / rms_i |Fref_i|) over all particles."""
+    d = np.asarray(F) - np.asarray(Fref)
+    nref = np.linalg.norm(Fref)
+    rms = nref / np.sqrt(max(len(Fref), 1))
+    return float(np.linalg.norm(d) / nref), float(np.max(np.linalg.norm(d, axis=1)) / rms)
