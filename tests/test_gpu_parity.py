@@ -132,7 +132,8 @@ def test_walls_vs_oracle():
     e = W.engine_for(cfg)
     F = e.forces(cfg["xyz"], cfg["q"], terms=L.QEM_TERM_LJ)
     Fref, bad = O.lj_two_walls(cfg["xyz"], cfg["walls"])
-    assert bad == 0 and np.allclose(F, Fref, rtol=1e-14, atol=1e-300)
+    # 2 s^12 - s^6 cancels near the LJ minimum: compare against the largest wall force
+    assert bad == 0 and np.allclose(F, Fref, rtol=1e-13, atol=1e-14 * np.abs(Fref).max())
 
 
 def test_config1_total_fp64():
@@ -282,7 +283,7 @@ def test_device_path_and_autograd():
     x = torch.tensor(cfg["xyz"], device="cuda", dtype=torch.float64, requires_grad=True)
     q = torch.tensor(cfg["q"], device="cuda", dtype=torch.float64)
     E, F = QEMEnergyForces.apply(x, q, e)
-    assert np.array_equal(F.cpu().numpy(), Fh) and float(E) == Eh
+    assert np.array_equal(F.cpu().numpy(), Fh) and float(E.detach()) == Eh
     E.backward()
     assert torch.equal(x.grad, -F)
 
