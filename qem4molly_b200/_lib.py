@@ -24,6 +24,7 @@ QEM_PYTHON_MODE = QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL
 QEM_FP64, QEM_FP32_FIX = 0, 1
 QEM_TERM_SHORT, QEM_TERM_LONG, QEM_TERM_LJ, QEM_TERM_ALL = 0x1, 0x2, 0x4, 0x7
 QEM_MEM_HOST, QEM_MEM_DEVICE = 0, 1
+QEM_NOALLOC_MAX_N, QEM_NOALLOC_MAX_P = 32768, 512
 
 
 class QemError(RuntimeError):
@@ -94,6 +95,7 @@ def load(build: bool = False):
         "qem_get_counts": (C.c_int32, [H, C.POINTER(C.c_int64), C.c_int32]),
         "qem_version": (C.c_char_p, []),
         "qem_measure_peaks": (C.c_int32, [C.c_int32, dp, dp]),
+        "qem_long_forces_noalloc": (C.c_int32, [PP, C.c_int32, vp, vp, C.c_int32, dp, C.c_double, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
