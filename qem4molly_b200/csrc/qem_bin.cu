@@ -172,22 +172,67 @@ __global__ void k_cell_scatter(int N, const int *__restrict__ cell, int *fill, i
     if (i < N) list[atomicAdd(&fill[cell[i]], 1)] = i;
 }
 
-// ascending particle index inside every cell (makes the slot order of the
-// atomic scatter irrelevant), and the inverse map particle -> sorted slot
-__global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__restrict__ list, int *__restrict__ pos_of)
+// ascending order of up to 32 values held one per lane (bitonic network)
+template <typename T>
+__device__ __forceinline__ T warp_sort32(T v, int lane)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    int b = start[c], e = start[c + 1];
-    for (int s = b + 1; s < e; s++) {
-        int v = list[s], t = s - 1;
-        while (t >= b && list[t] > v) {
-            list[t + 1] = list[t];
-            t--;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const T other = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool up = ((lane & size) == 0) || size == 32;
+            const bool lower = (lane & stride) == 0;
+            v = (lower == up) ? (other < v ? other : v) : (other > v ? other : v);
         }
-        list[t + 1] = v;
     }
-    for (int s = b; s < e; s++) pos_of[list[s]] = s;
+    return v;
+}
+
+// one warp per segment [b, e): ascending order (segments longer than 32 fall
+// back to an insertion sort by lane 0)
+template <typename T>
+__device__ __forceinline__ void warp_sort_segment(T *list, int64_t b, int64_t e, int lane, T pad)
+{
+    const int64_t n = e - b;
+    if (n <= 1) return;
+    if (n <= 32) {
+        T v = lane < n ? list[b + lane] : pad;
+        v = warp_sort32(v, lane);
+        if (lane < n) list[b + lane] = v;
+        return;
+    }
+    if (lane == 0) {
+        for (int64_t s = b + 1; s < e; s++) {
+            T v = list[s];
+            int64_t t = s - 1;
+            while (t >= b && list[t] > v) {
+                list[t + 1] = list[t];
+                t--;
+            }
+            list[t + 1] = v;
+        }
+    }
+    __syncwarp();
+}
+
+// ascending particle index inside every cell (makes the slot order of the
+// atomic scatter irrelevant), the inverse map particle -> sorted slot, and the
+// positions in cell order; one warp per cell
+__global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__restrict__ list, int *__restrict__ pos_of,
+                            const double4 *__restrict__ pos, double4 *__restrict__ pos_c)
+{
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= ncell) return;
+    const int b = start[c], e = start[c + 1];
+    warp_sort_segment<int>(list, b, e, lane, 0x7fffffff);
+    __syncwarp();
+    for (int s = b + lane; s < e; s += 32) {
+        const int i = list[s];
+        pos_of[i] = s;
+        pos_c[s] = pos[i];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -210,17 +255,28 @@ __device__ __forceinline__ void stencil_range(int n, int &lo, int &hi)
     else { lo = 0; hi = 0; }
 }
 
+// pos_c: positions in cell order (pos_c[s] is particle clist[s]).  Pairs are
+// stored as (owner, other) -- not ordered by index.  The fill pass writes at
+// most cap pairs (QEM_ST_OVERFLOW beyond) and counts each pair's incoming
+// entry for its second particle.
 template <bool FILL>
-__global__ void k_pairs(int N, const double4 *__restrict__ pos, const int *__restrict__ cell,
+__global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__restrict__ cell,
                         const int *__restrict__ cstart, const int *__restrict__ clist, CellGeom g, double rc2,
-                        int *__restrict__ pcount, const int64_t *__restrict__ poff, int2 *__restrict__ pairs)
+                        int *__restrict__ pcount, const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
+                        int64_t cap, int *__restrict__ in_cnt, unsigned *status)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= N) return;
     int i = clist[t];
-    double4 pi = pos[i];
+    double4 pi = pos_c[t];
     int c = cell[i];
     int cx = c / g.ncy, cy = c - cx * g.ncy;
+    // Ownership: with at least 3 cells per direction the pair belongs to the
+    // particle whose half stencil (own cell after it, plus the 4 forward
+    // cells) contains the other one, so every cell pair is visited once and
+    // incoming lists stay balanced; otherwise the full (deduplicated)
+    // stencil with "later in cell order" ownership.
+    const bool half = g.ncx >= 3 && g.ncy >= 3;
     int xlo, xhi, ylo, yhi;
     stencil_range(g.ncx, xlo, xhi);
     stencil_range(g.ncy, ylo, yhi);
@@ -230,15 +286,24 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos, const int *__res
         int nx = cx + ox;
         nx = nx < 0 ? nx + g.ncx : (nx >= g.ncx ? nx - g.ncx : nx);
         for (int oy = ylo; oy <= yhi; oy++) {
+            if (half && (ox < 0 || (ox == 0 && oy < 0))) continue;  // backward half of the stencil
             int ny = cy + oy;
             ny = ny < 0 ? ny + g.ncy : (ny >= g.ncy ? ny - g.ncy : ny);
             int cc = nx * g.ncy + ny;
+            const bool same = (cc == c);
             int b = cstart[cc], e = cstart[cc + 1];
             for (int s = b; s < e; s++) {
+                if ((same || !half) && s <= t) continue;
                 int j = clist[s];
-                if (j <= i) continue;
-                if (rho2_exact(pi, pos[j], g) <= rc2) {
-                    if (FILL) pairs[o + cnt] = make_int2(i, j);
+                if (rho2_exact(pi, pos_c[s], g) <= rc2) {
+                    if (FILL) {
+                        if (o + cnt < cap) {
+                            pairs[o + cnt] = make_int2(i, j);
+                            atomicAdd(&in_cnt[j], 1);
+                        } else {
+                            atomicOr(status, QEM_ST_OVERFLOW);
+                        }
+                    }
                     cnt++;
                 }
             }
@@ -250,34 +315,24 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos, const int *__res
 // ---------------------------------------------------------------------------
 // incoming pairs per particle (CSR over the second index), sorted by pair id
 // ---------------------------------------------------------------------------
-__global__ void k_in_count(int64_t Np, const int2 *__restrict__ pairs, int *cnt)
+// the pair count lives on the device (*np = poff[N]); grids are sized for
+// the capacity and threads beyond the count return
+__global__ void k_in_fill(const int64_t *__restrict__ np, int64_t cap, const int2 *__restrict__ pairs,
+                          const int64_t *__restrict__ off, int *fill, int64_t *__restrict__ list)
 {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < Np) atomicAdd(&cnt[pairs[p].y], 1);
-}
-
-__global__ void k_in_fill(int64_t Np, const int2 *__restrict__ pairs, const int64_t *__restrict__ off, int *fill,
-                          int64_t *__restrict__ list)
-{
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= Np) return;
-    int j = pairs[p].y;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= *np || p >= cap) return;
+    const int j = pairs[p].y;
     list[off[j] + atomicAdd(&fill[j], 1)] = p;
 }
 
+// incoming lists in ascending pair order; one warp per particle
 __global__ void k_in_sort(int N, const int64_t *__restrict__ off, int64_t *__restrict__ list)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (i >= N) return;
-    int64_t b = off[i], e = off[i + 1];
-    for (int64_t s = b + 1; s < e; s++) {
-        int64_t v = list[s], t = s - 1;
-        while (t >= b && list[t] > v) {
-            list[t + 1] = list[t];
-            t--;
-        }
-        list[t + 1] = v;
-    }
+    warp_sort_segment<long long>((long long *)list, off[i], off[i + 1], lane, 0x7fffffffffffffffLL);
 }
 
 // ---------------------------------------------------------------------------
@@ -412,8 +467,9 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
     return cudaGetLastError();
 }
 
-cudaError_t qem_launch_cells(int N, int ncell, const int *cell, int *cell_cnt, int *cell_start, int *cell_fill,
-                             int *cell_list, int *pos_of, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
+cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *pos, int *cell_cnt, int *cell_start,
+                             int *cell_fill, int *cell_list, int *pos_of, double4 *pos_c, void *scan_tmp,
+                             size_t scan_tmp_bytes, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(cell_cnt, 0, sizeof(int) * ncell, s);
     if (e != cudaSuccess) return e;
@@ -423,38 +479,37 @@ cudaError_t qem_launch_cells(int N, int ncell, const int *cell, int *cell_cnt, i
     e = cudaMemcpyAsync(cell_fill, cell_start, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return e;
     k_cell_scatter<<<nblk(N, 256), 256, 0, s>>>(N, cell, cell_fill, cell_list);
-    k_cell_sort<<<nblk(ncell, 128), 128, 0, s>>>(ncell, cell_start, cell_list, pos_of);
+    k_cell_sort<<<nblk((int64_t)ncell * 32, 256), 256, 0, s>>>(ncell, cell_start, cell_list, pos_of, pos, pos_c);
     return cudaGetLastError();
 }
 
-cudaError_t qem_launch_pair_count(int N, const double4 *pos, const int *cell, const int *cell_start,
+cudaError_t qem_launch_pair_count(int N, const double4 *pos_c, const int *cell, const int *cell_start,
                                   const int *cell_list, CellGeom g, double rc2, int *pcount, cudaStream_t s)
 {
-    k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
-                                                 nullptr);
+    k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
+                                                 nullptr, 0, nullptr, nullptr);
     return cudaGetLastError();
 }
 
-cudaError_t qem_launch_pair_fill(int N, const double4 *pos, const int *cell, const int *cell_start,
+cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, const int *cell_start,
                                  const int *cell_list, CellGeom g, double rc2, const int64_t *poff, int2 *pairs,
-                                 cudaStream_t s)
+                                 int64_t cap, int *in_cnt, unsigned *status, cudaStream_t s)
 {
-    k_pairs<true><<<nblk(N, 128), 128, 0, s>>>(N, pos, cell, cell_start, cell_list, g, rc2, nullptr, poff, pairs);
+    k_pairs<true><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, nullptr, poff, pairs,
+                                                cap, in_cnt, status);
     return cudaGetLastError();
 }
 
-cudaError_t qem_launch_incoming(int N, int64_t Np, const int2 *pairs, int *in_cnt, int64_t *in_off, int *in_fill,
-                                int64_t *in_list, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
+cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
+                                int64_t *in_off, int *in_fill, int64_t *in_list, void *scan_tmp,
+                                size_t scan_tmp_bytes, cudaStream_t s)
 {
-    cudaError_t e = cudaMemsetAsync(in_cnt, 0, sizeof(int) * N, s);
+    cudaError_t e = cudaMemsetAsync(in_fill, 0, sizeof(int) * N, s);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(in_fill, 0, sizeof(int) * N, s);
-    if (e != cudaSuccess) return e;
-    if (Np > 0) k_in_count<<<nblk(Np, 256), 256, 0, s>>>(Np, pairs, in_cnt);
     e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s);
     if (e != cudaSuccess) return e;
-    if (Np > 0) k_in_fill<<<nblk(Np, 256), 256, 0, s>>>(Np, pairs, in_off, in_fill, in_list);
-    k_in_sort<<<nblk(N, 128), 128, 0, s>>>(N, in_off, in_list);
+    if (cap > 0) k_in_fill<<<nblk(cap, 256), 256, 0, s>>>(np, cap, pairs, in_off, in_fill, in_list);
+    k_in_sort<<<nblk((int64_t)N * 32, 256), 256, 0, s>>>(N, in_off, in_list);
     return cudaGetLastError();
 }
 

@@ -136,7 +136,11 @@ struct qem_handle {
     DevBuf xyz, q, F, pos, cell, cell_cnt, cell_start, cell_fill, cell_list, pos_of, pcount, poff, pairs, R, Upair,
         in_cnt, in_off, in_fill, in_list, scan_tmp;
     DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, tot, off, Utot, Epart, status,
-        Eout;
+        Eout, Fpart, pos_c;
+    int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
+    DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
+    cudaStream_t s2 = nullptr;  // side stream of the long range
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     unsigned *h_status = nullptr;
     double *h_E = nullptr;
     int64_t *h_np = nullptr;
@@ -305,10 +309,14 @@ static void sample_kset(qem_handle *h, int P)
 // ---------------------------------------------------------------------------
 // one evaluation
 // ---------------------------------------------------------------------------
-static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
-                      uint32_t terms, int mem, cudaStream_t s)
+// retry = true asks the caller to evaluate again (the pair list outgrew its
+// capacity, which has been enlarged).
+static qem_status run_once(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
+                           uint32_t terms, int mem, cudaStream_t s, bool &retry)
 {
+    retry = false;
     if (!h) return QEM_ERR_ARG;
+    const int64_t short_calls0 = h->short_calls;
     if (N < 0) return fail(h, QEM_ERR_ARG, "N < 0");
     if (terms & ~QEM_TERM_ALL) return fail(h, QEM_ERR_ARG, "unknown term bit");
     if (mem != QEM_MEM_HOST && mem != QEM_MEM_DEVICE) return fail(h, QEM_ERR_ARG, "mem must be HOST or DEVICE");
@@ -349,71 +357,23 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
     CU(qem_launch_pack(N, xyz_d, q_d, ptr<double4>(h->pos), ptr<int>(h->cell), h->geom, st, s));
     launches++;
 
-    // energy partials: [short blocks | long chunks | k0 blocks | P split terms]
+    // energy partials: [short blocks | ks x long chunks | k0 blocks | P split terms]
     const int LCH = qem_long_chunk();
     const int nbS = (N + 255) / 256, nch = (N + LCH - 1) / LCH, nb0 = (N + 255) / 256;
+    const int ks = qem_long_ksplit(nch, 1 << 30, 8);
     const int P = do_long ? (h->has_kset ? h->P : 0) : 0;
-    CU(grow(h->Epart, sizeof(double) * (size_t)(nbS + nch + nb0 + std::max(P, h->p.rbe_p) + 8)));
+    const size_t nEpart = (size_t)nbS + (size_t)ks * nch + nb0 + std::max(P, h->p.rbe_p) + 8;
+    CU(grow(h->Epart, sizeof(double) * nEpart));
     double *Ep = ptr<double>(h->Epart);
-    if (want_E) CU(cudaMemsetAsync(Ep, 0, sizeof(double) * (size_t)(nbS + nch + nb0 + std::max(P, h->p.rbe_p) + 8), s));
+    if (want_E) CU(cudaMemsetAsync(Ep, 0, sizeof(double) * nEpart, s));
     CU(grow(h->scan_tmp, qem_scan_tmp_bytes(std::max(std::max(N, h->ncell), 1)) + 64));
 
-    int mk_bin = -1, mk_pair = -1, mk_gather = -1;
-    if (do_short) {
-        const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
-        const bool rebuild = !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
-        if (rebuild) {
-            CU(grow(h->cell_cnt, sizeof(int) * h->ncell));
-            CU(grow(h->cell_start, sizeof(int) * (h->ncell + 1)));
-            CU(grow(h->cell_fill, sizeof(int) * h->ncell));
-            CU(grow(h->cell_list, sizeof(int) * N));
-            CU(grow(h->pos_of, sizeof(int) * N));
-            CU(grow(h->pcount, sizeof(int) * N));
-            CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
-            CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<int>(h->cell_cnt), ptr<int>(h->cell_start),
-                                ptr<int>(h->cell_fill), ptr<int>(h->cell_list), ptr<int>(h->pos_of), h->scan_tmp.p,
-                                h->scan_tmp.cap, s));
-            CU(qem_launch_pair_count(N, ptr<double4>(h->pos), ptr<int>(h->cell), ptr<int>(h->cell_start),
-                                     ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), s));
-            CU(qem_scan_i32_to_i64(ptr<int>(h->pcount), ptr<int64_t>(h->poff), N, h->scan_tmp.p, h->scan_tmp.cap, s));
-            CU(cudaMemcpyAsync(h->h_np, ptr<int64_t>(h->poff) + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-            CU(cudaStreamSynchronize(s));
-            const int64_t Np = *h->h_np;
-            CU(grow(h->pairs, sizeof(int2) * std::max<int64_t>(Np, 1)));
-            CU(grow(h->R, sizeof(double4) * std::max<int64_t>(Np, 1)));
-            CU(grow(h->Upair, sizeof(double) * std::max<int64_t>(Np, 1)));
-            CU(grow(h->in_cnt, sizeof(int) * N));
-            CU(grow(h->in_fill, sizeof(int) * N));
-            CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
-            CU(grow(h->in_list, sizeof(int64_t) * std::max<int64_t>(Np, 1)));
-            CU(qem_launch_pair_fill(N, ptr<double4>(h->pos), ptr<int>(h->cell), ptr<int>(h->cell_start),
-                                    ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
-                                    ptr<int2>(h->pairs), s));
-            CU(qem_launch_incoming(N, Np, ptr<int2>(h->pairs), ptr<int>(h->in_cnt), ptr<int64_t>(h->in_off),
-                                   ptr<int>(h->in_fill), ptr<int64_t>(h->in_list), h->scan_tmp.p, h->scan_tmp.cap, s));
-            launches += 16;
-            h->Np = Np;
-            h->pairs_N = N;
-            h->pairs_valid = true;
-        }
-        h->short_calls++;
-        mk_bin = h->prof.mark(s);
-        CU(qem_launch_short_pairs(prec, want_E, h->Np, ptr<int2>(h->pairs), ptr<double4>(h->pos), ptr<double4>(h->R),
-                                  ptr<double>(h->Upair), h->sc, s));
-        launches += h->Np > 0;
-        mk_pair = h->prof.mark(s);
-    }
-    if (do_short || do_lj) {
-        CU(qem_launch_short_gather(prec, want_E, do_short, do_lj, N, ptr<double4>(h->pos), ptr<int>(h->pos_of),
-                                   ptr<int64_t>(h->poff), ptr<double4>(h->R), ptr<double>(h->Upair),
-                                   ptr<int64_t>(h->in_off), ptr<int64_t>(h->in_list), h->sc, F_d, Ep, st, s));
-        launches++;
-    } else {
-        CU(cudaMemsetAsync(F_d, 0, sizeof(double) * 3 * N, s));
-    }
-    mk_gather = h->prof.mark(s);
-
-    int mk_lprep = -1, mk_lforce = -1;
+    // Long range first, on the side stream when short-range / wall work runs
+    // too: the two pipelines are independent until their forces are summed.
+    const bool concurrent = do_long && (do_short || do_lj);
+    cudaStream_t sl = concurrent ? h->s2 : s;
+    int mk_lstart = -1, mk_lprep = -1, mk_lforce = -1;
+    h->counts[2] = 0;
     if (do_long) {
         if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
         else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
@@ -421,10 +381,6 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
         if (prec == QEM_FP32_FIX && Pk > 0 && h->kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
         CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
-        if (h->kset_dirty && Pk > 0) {
-            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
-            h->kset_dirty = false;
-        }
         CU(grow(h->zperm, sizeof(int) * N));
         CU(grow(h->ztmp, sizeof(int) * N));
         CU(grow(h->zkey, sizeof(double) * N));
@@ -440,9 +396,23 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
         CU(grow(h->kc, sizeof(KConst) * std::max(Pk, 1)));
         CU(grow(h->tot, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
         CU(grow(h->off, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
+        CU(grow(h->Fpart, sizeof(double) * 3 * (size_t)ks * N));
         CU(grow(h->Utot, sizeof(double) * 4 * std::max(Pk, 1)));
+        CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
+        CU(grow(h->Flong, sizeof(double) * 3 * N));
+        if (concurrent) {  // fork after pack (positions) and the energy-partial clear
+            CU(cudaEventRecord(h->ev_fork, s));
+            CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
+        }
+        mk_lstart = h->prof.mark(sl);
+        if (h->kset_dirty && Pk > 0) {
+            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, sl));
+            h->kset_dirty = false;
+        }
+        double *FL = concurrent ? ptr<double>(h->Flong) : F_d;
+        CU(cudaMemsetAsync(FL, 0, sizeof(double) * 3 * N, sl));
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
-                            ptr<double>(h->zkey2), s));
+                            ptr<double>(h->zkey2), sl));
         LongBuffers b;
         b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
         b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
@@ -451,35 +421,116 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
         b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
         b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
         b.Epart = Ep + nbS;
-        b.Eks = Ep + nbS + nch + nb0;
-        b.stmp = h->scan_tmp.p; b.stmp_bytes = h->scan_tmp.cap;
+        b.Eks = Ep + nbS + (size_t)ks * nch + nb0;
+        b.Fpart = ptr<double>(h->Fpart);
+        b.ks = ks;
+        b.stmp = h->scan_tmp2.p; b.stmp_bytes = h->scan_tmp2.cap;
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
-                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, F_d, nch, st, s, 0));
-        mk_lprep = h->prof.mark(s);
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, FL, nch, st, sl, 0));
+        mk_lprep = h->prof.mark(sl);
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
-                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, F_d, nch, st, s, 1));
-        mk_lforce = h->prof.mark(s);
-        launches += 8;
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, FL, nch, st, sl, 1));
+        mk_lforce = h->prof.mark(sl);
+        launches += 22;
         h->counts[2] = Pk;
-    } else {
-        h->counts[2] = 0;
+    }
+
+    int mk_bin = -1, mk_pair = -1, mk_gather = -1;
+    if (do_short) {
+        const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
+        const bool rebuild = !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
+        if (rebuild) {
+            CU(grow(h->cell_cnt, sizeof(int) * h->ncell));
+            CU(grow(h->cell_start, sizeof(int) * (h->ncell + 1)));
+            CU(grow(h->cell_fill, sizeof(int) * h->ncell));
+            CU(grow(h->cell_list, sizeof(int) * N));
+            CU(grow(h->pos_of, sizeof(int) * N));
+            CU(grow(h->pcount, sizeof(int) * N));
+            CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
+            CU(grow(h->pos_c, sizeof(double4) * N));
+            // pair capacity: last count + 25 %, first time from the mean density; the
+            // count stays on the device (no host round trip inside the call)
+            if (h->pair_cap <= 0) {
+                const double dens = (double)N / (h->p.Lx * h->p.Ly);
+                h->pair_cap = (int64_t)(1.3 * 0.5 * N * QEM_PI * h->p.r_cutoff * h->p.r_cutoff * dens) + 4096;
+            }
+            const int64_t cap = h->pair_cap;
+            CU(grow(h->pairs, sizeof(int2) * cap));
+            CU(grow(h->R, sizeof(double4) * cap));
+            CU(grow(h->Upair, sizeof(double) * cap));
+            CU(grow(h->in_cnt, sizeof(int) * N));
+            CU(grow(h->in_fill, sizeof(int) * N));
+            CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
+            CU(grow(h->in_list, sizeof(int64_t) * cap));
+            CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<double4>(h->pos), ptr<int>(h->cell_cnt),
+                                ptr<int>(h->cell_start), ptr<int>(h->cell_fill), ptr<int>(h->cell_list),
+                                ptr<int>(h->pos_of), ptr<double4>(h->pos_c), h->scan_tmp.p, h->scan_tmp.cap, s));
+            CU(qem_launch_pair_count(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                                     ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), s));
+            CU(qem_scan_i32_to_i64(ptr<int>(h->pcount), ptr<int64_t>(h->poff), N, h->scan_tmp.p, h->scan_tmp.cap, s));
+            CU(cudaMemsetAsync(h->in_cnt.p, 0, sizeof(int) * N, s));
+            CU(qem_launch_pair_fill(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                                    ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
+                                    ptr<int2>(h->pairs), cap, ptr<int>(h->in_cnt), st, s));
+            CU(qem_launch_incoming(N, ptr<int64_t>(h->poff) + N, cap, ptr<int2>(h->pairs), ptr<int>(h->in_cnt),
+                                   ptr<int64_t>(h->in_off), ptr<int>(h->in_fill), ptr<int64_t>(h->in_list),
+                                   h->scan_tmp.p, h->scan_tmp.cap, s));
+            launches += 16;
+            h->pairs_N = N;
+            h->pairs_valid = true;
+        }
+        h->short_calls++;
+        mk_bin = h->prof.mark(s);
+        CU(qem_launch_short_pairs(prec, want_E, ptr<int64_t>(h->poff) + N, h->pair_cap, ptr<int2>(h->pairs),
+                                  ptr<double4>(h->pos), ptr<double4>(h->R), ptr<double>(h->Upair), h->sc, s));
+        launches++;
+        mk_pair = h->prof.mark(s);
+    }
+    if (do_short || do_lj) {
+        CU(qem_launch_short_gather(prec, want_E, do_short, do_lj, N, ptr<double4>(h->pos), ptr<int>(h->pos_of),
+                                   ptr<int64_t>(h->poff), ptr<double4>(h->R), ptr<double>(h->Upair),
+                                   ptr<int64_t>(h->in_off), ptr<int64_t>(h->in_list), h->pair_cap, h->sc, F_d, Ep,
+                                   st, s));
+        launches++;
+    } else if (!do_long) {  // (a long-only call has already zeroed F_d in front of its kernels)
+        CU(cudaMemsetAsync(F_d, 0, sizeof(double) * 3 * N, s));
+    }
+    mk_gather = h->prof.mark(s);
+    if (concurrent) {  // join: the long range ran on the side stream into Flong
+        CU(cudaEventRecord(h->ev_join, h->s2));
+        CU(cudaStreamWaitEvent(s, h->ev_join, 0));
+        CU(qem_launch_add3(3 * N, ptr<double>(h->Flong), F_d, s));
+        launches++;
     }
     if (want_E) {
-        const int nE = nbS + nch + nb0 + (do_long ? (h->has_kset ? h->P : 0) : 0);
+        const int nE = nbS + ks * nch + nb0 + (do_long ? (h->has_kset ? h->P : 0) : 0);
         CU(qem_launch_reduce_sum(Ep, nE, ptr<double>(h->Eout), s));
         launches++;
         CU(cudaMemcpyAsync(h->h_E, h->Eout.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
     if (mem == QEM_MEM_HOST) CU(cudaMemcpyAsync(F, F_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (do_short)
+        CU(cudaMemcpyAsync(h->h_np, ptr<int64_t>(h->poff) + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     const int mk_end = h->prof.mark(s);
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
+    if (do_short) {
+        h->Np = *h->h_np;
+        if (*h->h_status & QEM_ST_OVERFLOW) {  // pair capacity too small: grow and evaluate again
+            h->pair_cap = h->Np + h->Np / 4 + 4096;
+            h->pairs_valid = false;
+            h->short_calls = short_calls0;
+            retry = true;
+            return QEM_OK;
+        }
+        if (h->Np > h->pair_cap - h->pair_cap / 8) h->pair_cap = h->Np + h->Np / 4 + 4096;  // for the next build
+    }
     h->prof.span("upload", mk0, mk_in);
     h->prof.span("bin_pairs", mk_in, mk_bin);
     h->prof.span("short_pair", mk_bin, mk_pair);
     h->prof.span("short_gather", mk_pair >= 0 ? mk_pair : mk_in, mk_gather);
-    h->prof.span("long_prep", mk_gather, mk_lprep);
+    h->prof.span("long_prep", mk_lstart, mk_lprep);
     h->prof.span("long_force", mk_lprep, mk_lforce);
     h->prof.span("total", mk0, mk_end);
     if (h->prof.on) h->prof.finish();
@@ -492,6 +543,16 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
     if (want_E) *energy = *h->h_E;
     h->err.clear();
     return QEM_OK;
+}
+
+static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
+                      uint32_t terms, int mem, cudaStream_t s)
+{
+    bool retry = false;
+    qem_status st = run_once(h, N, xyz, q, F, energy, terms, mem, s, retry);
+    if (st == QEM_OK && retry) st = run_once(h, N, xyz, q, F, energy, terms, mem, s, retry);
+    if (st == QEM_OK && retry) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list grew past its capacity twice");
+    return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -542,7 +603,10 @@ qem_status qem_create(const qem_params *p, qem_handle **out)
     build_consts(h);
     if (cudaMallocHost(&h->h_status, sizeof(unsigned)) != cudaSuccess ||
         cudaMallocHost(&h->h_E, sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&h->h_np, sizeof(int64_t)) != cudaSuccess) {
+        cudaMallocHost(&h->h_np, sizeof(int64_t)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         qem_destroy(h);
         return QEM_ERR_CUDA;
     }
@@ -558,10 +622,17 @@ void qem_destroy(qem_handle *h)
                       &h->cell_list, &h->pos_of, &h->pcount, &h->poff, &h->pairs, &h->R, &h->Upair, &h->in_cnt,
                       &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
                       &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin,
-                      &h->tot, &h->off, &h->Utot, &h->Epart, &h->status, &h->Eout};
+                      &h->tot, &h->off, &h->Utot, &h->Epart, &h->status, &h->Eout, &h->Fpart,
+                      &h->pos_c, &h->scan_tmp2, &h->Flong};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
+    if (h->s2) {
+        cudaStreamSynchronize(h->s2);
+        cudaStreamDestroy(h->s2);
+    }
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->h_status) cudaFreeHost(h->h_status);
     if (h->h_E) cudaFreeHost(h->h_E);
     if (h->h_np) cudaFreeHost(h->h_np);
@@ -688,6 +759,8 @@ qem_status qem_pair_list(qem_handle *h, int32_t N, const double *xyz, int32_t *p
     if (pairs && cap > 0 && h->Np > 0) {
         const int64_t n = std::min(cap, h->Np);
         CU(cudaMemcpy(pairs, h->pairs.p, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+        for (int64_t t = 0; t < n; t++)  // stored as (owner, other): report (i, j) with i < j
+            if (pairs[2 * t] > pairs[2 * t + 1]) std::swap(pairs[2 * t], pairs[2 * t + 1]);
     }
     return QEM_OK;
 }

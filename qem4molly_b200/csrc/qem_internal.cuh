@@ -58,24 +58,33 @@ struct KConst {
 // ---------------------------------------------------------------------------
 cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *pos, int *cell, CellGeom g,
                             unsigned *status, cudaStream_t s);
-cudaError_t qem_launch_cells(int N, int ncell, const int *cell, int *cell_cnt, int *cell_start, int *cell_fill,
-                             int *cell_list, int *pos_of, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s);
-cudaError_t qem_launch_pair_count(int N, const double4 *pos, const int *cell, const int *cell_start,
+// cells: counting sort by cell, ascending index inside a cell, pos_of and the
+// positions in cell order (pos_c)
+cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *pos, int *cell_cnt, int *cell_start,
+                             int *cell_fill, int *cell_list, int *pos_of, double4 *pos_c, void *scan_tmp,
+                             size_t scan_tmp_bytes, cudaStream_t s);
+cudaError_t qem_launch_pair_count(int N, const double4 *pos_c, const int *cell, const int *cell_start,
                                   const int *cell_list, CellGeom g, double rc2, int *pcount, cudaStream_t s);
-cudaError_t qem_launch_pair_fill(int N, const double4 *pos, const int *cell, const int *cell_start,
+// fills at most cap pairs (QEM_ST_OVERFLOW beyond) and counts incoming pairs
+// per particle into in_cnt (zeroed by the caller)
+cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, const int *cell_start,
                                  const int *cell_list, CellGeom g, double rc2, const int64_t *poff, int2 *pairs,
-                                 cudaStream_t s);
-cudaError_t qem_launch_incoming(int N, int64_t Np, const int2 *pairs, int *in_cnt, int64_t *in_off, int *in_fill,
-                                int64_t *in_list, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s);
+                                 int64_t cap, int *in_cnt, unsigned *status, cudaStream_t s);
+// np: device pointer to the pair count (poff[N])
+cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
+                                int64_t *in_off, int *in_fill, int64_t *in_list, void *scan_tmp,
+                                size_t scan_tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
 
-cudaError_t qem_launch_short_pairs(int precision, bool energy, int64_t Np, const int2 *pairs, const double4 *pos,
-                                   double4 *R, double *Upair, const ShortConsts &c, cudaStream_t s);
+// np: device pointer to the pair count; cap: capacity of pairs / R / Upair
+cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np, int64_t cap, const int2 *pairs,
+                                   const double4 *pos, double4 *R, double *Upair, const ShortConsts &c,
+                                   cudaStream_t s);
 cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, bool do_lj, int N,
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
-                                    const double *Upair, const int64_t *in_off, const int64_t *in_list,
+                                    const double *Upair, const int64_t *in_off, const int64_t *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s);
 
@@ -95,19 +104,24 @@ struct LongBuffers {
     double *off;          // P x nch x 4 chunk offsets (u from below, v from above)
     double *Utot;         // P x 4 global totals
     double *Eks;          // P per-k split energy term
-    double *Epart;        // per-block energy partials
+    double *Epart;        // per-block energy partials (ks * nch + nb0 entries)
+    double *Fpart;        // ks x N x 3 per-k-slice force partials (z order)
+    int ks;               // number of k slices of the force pass
     void *stmp;           // scan scratch
     size_t stmp_bytes;
 };
+// number of k slices for nch chunks and P k-vectors (at most max_ks)
+int qem_long_ksplit(int nch, int P, int max_ks);
 // stage 0: z-ordered gather, k = 0 term, per-k constants, chunk totals and
-// their scan; stage 1: the per-chunk force pass (adds into F3).
+// their scan; stage 1: the k-sliced force pass, added into F3.
 cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const double4 *pos, const int *zperm,
                             const LongBuffers &b, double Lx, double Ly, double Lz, double g1, double g2, double eps0,
                             double sum_K, double *F3, int nch, unsigned *status, cudaStream_t s, int stage);
 int qem_long_chunk(void);
 
-cudaError_t qem_launch_add3(int N, const double *a, double *out, cudaStream_t s);
 cudaError_t qem_launch_reduce_sum(const double *in, int n, double *out, cudaStream_t s);
+// out[i] += a[i] for n doubles
+cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // device helpers

@@ -10,18 +10,20 @@
 //   energies      src/python_lib/Energy_long_range_njit.py:10-44,
 //                 src/python_lib/Sigma_Gamma_func_njit.py:8-69
 //
-// Layout: particles in z order (stable sortperm), SoA, chunks of LCH
-// consecutive particles.  Three passes per call:
+// Layout: particles in z order (stable sortperm), SoA, chunks of LCH = 512
+// consecutive particles; a thread owns PPT = 4 consecutive particles.
 //   1. k_ltot   grid (chunk, k-group): per (k, chunk) sums of
 //               u = q e^{k(z-h)} e^{i k.rho} and v = q e^{-k(z-h)} e^{i k.rho}
 //               (h = L_z / 2 keeps both exponentials inside FP32 range).
-//   2. k_lscan  one thread per k: FP64 exclusive scan of the chunk totals,
+//   2. k_lscan  one warp per k: FP64 exclusive scan of the chunk totals,
 //               forward for u (particles below) and backward for v (above).
-//   3. k_lforce one block per chunk, loop over all k: block exclusive scans
-//               (warp shuffles) give each particle its prefix / suffix sums,
-//               the Fl_non_sort + Fl_sort + Flz_self terms are formed in
-//               registers and accumulated over k (Kahan in FP32); one write
-//               per particle, no atomics.
+//   3. k_lforce grid (chunk, k-slice): per k, serial scans over the thread's
+//               4 particles, one warp shuffle scan of the thread totals and a
+//               4-warp prefix give every particle its prefix (A, B) and suffix
+//               (C, D) sums; Fl_non_sort + Fl_sort + Flz_self are formed in
+//               registers and summed over the slice's k in FP64.
+//   4. k_lfinal per particle: sum of the k-slices + the k = 0 term, added to F
+//               in the original particle order (fixed order: deterministic).
 // The suffix sums C, D are summed directly from above instead of the
 // reference's "total minus running sum" (Force_long.jl:97-98), which is the
 // same quantity without the cancellation that makes it useless in FP32.
@@ -31,8 +33,11 @@
 
 namespace {
 
-constexpr int LCH = 256;  // particles per chunk (= threads per block)
-constexpr int KPB = 16;   // k-vectors per block in the totals pass
+constexpr int LT = 128;         // threads per block
+constexpr int PPT = 4;          // particles per thread
+constexpr int LCH = LT * PPT;   // particles per chunk
+constexpr int NW = LT / 32;     // warps per block
+constexpr int KPB = 16;         // k-vectors per block in the totals pass
 
 template <typename Real>
 struct LM;
@@ -60,7 +65,7 @@ __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restri
     K.kx_2pi = kx / (2.0 * QEM_PI);
     K.ky_2pi = ky / (2.0 * QEM_PI);
     K.k = k;
-    K.W = exp(-0.5 * k * Lz);  // stored as sqrt(exp(-k L_z)); squared on use
+    K.W = exp(-0.5 * k * Lz);  // sqrt(exp(-k L_z)); squared on use
     K.g = 0.5 / (g12 * exp(-2.0 * k * Lz) - 1.0);
     K.fx = kx / k;
     K.fy = ky / k;
@@ -69,8 +74,7 @@ __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restri
     kc[m] = K;
 }
 
-// z-ordered SoA copy of the particles and the k = 0 term (Force_long.jl:130-161,
-// Energy_long_range_njit.py:25-44)
+// z-ordered SoA copy of the particles
 __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__restrict__ zperm, double h,
                           double *__restrict__ zx, double *__restrict__ zy, float *__restrict__ zhf,
                           double *__restrict__ zhd, float *__restrict__ qf, double *__restrict__ qd)
@@ -86,6 +90,7 @@ __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__r
     qf[m] = (float)p.w;
 }
 
+// k = 0 term (Force_long.jl:130-161, Energy_long_range_njit.py:25-44)
 __global__ void k_k0(int N, const double *__restrict__ qd, const double *__restrict__ zhd, double h,
                      const double *__restrict__ qscan, double fscale, double escale, double *__restrict__ k0,
                      double *__restrict__ Epart, int energy)
@@ -112,29 +117,51 @@ __global__ void k_k0(int N, const double *__restrict__ qd, const double *__restr
     }
 }
 
+// a thread's PPT particles in z order
 template <typename Real>
-__global__ void __launch_bounds__(LCH) k_ltot(int N, int P, int nch, const double *__restrict__ zx,
-                                               const double *__restrict__ zy, const Real *__restrict__ zh,
-                                               const Real *__restrict__ qv, const KConst *__restrict__ kc,
-                                               double *__restrict__ tot)
+struct Quad4 {
+    double x[PPT], y[PPT];
+    Real z[PPT], q[PPT];
+    __device__ __forceinline__ void load(int N, int m0, const double *zx, const double *zy, const Real *zh,
+                                         const Real *qv)
+    {
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const int m = m0 + j;
+            const bool ok = m < N;
+            x[j] = ok ? zx[m] : 0.0;
+            y[j] = ok ? zy[m] : 0.0;
+            z[j] = ok ? zh[m] : (Real)0;
+            q[j] = ok ? qv[m] : (Real)0;  // q = 0 makes padding particles contribute nothing
+        }
+    }
+};
+
+template <typename Real>
+__global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double *__restrict__ zx,
+                                             const double *__restrict__ zy, const Real *__restrict__ zh,
+                                             const Real *__restrict__ qv, const KConst *__restrict__ kc,
+                                             double *__restrict__ tot)
 {
-    __shared__ Real red[4][LCH / 32];
-    const int m = blockIdx.x * LCH + threadIdx.x;
-    const bool valid = m < N;
-    const double x = valid ? zx[m] : 0.0, y = valid ? zy[m] : 0.0;
-    const Real z = valid ? zh[m] : (Real)0, q = valid ? qv[m] : (Real)0;
+    __shared__ Real red[4][NW];
+    Quad4<Real> P4;
+    P4.load(N, blockIdx.x * LCH + threadIdx.x * PPT, zx, zy, zh, qv);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int kk = 0; kk < KPB; kk++) {
         const int kidx = blockIdx.y * KPB + kk;
         if (kidx >= P) break;
         const KConst K = kc[kidx];
-        double t = fma(K.kx_2pi, x, K.ky_2pi * y);
-        t -= rint(t);
-        Real s, c;
-        LM<Real>::sc(t, s, c);
-        const Real kz = (Real)K.k * z;
-        const Real ep = q * LM<Real>::ex(kz), em = q * LM<Real>::ex(-kz);
-        Real v[4] = {ep * c, ep * s, em * c, em * s};
+        Real v[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
+            t -= rint(t);
+            Real s, c;
+            LM<Real>::sc(t, s, c);
+            const Real kz = (Real)K.k * P4.z[j];
+            const Real ep = P4.q[j] * LM<Real>::ex(kz), em = P4.q[j] * LM<Real>::ex(-kz);
+            v[0] += ep * c; v[1] += ep * s; v[2] += em * c; v[3] += em * s;
+        }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
 #pragma unroll
@@ -147,151 +174,177 @@ __global__ void __launch_bounds__(LCH) k_ltot(int N, int P, int nch, const doubl
         __syncthreads();
         if (threadIdx.x < 4) {
             double sum = 0;
-            for (int ww = 0; ww < LCH / 32; ww++) sum += (double)red[threadIdx.x][ww];
+#pragma unroll
+            for (int ww = 0; ww < NW; ww++) sum += (double)red[threadIdx.x][ww];
             tot[((int64_t)kidx * nch + blockIdx.x) * 4 + threadIdx.x] = sum;
         }
         __syncthreads();
     }
 }
 
+// one warp per k: exclusive scans of the chunk totals (FP64)
 __global__ void k_lscan(int P, int nch, const double *__restrict__ tot, double *__restrict__ off,
                         double *__restrict__ Utot, const KConst *__restrict__ kc, double g1, double g2,
                         double *__restrict__ Eks)
 {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (m >= P) return;
     const double *T = tot + (int64_t)m * nch * 4;
     double *O = off + (int64_t)m * nch * 4;
-    double ur = 0, ui = 0;
-    for (int c = 0; c < nch; c++) {
-        O[4 * c] = ur;
-        O[4 * c + 1] = ui;
-        ur += T[4 * c];
-        ui += T[4 * c + 1];
+    double cr = 0, ci = 0;  // forward carry: u below
+    for (int base = 0; base < nch; base += 32) {
+        const int c = base + lane;
+        double r = c < nch ? T[4 * c] : 0.0, i = c < nch ? T[4 * c + 1] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double a = __shfl_up_sync(0xffffffffu, r, d), b = __shfl_up_sync(0xffffffffu, i, d);
+            if (lane >= d) { r += a; i += b; }
+        }
+        double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
+        if (lane == 0) { er = 0; ei = 0; }
+        if (c < nch) { O[4 * c] = cr + er; O[4 * c + 1] = ci + ei; }
+        cr += __shfl_sync(0xffffffffu, r, 31);
+        ci += __shfl_sync(0xffffffffu, i, 31);
     }
-    double vr = 0, vi = 0;
-    for (int c = nch - 1; c >= 0; c--) {
-        O[4 * c + 2] = vr;
-        O[4 * c + 3] = vi;
-        vr += T[4 * c + 2];
-        vi += T[4 * c + 3];
+    double dr = 0, di = 0;  // backward carry: v above
+    for (int base = 0; base < nch; base += 32) {
+        const int c = nch - 1 - (base + lane);
+        double r = c >= 0 ? T[4 * c + 2] : 0.0, i = c >= 0 ? T[4 * c + 3] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double a = __shfl_up_sync(0xffffffffu, r, d), b = __shfl_up_sync(0xffffffffu, i, d);
+            if (lane >= d) { r += a; i += b; }
+        }
+        double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
+        if (lane == 0) { er = 0; ei = 0; }
+        if (c >= 0) { O[4 * c + 2] = dr + er; O[4 * c + 3] = di + ei; }
+        dr += __shfl_sync(0xffffffffu, r, 31);
+        di += __shfl_sync(0xffffffffu, i, 31);
     }
-    Utot[4 * m] = ur;
-    Utot[4 * m + 1] = ui;
-    Utot[4 * m + 2] = vr;
-    Utot[4 * m + 3] = vi;
-    // split energy term Sigma_Gamma_func_s (Sigma_Gamma_func_njit.py:8-28) in scaled sums
-    const KConst K = kc[m];
-    const double W = K.W * K.W;
-    const double sig = K.g * (g2 * W * (ur * ur + ui * ui) + g1 * W * (vr * vr + vi * vi) +
-                              g1 * g2 * W * W * (ur * vr + ui * vi));
-    Eks[m] = K.ek * sig;
+    if (lane == 0) {
+        Utot[4 * m] = cr;
+        Utot[4 * m + 1] = ci;
+        Utot[4 * m + 2] = dr;
+        Utot[4 * m + 3] = di;
+        // split energy term Sigma_Gamma_func_s (Sigma_Gamma_func_njit.py:8-28) in scaled sums
+        const KConst K = kc[m];
+        const double W = K.W * K.W;
+        const double sig = K.g * (g2 * W * (cr * cr + ci * ci) + g1 * W * (dr * dr + di * di) +
+                                  g1 * g2 * W * W * (cr * dr + ci * di));
+        Eks[m] = K.ek * sig;
+    }
 }
 
-template <typename Real>
-struct Acc;
-template <>
-struct Acc<float> {
-    KahanF a;
-    __device__ __forceinline__ void init() { a.init(); }
-    __device__ __forceinline__ void add(float v) { a.add(v); }
-    __device__ __forceinline__ double get() const { return (double)a.s - (double)a.c; }
-};
-template <>
-struct Acc<double> {
-    double a;
-    __device__ __forceinline__ void init() { a = 0; }
-    __device__ __forceinline__ void add(double v) { a += v; }
-    __device__ __forceinline__ double get() const { return a; }
-};
-
 template <typename Real, bool ENERGY>
-__global__ void __launch_bounds__(LCH) k_lforce(int N, int P, int nch, const double *__restrict__ zx,
-                                                 const double *__restrict__ zy, const Real *__restrict__ zh,
-                                                 const Real *__restrict__ qv, const KConst *__restrict__ kc,
-                                                 const double *__restrict__ off, const double *__restrict__ Utot,
-                                                 const double *__restrict__ k0, const int *__restrict__ zperm,
-                                                 double g1, double g2, double *__restrict__ F3,
-                                                 double *__restrict__ Epart)
+__global__ void __launch_bounds__(LT) k_lforce(int N, int P, int nch, int ks_n, const double *__restrict__ zx,
+                                               const double *__restrict__ zy, const Real *__restrict__ zh,
+                                               const Real *__restrict__ qv, const KConst *__restrict__ kc,
+                                               const double *__restrict__ off, const double *__restrict__ Utot,
+                                               double g1, double g2, double *__restrict__ Fpart,
+                                               double *__restrict__ Epart)
 {
-    __shared__ Real wf[2][2][LCH / 32];  // [buffer][re/im] forward warp totals
-    __shared__ Real wb[2][2][LCH / 32];  // backward warp totals
-    __shared__ double ered[LCH / 32];
-    const int m = blockIdx.x * LCH + threadIdx.x;
-    const bool valid = m < N;
-    const double x = valid ? zx[m] : 0.0, y = valid ? zy[m] : 0.0;
-    const Real z = valid ? zh[m] : (Real)0, q = valid ? qv[m] : (Real)0;
+    __shared__ Real wsh[2][4][NW];  // [buffer][fwd re, fwd im, bwd re, bwd im][warp]
+    __shared__ double ered[NW];
+    Quad4<Real> P4;
+    const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
+    P4.load(N, m0, zx, zy, zh, qv);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ks = blockIdx.y;
+    const int kb = (int)((int64_t)P * ks / ks_n), ke = (int)((int64_t)P * (ks + 1) / ks_n);
     const Real G1 = (Real)g1, G2 = (Real)g2, G12 = (Real)(g1 * g2);
-    Acc<Real> ax, ay, az;
-    ax.init(); ay.init(); az.init();
+    double Fx[PPT], Fy[PPT], Fz[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) { Fx[j] = 0; Fy[j] = 0; Fz[j] = 0; }
     double E = 0;
-    for (int kidx = 0; kidx < P; kidx++) {
+    for (int kidx = kb; kidx < ke; kidx++) {
         const KConst K = kc[kidx];
-        const int buf = kidx & 1;
-        double t = fma(K.kx_2pi, x, K.ky_2pi * y);
-        t -= rint(t);
-        Real s, c;
-        LM<Real>::sc(t, s, c);
-        const Real kz = (Real)K.k * z;
-        const Real ep = LM<Real>::ex(kz), em = LM<Real>::ex(-kz);
-        const Real ur = q * ep * c, ui = q * ep * s, vr = q * em * c, vi = q * em * s;
-        // warp inclusive scans: forward for u, backward for v
-        Real fr = ur, fi = ui, br = vr, bi = vi;
+        const int buf = (kidx - kb) & 1;
+        Real c[PPT], s[PPT], ep[PPT], em[PPT], ur[PPT], ui[PPT], vr[PPT], vi[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
+            t -= rint(t);
+            LM<Real>::sc(t, s[j], c[j]);
+            const Real kz = (Real)K.k * P4.z[j];
+            ep[j] = LM<Real>::ex(kz);
+            em[j] = LM<Real>::ex(-kz);
+            ur[j] = P4.q[j] * ep[j] * c[j]; ui[j] = P4.q[j] * ep[j] * s[j];
+            vr[j] = P4.q[j] * em[j] * c[j]; vi[j] = P4.q[j] * em[j] * s[j];
+        }
+        // in-thread exclusive prefix (u, from below) and suffix (v, from above)
+        Real Ar[PPT], Ai[PPT], Cr[PPT], Ci[PPT];
+        Real tr = 0, ti = 0, br = 0, bi = 0;
+#pragma unroll
+        for (int j = 0; j < PPT; j++) { Ar[j] = tr; Ai[j] = ti; tr += ur[j]; ti += ui[j]; }
+#pragma unroll
+        for (int j = PPT - 1; j >= 0; j--) { Cr[j] = br; Ci[j] = bi; br += vr[j]; bi += vi[j]; }
+        // warp inclusive scans of the thread totals: forward for u, backward for v
+        Real fr = tr, fi = ti, gr = br, gi = bi;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const Real a1 = __shfl_up_sync(0xffffffffu, fr, d), a2 = __shfl_up_sync(0xffffffffu, fi, d);
-            const Real b1 = __shfl_down_sync(0xffffffffu, br, d), b2 = __shfl_down_sync(0xffffffffu, bi, d);
+            const Real b1 = __shfl_down_sync(0xffffffffu, gr, d), b2 = __shfl_down_sync(0xffffffffu, gi, d);
             if (lane >= d) { fr += a1; fi += a2; }
-            if (lane + d < 32) { br += b1; bi += b2; }
+            if (lane + d < 32) { gr += b1; gi += b2; }
         }
-        if (lane == 31) { wf[buf][0][w] = fr; wf[buf][1][w] = fi; }
-        if (lane == 0) { wb[buf][0][w] = br; wb[buf][1][w] = bi; }
-        // exclusive in-warp values by shifting the inclusive ones (no subtraction)
-        Real exr = __shfl_up_sync(0xffffffffu, fr, 1), exi = __shfl_up_sync(0xffffffffu, fi, 1);
-        Real eyr = __shfl_down_sync(0xffffffffu, br, 1), eyi = __shfl_down_sync(0xffffffffu, bi, 1);
-        if (lane == 0) { exr = 0; exi = 0; }
-        if (lane == 31) { eyr = 0; eyi = 0; }
+        if (lane == 31) { wsh[buf][0][w] = fr; wsh[buf][1][w] = fi; }
+        if (lane == 0) { wsh[buf][2][w] = gr; wsh[buf][3][w] = gi; }
+        // exclusive values by shifting the inclusive ones (no subtraction)
+        Real xr = __shfl_up_sync(0xffffffffu, fr, 1), xi = __shfl_up_sync(0xffffffffu, fi, 1);
+        Real yr = __shfl_down_sync(0xffffffffu, gr, 1), yi = __shfl_down_sync(0xffffffffu, gi, 1);
+        if (lane == 0) { xr = 0; xi = 0; }
+        if (lane == 31) { yr = 0; yi = 0; }
         __syncthreads();
-        Real pr = 0, pim = 0, sr = 0, sim = 0;
-        for (int ww = 0; ww < w; ww++) { pr += wf[buf][0][ww]; pim += wf[buf][1][ww]; }
-        for (int ww = LCH / 32 - 1; ww > w; ww--) { sr += wb[buf][0][ww]; sim += wb[buf][1][ww]; }
+#pragma unroll
+        for (int ww = 0; ww < NW; ww++) {
+            if (ww < w) { xr += wsh[buf][0][ww]; xi += wsh[buf][1][ww]; }
+            if (ww > w) { yr += wsh[buf][2][ww]; yi += wsh[buf][3][ww]; }
+        }
         const double *O = off + ((int64_t)kidx * nch + blockIdx.x) * 4;
         const double *U = Utot + 4 * kidx;
-        // prefix (A, B) of particles below and suffix (C, D) of particles above, in
-        // the scaled form A' = sum q e^{k(z - h)} cos, C' = sum q e^{-k(z - h)} cos
-        const Real A = (Real)O[0] + (pr + exr), B = (Real)O[1] + (pim + exi);
-        const Real Cs = (Real)O[2] + (sr + eyr), Ds = (Real)O[3] + (sim + eyi);
-        // totals with the particle's own term removed (Force_long.jl:33-36)
-        const Real f1 = (Real)U[0] - ur, f2 = (Real)U[1] - ui, f3 = (Real)U[2] - vr, f4 = (Real)U[3] - vi;
-        const Real Wh = (Real)K.W;
-        const Real Xp = (Wh * ep) * Wh, Xm = (Wh * em) * Wh;  // e^{-kLz} e^{+-k(z-h)}
-        const Real Wf = Wh * Wh;
-        const Real Yp = Xp * Wf, Ym = Xm * Wf;                  // e^{-2kLz} e^{+-k(z-h)}
-        const Real g = (Real)K.g;
-        // Fl_non_sort (Force_long.jl:39-64)
-        const Real P1 = G2 * Xp + G12 * Ym, P2 = G1 * Xm + G12 * Yp;
-        const Real Q1 = G2 * Xp - G12 * Ym, Q2 = G12 * Yp - G1 * Xm;
-        const Real xy_ns = q * g * (c * (P1 * f2 + P2 * f4) - s * (P1 * f1 + P2 * f3));
-        const Real z_ns = q * g * (c * (Q1 * f1 + Q2 * f3) + s * (Q1 * f2 + Q2 * f4));
-        // Fl_sort (Force_long.jl:103-121)
-        const Real xy_s = em * (s * A - c * B) + ep * (s * Cs - c * Ds);
-        const Real cAB = c * A + s * B, cCD = c * Cs + s * Ds;
-        const Real z_s = (Real)0.5 * q * (em * cAB - ep * cCD);
-        // Flz_self (Force_long.jl:180)
-        const Real z_self = q * q * g * (G2 * Xp * ep - G1 * Xm * em);
-        const Real wk = (Real)K.wk;
-        const Real xy = xy_ns + (Real)0.5 * q * xy_s;
-        ax.add(wk * (Real)K.fx * xy);
-        ay.add(wk * (Real)K.fy * xy);
-        az.add(wk * (z_ns + z_s + z_self));
-        if (ENERGY) E += K.ek * 0.5 * (double)(-q * q - q * (em * cAB + ep * cCD));
+        const Real bAr = (Real)O[0] + xr, bAi = (Real)O[1] + xi;
+        const Real bCr = (Real)O[2] + yr, bCi = (Real)O[3] + yi;
+        const Real U0 = (Real)U[0], U1 = (Real)U[1], U2 = (Real)U[2], U3 = (Real)U[3];
+        const Real Wh = (Real)K.W, Wf = Wh * Wh, g = (Real)K.g, wk = (Real)K.wk;
+        const Real fx = (Real)K.fx, fy = (Real)K.fy;
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const Real q = P4.q[j];
+            // prefix (A, B) of particles below and suffix (C, D) of particles above,
+            // scaled: A' = sum q e^{k(z-h)} cos, C' = sum q e^{-k(z-h)} cos
+            const Real A = bAr + Ar[j], B = bAi + Ai[j], Cs = bCr + Cr[j], Ds = bCi + Ci[j];
+            // totals with the particle's own term removed (Force_long.jl:33-36)
+            const Real f1 = U0 - ur[j], f2 = U1 - ui[j], f3 = U2 - vr[j], f4 = U3 - vi[j];
+            const Real Xp = (Wh * ep[j]) * Wh, Xm = (Wh * em[j]) * Wh;  // e^{-kLz} e^{+-k(z-h)}
+            const Real Yp = Xp * Wf, Ym = Xm * Wf;                      // e^{-2kLz} e^{+-k(z-h)}
+            // Fl_non_sort (Force_long.jl:39-64)
+            const Real P1 = G2 * Xp + G12 * Ym, P2 = G1 * Xm + G12 * Yp;
+            const Real Q1 = G2 * Xp - G12 * Ym, Q2 = G12 * Yp - G1 * Xm;
+            const Real xy_ns = q * g * (c[j] * (P1 * f2 + P2 * f4) - s[j] * (P1 * f1 + P2 * f3));
+            const Real z_ns = q * g * (c[j] * (Q1 * f1 + Q2 * f3) + s[j] * (Q1 * f2 + Q2 * f4));
+            // Fl_sort (Force_long.jl:103-121)
+            const Real xy_s = em[j] * (s[j] * A - c[j] * B) + ep[j] * (s[j] * Cs - c[j] * Ds);
+            const Real cAB = c[j] * A + s[j] * B, cCD = c[j] * Cs + s[j] * Ds;
+            const Real z_s = (Real)0.5 * q * (em[j] * cAB - ep[j] * cCD);
+            // Flz_self (Force_long.jl:180)
+            const Real z_self = q * q * g * (G2 * Xp * ep[j] - G1 * Xm * em[j]);
+            const Real xy = wk * (xy_ns + (Real)0.5 * q * xy_s);
+            Fx[j] += (double)(fx * xy);
+            Fy[j] += (double)(fy * xy);
+            Fz[j] += (double)(wk * (z_ns + z_s + z_self));
+            if (ENERGY) E += K.ek * 0.5 * (double)(-q * q - q * (em[j] * cAB + ep[j] * cCD));
+        }
     }
-    if (valid) {
-        const int i = zperm[m];
-        F3[3 * i] += ax.get();
-        F3[3 * i + 1] += ay.get();
-        F3[3 * i + 2] += az.get() + k0[m];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int m = m0 + j;
+        if (m < N) {
+            double *o = Fpart + ((int64_t)ks * N + m) * 3;
+            o[0] = Fx[j];
+            o[1] = Fy[j];
+            o[2] = Fz[j];
+        }
     }
     if (ENERGY) {
         for (int d = 16; d > 0; d >>= 1) E += __shfl_down_sync(0xffffffffu, E, d);
@@ -299,15 +352,34 @@ __global__ void __launch_bounds__(LCH) k_lforce(int N, int P, int nch, const dou
         __syncthreads();
         if (threadIdx.x == 0) {
             double sum = 0;
-            for (int ww = 0; ww < LCH / 32; ww++) sum += ered[ww];
-            Epart[blockIdx.x] = sum;
+            for (int ww = 0; ww < NW; ww++) sum += ered[ww];
+            Epart[(int64_t)ks * nch + blockIdx.x] = sum;
         }
     }
 }
 
-__global__ void k_add3(int n, const double *__restrict__ a, double *__restrict__ out)
+// F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term
+__global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, const double *__restrict__ k0,
+                         const int *__restrict__ zperm, double *__restrict__ F3)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double fx = 0, fy = 0, fz = 0;
+    for (int ks = 0; ks < ks_n; ks++) {
+        const double *o = Fpart + ((int64_t)ks * N + m) * 3;
+        fx += o[0];
+        fy += o[1];
+        fz += o[2];
+    }
+    const int i = zperm[m];
+    F3[3 * i] += fx;
+    F3[3 * i + 1] += fy;
+    F3[3 * i + 2] += fz + k0[m];
+}
+
+__global__ void k_add(int n, const double *__restrict__ a, double *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += a[i];
 }
 
@@ -333,60 +405,68 @@ inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 
 int qem_long_chunk(void) { return LCH; }
 
-// Long range for N particles and P k-vectors; adds into F3 (original order).
-// Energy partials: b.Epart[0 .. nch) from k_lforce, [nch .. nch + nk0) from
-// k_k0 and the P split terms in b.Eks.
+int qem_long_ksplit(int nch, int P, int max_ks)
+{
+    int ks = (4 * 148 + nch - 1) / nch;  // enough blocks for every SM
+    ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
+    const int pm = P > 1 ? P : 1;
+    return ks < pm ? ks : pm;
+}
+
+// Energy partials: b.Epart[0 .. ks * nch) from k_lforce, [ks * nch .. + nb0)
+// from k_k0; the P split terms go to b.Eks.
 cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const double4 *pos, const int *zperm,
                             const LongBuffers &b, double Lx, double Ly, double Lz, double g1, double g2, double eps0,
                             double sum_K, double *F3, int nch, unsigned *status, cudaStream_t s, int stage)
 {
     (void)status;
     if (N <= 0) return cudaSuccess;
-    if (stage == 1) goto force_pass;
-    {
-    const double h = 0.5 * Lz;
-    k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd);
-    cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
-    if (e != cudaSuccess) return e;
-    const double fscale = 1.0 / (2.0 * Lx * Ly * eps0);
-    const double escale = -1.0 / (4.0 * eps0 * Lx * Ly);
-    k_k0<<<nblk(N, 256), 256, 0, s>>>(N, b.qd, b.zhd, h, b.qscan, fscale, escale, b.k0, b.Epart + nch, energy ? 1 : 0);
-    if (P > 0) {
-        const double wk = (sum_K / P) / (Lx * Ly * eps0);
-        const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
-        k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc);
-        dim3 g1d(nch, nblk(P, KPB));
-        if (precision == QEM_FP64)
-            k_ltot<double><<<g1d, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
-        else
-            k_ltot<float><<<g1d, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
-        k_lscan<<<nblk(P, 64), 64, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks);
+    if (stage == 0) {
+        const double h = 0.5 * Lz;
+        k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd);
+        cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
+        if (e != cudaSuccess) return e;
+        const double fscale = 1.0 / (2.0 * Lx * Ly * eps0);
+        const double escale = -1.0 / (4.0 * eps0 * Lx * Ly);
+        k_k0<<<nblk(N, 256), 256, 0, s>>>(N, b.qd, b.zhd, h, b.qscan, fscale, escale, b.k0, b.Epart + b.ks * nch,
+                                          energy ? 1 : 0);
+        if (P > 0) {
+            const double wk = (sum_K / P) / (Lx * Ly * eps0);
+            const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
+            k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc);
+            dim3 gt(nch, nblk(P, KPB));
+            if (precision == QEM_FP64)
+                k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
+            else
+                k_ltot<float><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
+            k_lscan<<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks);
+        }
+        return cudaGetLastError();
     }
-    }
-    if (stage == 0) return cudaGetLastError();
-force_pass:
+    dim3 gf(nch, b.ks);
     if (precision == QEM_FP64) {
         if (energy)
-            k_lforce<double, true><<<nch, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot, b.k0,
-                                                       zperm, g1, g2, F3, b.Epart);
+            k_lforce<double, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot,
+                                                     g1, g2, b.Fpart, b.Epart);
         else
-            k_lforce<double, false><<<nch, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot,
-                                                        b.k0, zperm, g1, g2, F3, b.Epart);
+            k_lforce<double, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot,
+                                                      g1, g2, b.Fpart, b.Epart);
     } else {
         if (energy)
-            k_lforce<float, true><<<nch, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot, b.k0,
-                                                      zperm, g1, g2, F3, b.Epart);
+            k_lforce<float, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot,
+                                                    g1, g2, b.Fpart, b.Epart);
         else
-            k_lforce<float, false><<<nch, LCH, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot,
-                                                       b.k0, zperm, g1, g2, F3, b.Epart);
+            k_lforce<float, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot,
+                                                     g1, g2, b.Fpart, b.Epart);
     }
+    k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3);
     return cudaGetLastError();
 }
 
 cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;
-    k_add3<<<nblk(n, 256), 256, 0, s>>>(n, a, out);
+    k_add<<<nblk(n, 256), 256, 0, s>>>(n, a, out);
     return cudaGetLastError();
 }
 

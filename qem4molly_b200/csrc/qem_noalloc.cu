@@ -26,7 +26,8 @@ namespace {
 
 constexpr int NA_MAX_N = QEM_NOALLOC_MAX_N;
 constexpr int NA_MAX_P = QEM_NOALLOC_MAX_P;
-constexpr int NA_CH = 256;  // particles per long-range chunk (qem_long_chunk())
+constexpr int NA_CH = 512;    // particles per long-range chunk (qem_long_chunk())
+constexpr int NA_MAX_KS = 2;  // k slices of the force pass
 constexpr int NA_MAX_NCH = (NA_MAX_N + NA_CH - 1) / NA_CH;
 
 constexpr size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -49,8 +50,9 @@ constexpr size_t O_KC = O_KIN + al(sizeof(double) * 3 * NA_MAX_P);
 constexpr size_t O_TOT = O_KC + al(sizeof(KConst) * NA_MAX_P);
 constexpr size_t O_OFF = O_TOT + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
 constexpr size_t O_UTOT = O_OFF + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
-constexpr size_t O_EPART = O_UTOT + al(sizeof(double) * 4 * NA_MAX_P);
-constexpr size_t N_EPART = NA_MAX_NCH + (NA_MAX_N + 255) / 256 + NA_MAX_P + 8;
+constexpr size_t O_FPART = O_UTOT + al(sizeof(double) * 4 * NA_MAX_P);
+constexpr size_t O_EPART = O_FPART + al(sizeof(double) * 3 * (size_t)NA_MAX_KS * NA_MAX_N);
+constexpr size_t N_EPART = NA_MAX_KS * NA_MAX_NCH + (NA_MAX_N + 255) / 256 + NA_MAX_P + 8;
 constexpr size_t O_STMP = O_EPART + al(sizeof(double) * N_EPART);
 constexpr size_t STMP_BYTES = sizeof(double) * ((NA_MAX_N + 1023) / 1024 + 8);
 constexpr size_t O_STATUS = O_STMP + al(STMP_BYTES);
@@ -108,6 +110,7 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
         kmax = std::max(kmax, k);
     }
     if (p->precision == QEM_FP32_FIX && P > 0 && kmax * p->Lz > 120.0) return QEM_ERR_RANGE;
+    if (qem_long_chunk() != NA_CH) return reject("scratch layout does not match the long-range chunk size");
     if (cudaSetDevice(p->device) != cudaSuccess) return QEM_ERR_CUDA;
     unsigned char *S = nullptr;
     qem_status st = scratch_address(p->device, &S);
@@ -134,9 +137,11 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     b.kc = (KConst *)(S + O_KC); b.kin = (double *)(S + O_KIN);
     b.tot = (double *)(S + O_TOT); b.off = (double *)(S + O_OFF); b.Utot = (double *)(S + O_UTOT);
     b.Epart = (double *)(S + O_EPART);
-    b.Eks = b.Epart + NA_MAX_NCH + (NA_MAX_N + 255) / 256;
-    b.stmp = S + O_STMP; b.stmp_bytes = STMP_BYTES;
     const int nch = (N + NA_CH - 1) / NA_CH;
+    b.ks = qem_long_ksplit(nch, P, NA_MAX_KS);
+    b.Fpart = (double *)(S + O_FPART);
+    b.Eks = b.Epart + (size_t)b.ks * nch + (NA_MAX_N + 255) / 256;
+    b.stmp = S + O_STMP; b.stmp_bytes = STMP_BYTES;
     for (int stage = 0; stage < 2 && e == cudaSuccess; stage++)
         e = qem_launch_long(p->precision, false, N, P, pos, zperm, b, p->Lx, p->Ly, p->Lz, p->gamma_down, p->gamma_up,
                             p->eps_0, sum_K, F, nch, status, s, stage);

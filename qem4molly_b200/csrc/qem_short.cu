@@ -11,21 +11,42 @@
 //
 // One thread per unordered pair evaluates the 4 image terms x {point, gauss}
 // x N_t Gauss-Legendre nodes in registers (nodes in the constant bank) and
-// writes (F_ij.x, F_ij.y, F_ij.z, z-force on j) to a per-pair record; a
-// per-particle pass sums its own and its incoming records in a fixed order,
-// adds the self term and the walls.  No atomics: results are bitwise
-// reproducible from run to run.
+// writes one record per pair (force on the pair's owner and z-force on the
+// other particle); a per-particle pass sums its own and its incoming records
+// in a fixed order, adds the self term and the walls.  No atomics: results
+// are bitwise reproducible from run to run.
+//
+// Both integral families share one node body: with
+//   point  (Gamma_2 term):  G = -g_u g_d b/2 e^{-k (a + 2 L_z)} / D,
+//   gauss  (Gamma_1 term):  G = -b/2 e^{-k (a + k / 4 alpha)} / D,
+//   D = 1 - g_u g_d e^{-2 k L_z},
+// every interval is G = pf exp(-k (a' + c2 k)) / D for per-interval (pf, a', c2),
+// so the 8 intervals run through one rolled loop (small code, no instruction
+// cache misses).  Each block orders its 256 pairs by rho in shared memory
+// before the quadrature, so the threads of a warp mostly take the same
+// Bessel branch; records are still written at the pair's own index.
 //
 // FP32 path: per-pair set-up (minimum image, rho, image distances, quadrature
 // limits, closed-form image terms) and all cross-image sums in FP64; the
 // per-node integrands in FP32 with hardware exp / rcp / cos and the
-// Abramowitz-Stegun Bessel approximations.  The image-series denominator
-// 1 - g_u g_d e^{-2 k L_z} is formed as (1 - g_u g_d) + g_u g_d (1 - e^{-t})
-// with (1 - g_u g_d) from FP64 and 1 - e^{-t} evaluated without cancellation,
-// so its relative error stays at FP32 rounding as |g_u g_d| -> 1.
+// Abramowitz-Stegun Bessel approximations.  The denominator D is formed as
+// (1 - g_u g_d) + g_u g_d (1 - e^{-t}) with (1 - g_u g_d) from FP64 and
+// 1 - e^{-t} evaluated without cancellation, so its relative error stays at
+// FP32 rounding as |g_u g_d| -> 1.
 #include "qem_internal.cuh"
 
 namespace {
+
+constexpr int PAIR_BLOCK = 256;
+// resident pair blocks per SM requested from the register allocator, and the
+// unroll factor of the FP32 node loop (tuning knobs; measured defaults)
+#ifndef QEM_PAIR_MINB
+#define QEM_PAIR_MINB 4
+#endif
+#ifndef QEM_NODE_UNROLL
+#define QEM_NODE_UNROLL 2
+#endif
+constexpr int NODE_UNROLL = QEM_NODE_UNROLL;
 
 // quadrature limits of image term l (Force_short.jl:48-67 / greens_function.jl:26-27,
 // or the python_lib global limits)
@@ -40,52 +61,69 @@ __device__ __forceinline__ double gauss_limit(const ShortConsts &c, double a)
     return c.neg_lnacc / (c.twoLz + a);
 }
 
-// ---------------------------------------------------------------------------
-// per-interval quadratures.  I_r = sum w k G J1, I_z = sum w k G J0 (image sign
-// applied by the caller), I_u = sum w G J0 (energy).  point: G = Gamma_2 term,
-// gauss: G = Gamma_1 term x exp(-k^2 / 4 alpha).
-// ---------------------------------------------------------------------------
-template <bool ENERGY, bool WITH_J1>
-__device__ __forceinline__ void quad_f64(const ShortConsts &c, bool point, double K, double a, double hb, double rho,
-                                         double &Ir, double &Iz, double &Iu)
+// interval constants: image term l, family (0 point, 1 gauss)
+struct Interval {
+    double K;    // upper limit
+    double ae;   // a' (a + 2 L_z for point, a for gauss)
+    double c2;   // 0 for point, 1 / (4 alpha) for gauss
+    double pf;   // -g_u g_d b / 2 for point, -b / 2 for gauss
+};
+__device__ __forceinline__ Interval interval(const ShortConsts &c, double a, double b, bool gauss)
 {
-    const double h = 0.5 * K;
-    Ir = 0; Iz = 0; Iu = 0;
+    Interval v;
+    if (gauss) {
+        v.K = gauss_limit(c, a);
+        v.ae = a;
+        v.c2 = c.inv4alpha;
+        v.pf = -0.5 * b;
+    } else {
+        v.K = point_limit(c, a);
+        v.ae = a + c.twoLz;
+        v.c2 = 0.0;
+        v.pf = -0.5 * b * c.g12;
+    }
+    return v;
+}
+
+// I_r = sum w k G J1, I_z = sum w k G J0 (image sign applied by the caller),
+// I_u = sum w G J0 (energy)
+template <bool ENERGY, bool WITH_J1>
+__device__ __forceinline__ void quad_f64(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
+                                         double &Iu)
+{
+    const double h = 0.5 * v.K;
+    double r = 0, z = 0, u = 0;
+#pragma unroll 1
     for (int n = 0; n < c.Nt; n++) {
         const double k = fma(h, c.xd[n], h);
         const double w = h * c.wd[n];
-        const double E2 = exp(-k * c.twoLz);
-        const double D = c.g12 * E2 - 1.0;
-        double G;
-        if (point) G = c.g12 * (hb * exp(-k * a)) * E2 / D;
-        else G = (hb * exp(-k * a - k * k * c.inv4alpha)) / D;
+        const double D = 1.0 - c.g12 * exp(-k * c.twoLz);
+        const double G = v.pf * exp(-k * fma(k, v.c2, v.ae)) / D;
         const double x = k * rho;
-        const double J0 = (rho == 0.0) ? 1.0 : j0(x);
+        const double J0 = WITH_J1 ? j0(x) : 1.0;
         const double cw = w * k * G;
-        if (WITH_J1) Ir = fma(cw, j1(x), Ir);
-        Iz = fma(cw, J0, Iz);
-        if (ENERGY) Iu = fma(w * G, J0, Iu);
+        if (WITH_J1) r = fma(cw, j1(x), r);
+        z = fma(cw, J0, z);
+        if (ENERGY) u = fma(w * G, J0, u);
     }
+    Ir = r; Iz = z; Iu = u;
 }
 
 template <bool ENERGY, bool WITH_J1>
-__device__ __forceinline__ void quad_f32(const ShortConsts &c, bool point, float K, float a, float hb, float rho,
-                                         float twoLz, float g12, float omg12, float inv4a, float &Ir, float &Iz,
+__device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, float rho, float &Ir, float &Iz,
                                          float &Iu)
 {
-    const float h = 0.5f * K;
+    const float h = 0.5f * (float)v.K;
+    const float ae = (float)v.ae, c2 = (float)v.c2, pf = (float)v.pf;
+    const float twoLz = (float)c.twoLz, g12 = (float)c.g12, omg = (float)c.one_minus_g12;
     float r = 0.f, z = 0.f, u = 0.f;
-#pragma unroll 2
+#pragma unroll NODE_UNROLL
     for (int n = 0; n < c.Nt; n++) {
         const float k = fmaf(h, c.xf[n], h);
         const float w = h * c.wf[n];
         const float t = k * twoLz;
-        const float E2 = __expf(-t);
-        const float Dp = fmaf(g12, one_minus_exp_neg(t, E2), omg12);  // 1 - g12 e^{-t} > 0
-        const float invD = fast_rcp(Dp);
-        float G;
-        if (point) G = -g12 * hb * __expf(-k * a) * E2 * invD;
-        else G = -hb * __expf(-k * fmaf(k, inv4a, a)) * invD;
+        const float Dp = fmaf(g12, one_minus_exp_neg(t, __expf(-t)), omg);  // 1 - g12 e^{-t} > 0
+        const float G = pf * __expf(-k * fmaf(k, c2, ae)) * fast_rcp(Dp);
         float J0 = 1.0f, J1 = 0.0f;
         if (WITH_J1) bessel01_f32(k * rho, J0, J1);
         const float cw = w * k * G;
@@ -96,17 +134,75 @@ __device__ __forceinline__ void quad_f32(const ShortConsts &c, bool point, float
     Ir = r; Iz = z; Iu = u;
 }
 
+template <int PREC, bool ENERGY, bool WITH_J1>
+__device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
+                                     double &Iu)
+{
+    if (PREC == QEM_FP64) {
+        quad_f64<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
+    } else {
+        float r, z, u;
+        quad_f32<ENERGY, WITH_J1>(c, v, (float)rho, r, z, u);
+        Ir = r; Iz = z; Iu = u;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // pair kernel
 // ---------------------------------------------------------------------------
+// np: device pointer to the pair count; the grid covers the capacity cap and
+// blocks past the count return (a count above cap, which the host treats as
+// an overflow and re-evaluates, is clamped so every access stays in bounds)
 template <int PREC, bool ENERGY>
-__global__ void __launch_bounds__(128) k_short_pair(int64_t Np, const int2 *__restrict__ pairs,
-                                                     const double4 *__restrict__ pos, double4 *__restrict__ R,
-                                                     double *__restrict__ Upair, const ShortConsts c)
+__global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const int64_t *__restrict__ np,
+                                                                           int64_t cap,
+                                                                           const int2 *__restrict__ pairs,
+                                                                           const double4 *__restrict__ pos,
+                                                                           double4 *__restrict__ R,
+                                                                           double *__restrict__ Upair,
+                                                                           const ShortConsts c)
 {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double skey[PAIR_BLOCK];
+    __shared__ int sidx[PAIR_BLOCK];
+    const int64_t Np = min(*np, cap);
+    if ((int64_t)blockIdx.x * PAIR_BLOCK >= Np) return;  // whole block: before any barrier
+    // 1. every thread loads one pair and its rho^2; order the block's pairs by rho^2
+    {
+        const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + threadIdx.x;
+        double key = 1e300;
+        if (p < Np) {
+            const int2 ij = pairs[p];
+            const double4 pi = pos[ij.x], pj = pos[ij.y];
+            const double dx = min_image(pi.x - pj.x, c.Lx, c.invLx), dy = min_image(pi.y - pj.y, c.Ly, c.invLy);
+            key = dx * dx + dy * dy;
+        }
+        skey[threadIdx.x] = key;
+        sidx[threadIdx.x] = threadIdx.x;
+        __syncthreads();
+        for (int size = 2; size <= PAIR_BLOCK; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const int t = threadIdx.x;
+                const int partner = t ^ stride;
+                if (partner > t) {
+                    const bool up = ((t & size) == 0);
+                    const double ka = skey[t], kb = skey[partner];
+                    if ((ka > kb) == up) {
+                        skey[t] = kb; skey[partner] = ka;
+                        const int ia = sidx[t];
+                        sidx[t] = sidx[partner]; sidx[partner] = ia;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + sidx[threadIdx.x];
     if (p >= Np) return;
-    const int2 ij = pairs[p];
+    // stored as (owner, other); evaluated as F_short_ij with i the lower index
+    // (the canonical orientation of QEM_short.jl:41-47), recorded for the owner
+    const int2 oo = pairs[p];
+    const bool owner_is_i = oo.x < oo.y;
+    const int2 ij = owner_is_i ? oo : make_int2(oo.y, oo.x);
     const double4 pi = pos[ij.x], pj = pos[ij.y];
     const double dxr = pi.x - pj.x, dyr = pi.y - pj.y;
     const double dx = min_image(dxr, c.Lx, c.invLx), dy = min_image(dyr, c.Ly, c.invLy);
@@ -120,59 +216,45 @@ __global__ void __launch_bounds__(128) k_short_pair(int64_t Np, const int2 *__re
     const double zi = pi.z, zj = pj.z;
     const double zn = fabs(zi - zj), zp = zi + zj;
     const double s = jl_sign(zi - zj);
-    const double av[4] = {zn, zp, c.twoLz - zp, c.twoLz - zn};
-    const double bv[4] = {1.0, c.g1, c.g2, c.g12};
-    const double si[4] = {-s, -1.0, 1.0, s};  // greens_function.jl:24
-    const double sj[4] = {s, -1.0, 1.0, -s};  // same element seen from j
-    double Fp1 = 0, Fg = 0, Fzp_i = 0, Fzp_j = 0, Fzg_i = 0, Fzg_j = 0, Up = 0, Ug = 0;
-    double Fp2 = 0, Fz2_i = 0, Fz2_j = 0, Ub = 0;
-    const bool has_rho = (rho != 0.0);
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-        const double a = av[l];
-        const double hb = 0.5 * bv[l];
-        const double Kp = point_limit(c, a), Kg = gauss_limit(c, a);
-        double pr, pz, pu, gr, gz, gu;
-        if (PREC == QEM_FP64) {
-            quad_f64<ENERGY, true>(c, true, Kp, a, hb, rho, pr, pz, pu);
-            quad_f64<ENERGY, true>(c, false, Kg, a, hb, rho, gr, gz, gu);
-        } else {
-            float fr, fz, fu;
-            const float twoLz = (float)c.twoLz, g12 = (float)c.g12, omg = (float)c.one_minus_g12,
-                        i4a = (float)c.inv4alpha;
-            quad_f32<ENERGY, true>(c, true, (float)Kp, (float)a, (float)hb, (float)rho, twoLz, g12, omg, i4a, fr, fz,
-                                   fu);
-            pr = fr; pz = fz; pu = fu;
-            quad_f32<ENERGY, true>(c, false, (float)Kg, (float)a, (float)hb, (float)rho, twoLz, g12, omg, i4a, fr,
-                                   fz, fu);
-            gr = fr; gz = fz; gu = fu;
+    // accumulated: Fr = -sum point_r + sum gauss_r; Fz = sum s_l (point_z - gauss_z); U = Ug - Up
+    double Fr = 0, Fzi = 0, Fzj = 0, U = 0, Fp2 = 0, Fz2i = 0, Fz2j = 0, Ub = 0;
+#pragma unroll 1
+    for (int iv = 0; iv < 8; iv++) {
+        const int l = iv >> 1;
+        const bool gauss = (iv & 1) != 0;
+        const double a = (l == 0) ? zn : (l == 1) ? zp : (l == 2) ? c.twoLz - zp : c.twoLz - zn;
+        const double b = (l == 0) ? 1.0 : (l == 1) ? c.g1 : (l == 2) ? c.g2 : c.g12;
+        const double si = (l == 0) ? -s : (l == 1) ? -1.0 : (l == 2) ? 1.0 : s;  // greens_function.jl:24
+        const double sj = (l == 1 || l == 2) ? si : -si;                          // the element seen from j
+        double Ir, Iz, Iu;
+        quad<PREC, ENERGY, true>(c, interval(c, a, b, gauss), rho, Ir, Iz, Iu);
+        const double sf = gauss ? 1.0 : -1.0;
+        Fr += sf * Ir;
+        Fzi -= sf * si * Iz;
+        Fzj -= sf * sj * Iz;
+        if (ENERGY) U += sf * Iu;
+        if (!gauss) {  // closed-form image terms (Force_short.jl:49, 65)
+            const double r2 = a * a + rho2;
+            const double inv15 = 1.0 / (r2 * sqrt(r2));
+            Fp2 += b * rho * inv15;
+            Fz2i += b * a * si * inv15;
+            Fz2j += b * a * sj * inv15;
+            if (ENERGY) Ub += 0.5 * b / sqrt(r2);
         }
-        Fp1 += pr;
-        Fg += gr;
-        Fzp_i += si[l] * pz;
-        Fzp_j += sj[l] * pz;
-        Fzg_i += si[l] * gz;
-        Fzg_j += sj[l] * gz;
-        if (ENERGY) { Up += pu; Ug += gu; }
-        const double r2 = a * a + rho2;
-        const double inv15 = 1.0 / (r2 * sqrt(r2));
-        Fp2 += bv[l] * rho * inv15;
-        Fz2_i += bv[l] * a * si[l] * inv15;
-        Fz2_j += bv[l] * a * sj[l] * inv15;
-        if (ENERGY) Ub += 0.5 * bv[l] / sqrt(r2);
     }
     const double pref = pi.w * pj.w * c.pref;
     double Fx = 0, Fy = 0;
-    if (has_rho) {
-        const double Fsr = -Fp1 + 0.5 * Fp2 + Fg;
+    if (rho != 0.0) {  // Force_short.jl:46
+        const double Fsr = Fr + 0.5 * Fp2;
         const bool mi = (c.flags & QEM_DIR_MINIMAGE) != 0;
         Fx = pref * Fsr * (mi ? dx : dxr) / rho;
         Fy = pref * Fsr * (mi ? dy : dyr) / rho;
     }
-    const double Fzi = pref * (Fzp_i - 0.5 * Fz2_i - Fzg_i);
-    const double Fzj = pref * (Fzp_j - 0.5 * Fz2_j - Fzg_j);
-    R[p] = make_double4(Fx, Fy, Fzi, (c.flags & QEM_PAIR_PHYSICAL) ? Fzj : -Fzi);
-    if (ENERGY) Upair[p] = pref * (Ug - Up + Ub);
+    const double Fz_i = pref * (Fzi - 0.5 * Fz2i);
+    const double Fz_j = (c.flags & QEM_PAIR_PHYSICAL) ? pref * (Fzj - 0.5 * Fz2j) : -Fz_i;
+    // record: x, y, z on the owner and z on the other particle (x, y on the other = -owner's)
+    R[p] = owner_is_i ? make_double4(Fx, Fy, Fz_i, Fz_j) : make_double4(-Fx, -Fy, Fz_j, Fz_i);
+    if (ENERGY) Upair[p] = pref * (U + Ub);
 }
 
 // ---------------------------------------------------------------------------
@@ -182,43 +264,29 @@ __global__ void __launch_bounds__(128) k_short_pair(int64_t Np, const int2 *__re
 template <int PREC, bool ENERGY>
 __device__ void self_terms(const ShortConsts &c, double z, double q, double &Fz, double &E)
 {
-    const double av[4] = {0.0, 2.0 * z, c.twoLz - 2.0 * z, c.twoLz};
-    const double bv[4] = {1.0, c.g1, c.g2, c.g12};
-    const double sa[4] = {0.0, -1.0, 1.0, 0.0};
-    double Fp1 = 0, Fg = 0, Up = 0, Ug = 0, Ub = 0;
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-        const bool zterm = (l == 1 || l == 2);  // sign_a = 0 for l = 1, 4
+    double Fs = 0, U = 0, Ub = 0;
+#pragma unroll 1
+    for (int iv = 0; iv < 8; iv++) {
+        const int l = iv >> 1;
+        const bool gauss = (iv & 1) != 0;
+        const bool zterm = (l == 1 || l == 2);  // sign_a = 0 for l = 1, 4 (greens_function.jl:42)
         if (!ENERGY && !zterm) continue;
-        const double a = av[l], hb = 0.5 * bv[l];
-        const double Kp = point_limit(c, a), Kg = gauss_limit(c, a);
-        double pr, pz, pu, gr, gz, gu;
-        if (PREC == QEM_FP64) {
-            quad_f64<ENERGY, false>(c, true, Kp, a, hb, 0.0, pr, pz, pu);
-            quad_f64<ENERGY, false>(c, false, Kg, a, hb, 0.0, gr, gz, gu);
-        } else {
-            float fr, fz, fu;
-            const float twoLz = (float)c.twoLz, g12 = (float)c.g12, omg = (float)c.one_minus_g12,
-                        i4a = (float)c.inv4alpha;
-            quad_f32<ENERGY, false>(c, true, (float)Kp, (float)a, (float)hb, 0.f, twoLz, g12, omg, i4a, fr, fz, fu);
-            pz = fz; pu = fu;
-            quad_f32<ENERGY, false>(c, false, (float)Kg, (float)a, (float)hb, 0.f, twoLz, g12, omg, i4a, fr, fz, fu);
-            gz = fz; gu = fu;
-        }
-        if (zterm) {
-            Fp1 += sa[l] * pz;
-            Fg += sa[l] * gz;
-        }
+        const double a = (l == 0) ? 0.0 : (l == 1) ? 2.0 * z : (l == 2) ? c.twoLz - 2.0 * z : c.twoLz;
+        const double b = (l == 0) ? 1.0 : (l == 1) ? c.g1 : (l == 2) ? c.g2 : c.g12;
+        const double sa = (l == 1) ? -1.0 : (l == 2) ? 1.0 : 0.0;
+        double Ir, Iz, Iu;
+        quad<PREC, ENERGY, false>(c, interval(c, a, b, gauss), 0.0, Ir, Iz, Iu);
+        const double sf = gauss ? 1.0 : -1.0;
+        if (zterm) Fs += sf * sa * Iz;  // -Fp1 + Fg
         if (ENERGY) {
-            Up += pu;
-            Ug += gu;
-            if (l > 0) Ub += 0.5 * bv[l] / a;
+            U += sf * Iu;
+            if (!gauss && l > 0) Ub += 0.5 * b / a;
         }
     }
-    const double Fp2 = 0.5 * (bv[1] * av[1] * sa[1] / (av[1] * av[1] * av[1]) +
-                              bv[2] * av[2] * sa[2] / (av[2] * av[2] * av[2]));
-    Fz = -q * q * c.pref * (-Fp1 + Fp2 + Fg);
-    if (ENERGY) E = 0.5 * q * q * c.pref * (Ug - Up + Ub);
+    const double a1 = 2.0 * z, a2 = c.twoLz - 2.0 * z;
+    const double Fp2 = 0.5 * (c.g1 * a1 * -1.0 / (a1 * a1 * a1) + c.g2 * a2 * 1.0 / (a2 * a2 * a2));
+    Fz = -q * q * c.pref * (Fs + Fp2);
+    if (ENERGY) E = 0.5 * q * q * c.pref * (U + Ub);
 }
 
 // ---------------------------------------------------------------------------
@@ -229,9 +297,10 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
                                                        const int *__restrict__ pos_of, const int64_t *__restrict__ poff,
                                                        const double4 *__restrict__ R, const double *__restrict__ Upair,
                                                        const int64_t *__restrict__ in_off,
-                                                       const int64_t *__restrict__ in_list, const ShortConsts c,
-                                                       double *__restrict__ F3, double *__restrict__ Epart,
-                                                       unsigned *status, int do_short, int do_lj)
+                                                       const int64_t *__restrict__ in_list, int64_t cap,
+                                                       const ShortConsts c, double *__restrict__ F3,
+                                                       double *__restrict__ Epart, unsigned *status, int do_short,
+                                                       int do_lj)
 {
     __shared__ double red[256 / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -240,7 +309,8 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
         const double4 pi = pos[i];
         if (do_short) {
             const int t = pos_of[i];
-            for (int64_t p = poff[t]; p < poff[t + 1]; p++) {
+            const int64_t pe = min(poff[t + 1], cap);
+            for (int64_t p = min(poff[t], cap); p < pe; p++) {
                 const double4 r = R[p];
                 Fx += r.x; Fy += r.y; Fz += r.z;
                 if (ENERGY) E += Upair[p];
@@ -289,25 +359,25 @@ inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 
 }  // namespace
 
-cudaError_t qem_launch_short_pairs(int precision, bool energy, int64_t Np, const int2 *pairs, const double4 *pos,
-                                   double4 *R, double *Upair, const ShortConsts &c, cudaStream_t s)
+cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np, int64_t cap, const int2 *pairs,
+                                   const double4 *pos, double4 *R, double *Upair, const ShortConsts &c,
+                                   cudaStream_t s)
 {
-    if (Np <= 0) return cudaSuccess;
-    const int B = 128;
-    const int G = nblk(Np, B);
+    if (cap <= 0) return cudaSuccess;
+    const int G = nblk(cap, PAIR_BLOCK);
     if (precision == QEM_FP64) {
-        if (energy) k_short_pair<QEM_FP64, true><<<G, B, 0, s>>>(Np, pairs, pos, R, Upair, c);
-        else k_short_pair<QEM_FP64, false><<<G, B, 0, s>>>(Np, pairs, pos, R, Upair, c);
+        if (energy) k_short_pair<QEM_FP64, true><<<G, PAIR_BLOCK, 0, s>>>(np, cap, pairs, pos, R, Upair, c);
+        else k_short_pair<QEM_FP64, false><<<G, PAIR_BLOCK, 0, s>>>(np, cap, pairs, pos, R, Upair, c);
     } else {
-        if (energy) k_short_pair<QEM_FP32_FIX, true><<<G, B, 0, s>>>(Np, pairs, pos, R, Upair, c);
-        else k_short_pair<QEM_FP32_FIX, false><<<G, B, 0, s>>>(Np, pairs, pos, R, Upair, c);
+        if (energy) k_short_pair<QEM_FP32_FIX, true><<<G, PAIR_BLOCK, 0, s>>>(np, cap, pairs, pos, R, Upair, c);
+        else k_short_pair<QEM_FP32_FIX, false><<<G, PAIR_BLOCK, 0, s>>>(np, cap, pairs, pos, R, Upair, c);
     }
     return cudaGetLastError();
 }
 
 cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, bool do_lj, int N,
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
-                                    const double *Upair, const int64_t *in_off, const int64_t *in_list,
+                                    const double *Upair, const int64_t *in_off, const int64_t *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s)
 {
@@ -317,18 +387,18 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
     const int ds = do_short ? 1 : 0, dl = do_lj ? 1 : 0;
     if (precision == QEM_FP64) {
         if (energy)
-            k_short_gather<QEM_FP64, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, c, F3,
-                                                            Epart, status, ds, dl);
+            k_short_gather<QEM_FP64, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap, c,
+                                                            F3, Epart, status, ds, dl);
         else
-            k_short_gather<QEM_FP64, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, c, F3,
-                                                             Epart, status, ds, dl);
+            k_short_gather<QEM_FP64, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap, c,
+                                                             F3, Epart, status, ds, dl);
     } else {
         if (energy)
-            k_short_gather<QEM_FP32_FIX, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, c,
-                                                                F3, Epart, status, ds, dl);
+            k_short_gather<QEM_FP32_FIX, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap,
+                                                                c, F3, Epart, status, ds, dl);
         else
-            k_short_gather<QEM_FP32_FIX, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, c,
-                                                                 F3, Epart, status, ds, dl);
+            k_short_gather<QEM_FP32_FIX, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list,
+                                                                 cap, c, F3, Epart, status, ds, dl);
     }
     return cudaGetLastError();
 }
