@@ -249,7 +249,12 @@ static void build_consts(qem_handle *h)
     gauss_legendre(p.N_t, x, w);
     for (int i = 0; i < p.N_t; i++) {
         c.xd[i] = x[i]; c.wd[i] = w[i];
-        c.xf[i] = (float)x[i]; c.wf[i] = (float)w[i];
+    }
+    c.Nt2 = (p.N_t + 1) / 2;
+    for (int m = 0; m < c.Nt2; m++) {
+        const int a = 2 * m, b = 2 * m + 1;
+        c.xf2[m] = make_float2((float)x[a], b < p.N_t ? (float)x[b] : -1.0f);
+        c.wf2[m] = make_float2((float)w[a], b < p.N_t ? (float)w[b] : 0.0f);
     }
     // in-plane cells of side >= r_cutoff
     CellGeom &g = h->geom;

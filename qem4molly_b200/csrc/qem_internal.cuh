@@ -31,7 +31,12 @@ struct ShortConsts {
     int n_walls;
     int pad;
     double wall_cut[2], wall_sig2[2], wall_eps[2], wall_pos[2], wall_dir[2];
-    float xf[QEM_MAX_NT], wf[QEM_MAX_NT];   // Gauss-Legendre nodes/weights on [-1, 1]
+    // Gauss-Legendre nodes/weights on [-1, 1]: FP32 as node pairs (2m, 2m+1)
+    // for the packed FP32x2 loop, an odd N_t padded with (x = -1, w = 0),
+    // i.e. a node at k = 0 of weight zero; FP64 as plain arrays
+    int Nt2;              // (N_t + 1) / 2
+    int pad2;
+    float2 xf2[QEM_MAX_NT / 2], wf2[QEM_MAX_NT / 2];
     double xd[QEM_MAX_NT], wd[QEM_MAX_NT];
 };
 
@@ -131,58 +136,122 @@ __device__ __forceinline__ double jl_sign(double v) { return (double)((v > 0) - 
 
 __device__ __forceinline__ double min_image(double d, double L, double invL) { return d - L * rint(d * invL); }
 
-// Bessel J0 and J1 in FP32 from the polynomial approximations of
-// Abramowitz & Stegun, Handbook of Mathematical Functions, 9.4.1 / 9.4.4
-// (|x| <= 3) and 9.4.3 / 9.4.6 (x >= 3; modulus/phase form).  Published
-// absolute error <= 5e-8 (J0) and <= 4e-8 (J1), i.e. at FP32 rounding level.
-__device__ __forceinline__ void bessel01_f32(float x, float &J0, float &J1)
+// ---- packed FP32x2 arithmetic (sm_100: one instruction, two lanes) -------
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// 2^x (hardware approximation, denormal results flushed to zero)
+__device__ __forceinline__ float ex2_approx(float x)
 {
-    if (x < 3.0f) {
-        const float y = x * x * (1.0f / 9.0f);
-        J0 = fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, 0.0002100f, -0.0039444f), 0.0444479f), -0.3163866f),
-                                   1.2656208f), -2.2499997f), 1.0f);
-        J1 = x * fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, 0.00001109f, -0.00031761f), 0.00443319f),
-                                                -0.03954289f), 0.21093573f), -0.56249985f), 0.5f);
-    } else {
-        const float r = rsqrtf(x);
-        const float t = 3.0f * r * r;  // 3 / x
-        const float f0 = fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, 0.00014476f, -0.00072805f), 0.00137237f),
-                                                      -0.00009512f), -0.00552740f), -0.00000077f), 0.79788456f);
-        const float p0 = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, 0.00013558f, -0.00029333f), -0.00054125f),
-                                                 0.00262573f), -0.00003954f), -0.04166397f);
-        const float f1 = fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, -0.00020033f, 0.00113653f), -0.00249511f),
-                                                      0.00017105f), 0.01659667f), 0.00000156f), 0.79788456f);
-        const float p1 = t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, fmaf(t, -0.00029166f, 0.00079824f), 0.00074348f),
-                                                 -0.00637879f), 0.00005650f), 0.12499612f);
-        // theta = x - pi/4 + p0 and x - 3 pi/4 + p1, reduced modulo 2 pi in two
-        // FMA steps (Cody-Waite split of 2 pi) before the hardware cosine.
-        const float TWO_PI_HI = 6.28318548202514648f, TWO_PI_LO = -1.7484555314695172e-07f;
-        float th0 = (x - 0.78539816f) + p0;
-        float th1 = (x - 2.35619449f) + p1;
-        float n0 = rintf(th0 * 0.15915494309189535f), n1 = rintf(th1 * 0.15915494309189535f);
-        th0 = fmaf(-n0, TWO_PI_LO, fmaf(-n0, TWO_PI_HI, th0));
-        th1 = fmaf(-n1, TWO_PI_LO, fmaf(-n1, TWO_PI_HI, th1));
-        J0 = f0 * r * __cosf(th0);
-        J1 = f1 * r * __cosf(th1);
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float cos_ftz(float x)
+{
+    float r;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Bessel J0 and J1 in FP32 at two arguments x = (x0, x1) at once, one per
+// packed lane, from the polynomial approximations of Abramowitz & Stegun,
+// Handbook of Mathematical Functions, 9.4.1 / 9.4.4 (|x| <= 3) and 9.4.3 /
+// 9.4.6 (x >= 3; modulus/phase form); published absolute error <= 5e-8 (J0)
+// and <= 4e-8 (J1), i.e. at FP32 rounding level.  The coefficients are
+// rescaled so the small-x series run in y = x^2 (A&S use (x/3)^2) and the
+// large-x series in u = 1/x (A&S use 3/x).  A branch runs when either lane
+// needs it and each lane keeps its own branch's result.  Large-x phases
+// theta0,1 = x - (pi/4, 3 pi/4) + (p0, p1) are reduced modulo 2 pi by
+// n = round(theta / 2 pi) (adding and subtracting 1.5 * 2^23, valid while
+// |theta| / 2 pi < 2^22) and a two-term Cody-Waite split of 2 pi.
+namespace bj {
+__host__ __device__ constexpr float s9(double c, int j) { return (float)(c / (j == 0 ? 1.0 : j == 1 ? 9.0 : j == 2 ? 81.0 : j == 3 ? 729.0 : j == 4 ? 6561.0 : j == 5 ? 59049.0 : 531441.0)); }
+__host__ __device__ constexpr float s3(double c, int j) { return (float)(c * (j == 0 ? 1.0 : j == 1 ? 3.0 : j == 2 ? 9.0 : j == 3 ? 27.0 : j == 4 ? 81.0 : j == 5 ? 243.0 : 729.0)); }
+}  // namespace bj
+
+__device__ __forceinline__ void bessel01_x2(float2 x, float2 &J0, float2 &J1)
+{
+    using namespace bj;
+    const bool s0 = x.x < 3.0f, s1 = x.y < 3.0f;
+    if (s0 || s1) {
+        const float2 y = mul2(x, x);
+        float2 a = fma2(y, f2s(s9(0.0002100, 6)), f2s(s9(-0.0039444, 5)));
+        a = fma2(y, a, f2s(s9(0.0444479, 4)));
+        a = fma2(y, a, f2s(s9(-0.3163866, 3)));
+        a = fma2(y, a, f2s(s9(1.2656208, 2)));
+        a = fma2(y, a, f2s(s9(-2.2499997, 1)));
+        J0 = fma2(y, a, f2s(1.0f));
+        float2 b = fma2(y, f2s(s9(0.00001109, 6)), f2s(s9(-0.00031761, 5)));
+        b = fma2(y, b, f2s(s9(0.00443319, 4)));
+        b = fma2(y, b, f2s(s9(-0.03954289, 3)));
+        b = fma2(y, b, f2s(s9(0.21093573, 2)));
+        b = fma2(y, b, f2s(s9(-0.56249985, 1)));
+        J1 = mul2(x, fma2(y, b, f2s(0.5f)));
+    }
+    if (!(s0 && s1)) {
+        const float2 r = f2(rsqrt_ftz(x.x), rsqrt_ftz(x.y));
+        const float2 u = mul2(r, r);  // 1 / x
+        float2 f = fma2(u, f2s(s3(0.00014476, 6)), f2s(s3(-0.00072805, 5)));
+        f = fma2(u, f, f2s(s3(0.00137237, 4)));
+        f = fma2(u, f, f2s(s3(-0.00009512, 3)));
+        f = fma2(u, f, f2s(s3(-0.00552740, 2)));
+        f = fma2(u, f, f2s(s3(-0.00000077, 1)));
+        f = fma2(u, f, f2s(0.79788456f));
+        float2 g = fma2(u, f2s(s3(-0.00020033, 6)), f2s(s3(0.00113653, 5)));
+        g = fma2(u, g, f2s(s3(-0.00249511, 4)));
+        g = fma2(u, g, f2s(s3(0.00017105, 3)));
+        g = fma2(u, g, f2s(s3(0.01659667, 2)));
+        g = fma2(u, g, f2s(s3(0.00000156, 1)));
+        g = fma2(u, g, f2s(0.79788456f));
+        // phase corrections p = t P(t), t = 3u: u (3^(j+1) c_j) u^j
+        float2 p = fma2(u, f2s(s3(0.00013558, 6)), f2s(s3(-0.00029333, 5)));
+        p = fma2(u, p, f2s(s3(-0.00054125, 4)));
+        p = fma2(u, p, f2s(s3(0.00262573, 3)));
+        p = fma2(u, p, f2s(s3(-0.00003954, 2)));
+        p = fma2(u, p, f2s(s3(-0.04166397, 1)));
+        float2 q = fma2(u, f2s(s3(-0.00029166, 6)), f2s(s3(0.00079824, 5)));
+        q = fma2(u, q, f2s(s3(0.00074348, 4)));
+        q = fma2(u, q, f2s(s3(-0.00637879, 3)));
+        q = fma2(u, q, f2s(s3(0.00005650, 2)));
+        q = fma2(u, q, f2s(s3(0.12499612, 1)));
+        float2 th0 = fma2(u, p, add2(x, f2s(-0.78539816f)));
+        float2 th1 = fma2(u, q, add2(x, f2s(-2.35619449f)));
+        const float2 MAGIC = f2s(12582912.0f), INV2PI = f2s(0.15915494309189535f);
+        const float2 n0 = add2(fma2(th0, INV2PI, MAGIC), f2s(-12582912.0f));
+        const float2 n1 = add2(fma2(th1, INV2PI, MAGIC), f2s(-12582912.0f));
+        th0 = fma2(n0, f2s(1.7484555314695172e-07f), fma2(n0, f2s(-6.28318548202514648f), th0));
+        th1 = fma2(n1, f2s(1.7484555314695172e-07f), fma2(n1, f2s(-6.28318548202514648f), th1));
+        const float2 L0 = mul2(mul2(f, r), f2(cos_ftz(th0.x), cos_ftz(th0.y)));
+        const float2 L1 = mul2(mul2(g, r), f2(cos_ftz(th1.x), cos_ftz(th1.y)));
+        if (!s0) { J0.x = L0.x; J1.x = L1.x; }
+        if (!s1) { J0.y = L0.y; J1.y = L1.y; }
     }
 }
 
-// 1 - exp(-t) for t >= 0 to FP32 relative precision without cancellation:
-// Taylor series below 0.5 (truncation < 2e-8 relative), 1 - exp(-t) above.
-__device__ __forceinline__ float one_minus_exp_neg(float t, float e)
+// packed 1 - exp(-t) by its Taylor series, for 0 <= t < 0.5 (truncation
+// < 2e-8 relative)
+__device__ __forceinline__ float2 one_minus_exp_neg_series(float2 t)
 {
-    if (t < 0.5f) {
-        float s = fmaf(t, -1.0f / 362880.0f, 1.0f / 40320.0f);
-        s = fmaf(t, s, -1.0f / 5040.0f);
-        s = fmaf(t, s, 1.0f / 720.0f);
-        s = fmaf(t, s, -1.0f / 120.0f);
-        s = fmaf(t, s, 1.0f / 24.0f);
-        s = fmaf(t, s, -1.0f / 6.0f);
-        s = fmaf(t, s, 0.5f);
-        s = fmaf(t, -s, 1.0f);
-        return t * s;
-    }
-    return 1.0f - e;
+    float2 s = fma2(t, f2s(-1.0f / 362880.0f), f2s(1.0f / 40320.0f));
+    s = fma2(t, s, f2s(-1.0f / 5040.0f));
+    s = fma2(t, s, f2s(1.0f / 720.0f));
+    s = fma2(t, s, f2s(-1.0f / 120.0f));
+    s = fma2(t, s, f2s(1.0f / 24.0f));
+    s = fma2(t, s, f2s(-1.0f / 6.0f));
+    s = fma2(t, s, f2s(0.5f));
+    s = fma2(t, mul2(s, f2s(-1.0f)), f2s(1.0f));
+    return mul2(t, s);
 }
 
 __device__ __forceinline__ float fast_rcp(float x)

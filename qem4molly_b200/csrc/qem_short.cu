@@ -29,7 +29,10 @@
 // FP32 path: per-pair set-up (minimum image, rho, image distances, quadrature
 // limits, closed-form image terms) and all cross-image sums in FP64; the
 // per-node integrands in FP32 with hardware exp / rcp / cos and the
-// Abramowitz-Stegun Bessel approximations.  The denominator D is formed as
+// Abramowitz-Stegun Bessel approximations, two nodes per packed FP32x2
+// instruction (the kernel is instruction-issue bound, and the packed
+// arithmetic halves the issue slots of everything but the MUFU operations).
+// The denominator D is formed as
 // (1 - g_u g_d) + g_u g_d (1 - e^{-t}) with (1 - g_u g_d) from FP64 and
 // 1 - e^{-t} evaluated without cancellation, so its relative error stays at
 // FP32 rounding as |g_u g_d| -> 1.
@@ -109,29 +112,52 @@ __device__ __forceinline__ void quad_f64(const ShortConsts &c, const Interval &v
     Ir = r; Iz = z; Iu = u;
 }
 
+// FP32 nodes two at a time in packed FP32x2 lanes (nodes 2m, 2m+1, Bessel
+// functions included); the exponentials as 2^(...) with log2(e) folded into
+// the per-interval constants; 1 - e^{-t} by its series below t = 0.5; the
+// two lanes' partial sums are added at the end.
 template <bool ENERGY, bool WITH_J1>
 __device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, float rho, float &Ir, float &Iz,
                                          float &Iu)
 {
-    const float h = 0.5f * (float)v.K;
-    const float ae = (float)v.ae, c2 = (float)v.c2, pf = (float)v.pf;
-    const float twoLz = (float)c.twoLz, g12 = (float)c.g12, omg = (float)c.one_minus_g12;
-    float r = 0.f, z = 0.f, u = 0.f;
+    constexpr double LOG2E = 1.4426950408889634;
+    const float2 h = f2s(0.5f * (float)v.K);
+    const float2 ae = f2s((float)(-LOG2E * v.ae)), c2 = f2s((float)(-LOG2E * v.c2)), pf = f2s((float)v.pf);
+    const float2 nt = f2s((float)(-LOG2E * c.twoLz));  // e^{-t} = 2^(k nt)
+    const float2 g12 = f2s((float)c.g12), omg = f2s((float)c.one_minus_g12);
+    const float2 rho2 = f2s(rho), twoLz = f2s((float)c.twoLz);
+    const float tsmall = (float)(-0.5 * LOG2E);         // k nt > tsmall  <=>  t < 0.5
+    float2 r = f2s(0.f), z = f2s(0.f), u = f2s(0.f);
 #pragma unroll NODE_UNROLL
-    for (int n = 0; n < c.Nt; n++) {
-        const float k = fmaf(h, c.xf[n], h);
-        const float w = h * c.wf[n];
-        const float t = k * twoLz;
-        const float Dp = fmaf(g12, one_minus_exp_neg(t, __expf(-t)), omg);  // 1 - g12 e^{-t} > 0
-        const float G = pf * __expf(-k * fmaf(k, c2, ae)) * fast_rcp(Dp);
-        float J0 = 1.0f, J1 = 0.0f;
-        if (WITH_J1) bessel01_f32(k * rho, J0, J1);
-        const float cw = w * k * G;
-        if (WITH_J1) r = fmaf(cw, J1, r);
-        z = fmaf(cw, J0, z);
-        if (ENERGY) u = fmaf(w * G, J0, u);
+    for (int m = 0; m < c.Nt2; m++) {
+        const float2 k = fma2(h, c.xf2[m], h);
+        const float2 w = mul2(h, c.wf2[m]);
+        const float2 s = mul2(k, nt);
+        float2 om = fma2(f2(ex2_approx(s.x), ex2_approx(s.y)), f2s(-1.0f), f2s(1.0f));  // 1 - e^{-t}
+        if (s.x > tsmall) {  // nodes ascend, so lane x holds the smaller k
+            const float2 t = mul2(k, twoLz);
+            const float2 tay = one_minus_exp_neg_series(t);
+            if (t.x < 0.5f) om.x = tay.x;
+            if (t.y < 0.5f) om.y = tay.y;
+        }
+        const float2 Dp = fma2(g12, om, omg);  // 1 - g12 e^{-t} > 0
+        const float2 ex = mul2(k, fma2(k, c2, ae));
+        const float2 G = mul2(mul2(pf, f2(ex2_approx(ex.x), ex2_approx(ex.y))),
+                              f2(fast_rcp(Dp.x), fast_rcp(Dp.y)));
+        const float2 wG = mul2(w, G);
+        const float2 cw = mul2(wG, k);
+        if (WITH_J1) {
+            float2 J0, J1;
+            bessel01_x2(mul2(k, rho2), J0, J1);
+            r = fma2(cw, J1, r);
+            z = fma2(cw, J0, z);
+            if (ENERGY) u = fma2(wG, J0, u);
+        } else {
+            z = add2(z, cw);
+            if (ENERGY) u = add2(u, wG);
+        }
     }
-    Ir = r; Iz = z; Iu = u;
+    Ir = r.x + r.y; Iz = z.x + z.y; Iu = u.x + u.y;
 }
 
 template <int PREC, bool ENERGY, bool WITH_J1>
