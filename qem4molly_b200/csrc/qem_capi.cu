@@ -135,7 +135,7 @@ struct qem_handle {
     // device scratch
     DevBuf xyz, q, F, pos, cell, cell_cnt, cell_start, cell_fill, cell_list, pos_of, pcount, poff, pairs, R, Upair,
         in_cnt, in_off, in_fill, in_list, scan_tmp;
-    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, tot, off, Utot, Epart, status,
+    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, tot, off, Utot, kf, Epart, status,
         Eout, Fpart, pos_c;
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
@@ -403,6 +403,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         CU(grow(h->off, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
         CU(grow(h->Fpart, sizeof(double) * 3 * (size_t)ks * N));
         CU(grow(h->Utot, sizeof(double) * 4 * std::max(Pk, 1)));
+        CU(grow(h->kf, sizeof(KForce<double>) * std::max(Pk, 1)));
         CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
         CU(grow(h->Flong, sizeof(double) * 3 * N));
         if (concurrent) {  // fork after pack (positions) and the energy-partial clear
@@ -425,6 +426,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
         b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
         b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
+        b.kf = h->kf.p;
         b.Epart = Ep + nbS;
         b.Eks = Ep + nbS + (size_t)ks * nch + nb0;
         b.Fpart = ptr<double>(h->Fpart);
@@ -627,7 +629,7 @@ void qem_destroy(qem_handle *h)
                       &h->cell_list, &h->pos_of, &h->pcount, &h->poff, &h->pairs, &h->R, &h->Upair, &h->in_cnt,
                       &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
                       &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin,
-                      &h->tot, &h->off, &h->Utot, &h->Epart, &h->status, &h->Eout, &h->Fpart,
+                      &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);

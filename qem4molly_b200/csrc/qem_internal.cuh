@@ -58,6 +58,16 @@ struct KConst {
     double ek;              // energy weight -(sum_K / P) / (2 eps_0 Lx Ly) / k
 };
 
+// Per-k constants of the long-range force pass in its own precision
+// (written by the chunk-scan kernel from the structure-sum totals):
+// S1 = g e^{-k L_z} (g2 U + g12 e^{-k L_z} V), S2 = g e^{-k L_z} (g12 e^{-k L_z} U + g1 V)
+// with U, V the totals of q e^{+-k(z-h)} e^{i k.rho} and g from KConst.
+template <typename Real>
+struct KForce {
+    Real k, wfx, wfy, wk;       // k, w_k kx / k, w_k ky / k, w_k
+    Real s1r, s1i, s2r, s2i;
+};
+
 // ---------------------------------------------------------------------------
 // host-side launch wrappers (defined in the .cu files)
 // ---------------------------------------------------------------------------
@@ -106,7 +116,9 @@ struct LongBuffers {
     KConst *kc;           // P per-k constants
     double *kin;          // P x 3 (kx, ky, k) FP64
     double *tot;          // P x nch x 4 chunk totals
-    double *off;          // P x nch x 4 chunk offsets (u from below, v from above)
+    double *off;          // P x nch x 4 chunk offsets (u from below, v from above), stored
+                          // as float in the FP32 path
+    void *kf;             // P KForce<float | double> force constants
     double *Utot;         // P x 4 global totals
     double *Eks;          // P per-k split energy term
     double *Epart;        // per-block energy partials (ks * nch + nb0 entries)

@@ -38,6 +38,11 @@ constexpr int PPT = 4;          // particles per thread
 constexpr int LCH = LT * PPT;   // particles per chunk
 constexpr int NW = LT / 32;     // warps per block
 constexpr int KPB = 16;         // k-vectors per block in the totals pass
+constexpr int LKB = 8;          // k-vectors per FP32 accumulation batch of the force pass
+#ifndef QEM_LF_MINB
+#define QEM_LF_MINB 6
+#endif
+constexpr int LF_MINB = QEM_LF_MINB;  // resident FP32 force-pass blocks per SM (register budget)
 
 template <typename Real>
 struct LM;
@@ -182,16 +187,18 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
     }
 }
 
-// one warp per k: exclusive scans of the chunk totals (FP64)
-__global__ void k_lscan(int P, int nch, const double *__restrict__ tot, double *__restrict__ off,
+// one warp per k: exclusive scans of the chunk totals (FP64), written in the
+// force pass's precision, and the per-k force constants
+template <typename Real>
+__global__ void k_lscan(int P, int nch, const double *__restrict__ tot, Real *__restrict__ off,
                         double *__restrict__ Utot, const KConst *__restrict__ kc, double g1, double g2,
-                        double *__restrict__ Eks)
+                        double *__restrict__ Eks, KForce<Real> *__restrict__ kf)
 {
     const int lane = threadIdx.x & 31;
     const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (m >= P) return;
     const double *T = tot + (int64_t)m * nch * 4;
-    double *O = off + (int64_t)m * nch * 4;
+    Real *O = off + (int64_t)m * nch * 4;
     double cr = 0, ci = 0;  // forward carry: u below
     for (int base = 0; base < nch; base += 32) {
         const int c = base + lane;
@@ -203,7 +210,7 @@ __global__ void k_lscan(int P, int nch, const double *__restrict__ tot, double *
         }
         double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
         if (lane == 0) { er = 0; ei = 0; }
-        if (c < nch) { O[4 * c] = cr + er; O[4 * c + 1] = ci + ei; }
+        if (c < nch) { O[4 * c] = (Real)(cr + er); O[4 * c + 1] = (Real)(ci + ei); }
         cr += __shfl_sync(0xffffffffu, r, 31);
         ci += __shfl_sync(0xffffffffu, i, 31);
     }
@@ -218,7 +225,7 @@ __global__ void k_lscan(int P, int nch, const double *__restrict__ tot, double *
         }
         double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
         if (lane == 0) { er = 0; ei = 0; }
-        if (c >= 0) { O[4 * c + 2] = dr + er; O[4 * c + 3] = di + ei; }
+        if (c >= 0) { O[4 * c + 2] = (Real)(dr + er); O[4 * c + 3] = (Real)(di + ei); }
         dr += __shfl_sync(0xffffffffu, r, 31);
         di += __shfl_sync(0xffffffffu, i, 31);
     }
@@ -227,22 +234,48 @@ __global__ void k_lscan(int P, int nch, const double *__restrict__ tot, double *
         Utot[4 * m + 1] = ci;
         Utot[4 * m + 2] = dr;
         Utot[4 * m + 3] = di;
-        // split energy term Sigma_Gamma_func_s (Sigma_Gamma_func_njit.py:8-28) in scaled sums
         const KConst K = kc[m];
-        const double W = K.W * K.W;
+        const double W = K.W * K.W;  // e^{-k L_z}
+        // split energy term Sigma_Gamma_func_s (Sigma_Gamma_func_njit.py:8-28) in scaled sums
         const double sig = K.g * (g2 * W * (cr * cr + ci * ci) + g1 * W * (dr * dr + di * di) +
                                   g1 * g2 * W * W * (cr * dr + ci * di));
         Eks[m] = K.ek * sig;
+        // force constants: S1 = g W (g2 U + g12 W V), S2 = g W (g12 W U + g1 V)
+        const double gW = K.g * W, g12W = g1 * g2 * W;
+        KForce<Real> F;
+        F.k = (Real)K.k;
+        F.wfx = (Real)(K.wk * K.fx);
+        F.wfy = (Real)(K.wk * K.fy);
+        F.wk = (Real)K.wk;
+        F.s1r = (Real)(gW * (g2 * cr + g12W * dr));
+        F.s1i = (Real)(gW * (g2 * ci + g12W * di));
+        F.s2r = (Real)(gW * (g12W * cr + g1 * dr));
+        F.s2i = (Real)(gW * (g12W * ci + g1 * di));
+        kf[m] = F;
     }
 }
 
+// Force pass.  For particle j with phase e^{i theta} = c + i s, ep = e^{k(z-h)},
+// em = e^{-k(z-h)}, prefix A = sum_{below} q ep e^{i theta} and suffix
+// C = sum_{above} q em e^{i theta} (complex), the reference's per-k terms
+// (Force_long.jl:39-64 Fl_non_sort with the particle's own term removed,
+// 103-121 Fl_sort, 180 Flz_self) sum to
+//   F_xy = w_k q Im[e^{-i theta} X1],  F_z = w_k q Re[e^{-i theta} X2],
+//   X1 = ep a + em b,  X2 = ep a - em b,  a = S1 - C / 2,  b = S2 - A / 2,
+// with the per-k constants S1, S2 of k_lscan: the own-term removal of the
+// non-sorted sum only changes the real part, and there it cancels the self
+// image force exactly.  The sums over k run in Real in batches of KB
+// k-vectors, each batch added into FP64; the common factor q is applied at
+// the end.  Slices and batches cover whole groups of LKB consecutive k, so
+// the batches are the same for every number of slices.
 template <typename Real, bool ENERGY>
-__global__ void __launch_bounds__(LT) k_lforce(int N, int P, int nch, int ks_n, const double *__restrict__ zx,
-                                               const double *__restrict__ zy, const Real *__restrict__ zh,
-                                               const Real *__restrict__ qv, const KConst *__restrict__ kc,
-                                               const double *__restrict__ off, const double *__restrict__ Utot,
-                                               double g1, double g2, double *__restrict__ Fpart,
-                                               double *__restrict__ Epart)
+__global__ void __launch_bounds__(LT, sizeof(Real) == 4 ? LF_MINB : 4) k_lforce(int N, int P, int nch, int ks_n,
+                                                       const double *__restrict__ zx, const double *__restrict__ zy,
+                                                       const Real *__restrict__ zh, const Real *__restrict__ qv,
+                                                       const KConst *__restrict__ kc,
+                                                       const KForce<Real> *__restrict__ kf,
+                                                       const Real *__restrict__ off, double *__restrict__ Fpart,
+                                                       double *__restrict__ Epart)
 {
     __shared__ Real wsh[2][4][NW];  // [buffer][fwd re, fwd im, bwd re, bwd im][warp]
     __shared__ double ered[NW];
@@ -251,26 +284,30 @@ __global__ void __launch_bounds__(LT) k_lforce(int N, int P, int nch, int ks_n, 
     P4.load(N, m0, zx, zy, zh, qv);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ks = blockIdx.y;
-    const int kb = (int)((int64_t)P * ks / ks_n), ke = (int)((int64_t)P * (ks + 1) / ks_n);
-    const Real G1 = (Real)g1, G2 = (Real)g2, G12 = (Real)(g1 * g2);
+    const int ng = (P + LKB - 1) / LKB;
+    const int kb = LKB * (int)((int64_t)ng * ks / ks_n);
+    const int ke = min(P, LKB * (int)((int64_t)ng * (ks + 1) / ks_n));
     double Fx[PPT], Fy[PPT], Fz[PPT];
+    Real bx[PPT], by[PPT], bz[PPT];
 #pragma unroll
-    for (int j = 0; j < PPT; j++) { Fx[j] = 0; Fy[j] = 0; Fz[j] = 0; }
+    for (int j = 0; j < PPT; j++) { Fx[j] = 0; Fy[j] = 0; Fz[j] = 0; bx[j] = 0; by[j] = 0; bz[j] = 0; }
     double E = 0;
     for (int kidx = kb; kidx < ke; kidx++) {
-        const KConst K = kc[kidx];
+        const double kx2 = kc[kidx].kx_2pi, ky2 = kc[kidx].ky_2pi;
+        const KForce<Real> K = kf[kidx];
         const int buf = (kidx - kb) & 1;
         Real c[PPT], s[PPT], ep[PPT], em[PPT], ur[PPT], ui[PPT], vr[PPT], vi[PPT];
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
-            double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
+            double t = fma(kx2, P4.x[j], ky2 * P4.y[j]);
             t -= rint(t);
             LM<Real>::sc(t, s[j], c[j]);
-            const Real kz = (Real)K.k * P4.z[j];
+            const Real kz = K.k * P4.z[j];
             ep[j] = LM<Real>::ex(kz);
             em[j] = LM<Real>::ex(-kz);
-            ur[j] = P4.q[j] * ep[j] * c[j]; ui[j] = P4.q[j] * ep[j] * s[j];
-            vr[j] = P4.q[j] * em[j] * c[j]; vi[j] = P4.q[j] * em[j] * s[j];
+            const Real qp = P4.q[j] * ep[j], qm = P4.q[j] * em[j];
+            ur[j] = qp * c[j]; ui[j] = qp * s[j];
+            vr[j] = qm * c[j]; vi[j] = qm * s[j];
         }
         // in-thread exclusive prefix (u, from below) and suffix (v, from above)
         Real Ar[PPT], Ai[PPT], Cr[PPT], Ci[PPT];
@@ -301,49 +338,44 @@ __global__ void __launch_bounds__(LT) k_lforce(int N, int P, int nch, int ks_n, 
             if (ww < w) { xr += wsh[buf][0][ww]; xi += wsh[buf][1][ww]; }
             if (ww > w) { yr += wsh[buf][2][ww]; yi += wsh[buf][3][ww]; }
         }
-        const double *O = off + ((int64_t)kidx * nch + blockIdx.x) * 4;
-        const double *U = Utot + 4 * kidx;
-        const Real bAr = (Real)O[0] + xr, bAi = (Real)O[1] + xi;
-        const Real bCr = (Real)O[2] + yr, bCi = (Real)O[3] + yi;
-        const Real U0 = (Real)U[0], U1 = (Real)U[1], U2 = (Real)U[2], U3 = (Real)U[3];
-        const Real Wh = (Real)K.W, Wf = Wh * Wh, g = (Real)K.g, wk = (Real)K.wk;
-        const Real fx = (Real)K.fx, fy = (Real)K.fy;
+        const Real *O = off + ((int64_t)kidx * nch + blockIdx.x) * 4;
+        const Real bAr = O[0] + xr, bAi = O[1] + xi, bCr = O[2] + yr, bCi = O[3] + yi;
+        const double ek = ENERGY ? kc[kidx].ek : 0.0;
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
-            const Real q = P4.q[j];
-            // prefix (A, B) of particles below and suffix (C, D) of particles above,
-            // scaled: A' = sum q e^{k(z-h)} cos, C' = sum q e^{-k(z-h)} cos
-            const Real A = bAr + Ar[j], B = bAi + Ai[j], Cs = bCr + Cr[j], Ds = bCi + Ci[j];
-            // totals with the particle's own term removed (Force_long.jl:33-36)
-            const Real f1 = U0 - ur[j], f2 = U1 - ui[j], f3 = U2 - vr[j], f4 = U3 - vi[j];
-            const Real Xp = (Wh * ep[j]) * Wh, Xm = (Wh * em[j]) * Wh;  // e^{-kLz} e^{+-k(z-h)}
-            const Real Yp = Xp * Wf, Ym = Xm * Wf;                      // e^{-2kLz} e^{+-k(z-h)}
-            // Fl_non_sort (Force_long.jl:39-64)
-            const Real P1 = G2 * Xp + G12 * Ym, P2 = G1 * Xm + G12 * Yp;
-            const Real Q1 = G2 * Xp - G12 * Ym, Q2 = G12 * Yp - G1 * Xm;
-            const Real xy_ns = q * g * (c[j] * (P1 * f2 + P2 * f4) - s[j] * (P1 * f1 + P2 * f3));
-            const Real z_ns = q * g * (c[j] * (Q1 * f1 + Q2 * f3) + s[j] * (Q1 * f2 + Q2 * f4));
-            // Fl_sort (Force_long.jl:103-121)
-            const Real xy_s = em[j] * (s[j] * A - c[j] * B) + ep[j] * (s[j] * Cs - c[j] * Ds);
-            const Real cAB = c[j] * A + s[j] * B, cCD = c[j] * Cs + s[j] * Ds;
-            const Real z_s = (Real)0.5 * q * (em[j] * cAB - ep[j] * cCD);
-            // Flz_self (Force_long.jl:180)
-            const Real z_self = q * q * g * (G2 * Xp * ep[j] - G1 * Xm * em[j]);
-            const Real xy = wk * (xy_ns + (Real)0.5 * q * xy_s);
-            Fx[j] += (double)(fx * xy);
-            Fy[j] += (double)(fy * xy);
-            Fz[j] += (double)(wk * (z_ns + z_s + z_self));
-            if (ENERGY) E += K.ek * 0.5 * (double)(-q * q - q * (em[j] * cAB + ep[j] * cCD));
+            const Real A_r = bAr + Ar[j], A_i = bAi + Ai[j], C_r = bCr + Cr[j], C_i = bCi + Ci[j];
+            const Real ar = K.s1r - (Real)0.5 * C_r, ai = K.s1i - (Real)0.5 * C_i;
+            const Real br_ = K.s2r - (Real)0.5 * A_r, bi_ = K.s2i - (Real)0.5 * A_i;
+            const Real pr = ep[j] * ar, pi = ep[j] * ai, mr = em[j] * br_, mi = em[j] * bi_;
+            const Real im1 = c[j] * (pi + mi) - s[j] * (pr + mr);  // Im[e^{-i theta} X1]
+            const Real re2 = c[j] * (pr - mr) + s[j] * (pi - mi);  // Re[e^{-i theta} X2]
+            bx[j] += K.wfx * im1;
+            by[j] += K.wfy * im1;
+            bz[j] += K.wk * re2;
+            if (ENERGY) {
+                // Energy_long_range_njit.py:10-24 (sorted part), Re[e^{-i theta}(em A + ep C)]
+                const Real q = P4.q[j];
+                const Real zr = em[j] * A_r + ep[j] * C_r, zi = em[j] * A_i + ep[j] * C_i;
+                E += ek * 0.5 * (double)(-q * q - q * (c[j] * zr + s[j] * zi));
+            }
+        }
+        if ((kidx + 1) % LKB == 0) {
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
+                Fx[j] += (double)bx[j]; Fy[j] += (double)by[j]; Fz[j] += (double)bz[j];
+                bx[j] = 0; by[j] = 0; bz[j] = 0;
+            }
         }
     }
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int m = m0 + j;
         if (m < N) {
+            const double q = (double)P4.q[j];
             double *o = Fpart + ((int64_t)ks * N + m) * 3;
-            o[0] = Fx[j];
-            o[1] = Fy[j];
-            o[2] = Fz[j];
+            o[0] = q * (Fx[j] + (double)bx[j]);
+            o[1] = q * (Fy[j] + (double)by[j]);
+            o[2] = q * (Fz[j] + (double)bz[j]);
         }
     }
     if (ENERGY) {
@@ -409,7 +441,7 @@ int qem_long_ksplit(int nch, int P, int max_ks)
 {
     int ks = (4 * 148 + nch - 1) / nch;  // enough blocks for every SM
     ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
-    const int pm = P > 1 ? P : 1;
+    const int pm = P > LKB ? (P + LKB - 1) / LKB : 1;  // at most one slice per k group
     return ks < pm ? ks : pm;
 }
 
@@ -439,25 +471,33 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
                 k_ltot<float><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
-            k_lscan<<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks);
+            if (precision == QEM_FP64)
+                k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
+                                                           (KForce<double> *)b.kf);
+            else
+                k_lscan<float><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, (float *)b.off, b.Utot, b.kc, g1, g2,
+                                                          b.Eks, (KForce<float> *)b.kf);
         }
         return cudaGetLastError();
     }
     dim3 gf(nch, b.ks);
     if (precision == QEM_FP64) {
+        const KForce<double> *kf = (const KForce<double> *)b.kf;
         if (energy)
-            k_lforce<double, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot,
-                                                     g1, g2, b.Fpart, b.Epart);
+            k_lforce<double, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, kf, b.off,
+                                                     b.Fpart, b.Epart);
         else
-            k_lforce<double, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.off, b.Utot,
-                                                      g1, g2, b.Fpart, b.Epart);
+            k_lforce<double, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhd, b.qd, b.kc, kf, b.off,
+                                                      b.Fpart, b.Epart);
     } else {
+        const KForce<float> *kf = (const KForce<float> *)b.kf;
+        const float *of = (const float *)b.off;
         if (energy)
-            k_lforce<float, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot,
-                                                    g1, g2, b.Fpart, b.Epart);
+            k_lforce<float, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of,
+                                                    b.Fpart, b.Epart);
         else
-            k_lforce<float, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, b.off, b.Utot,
-                                                     g1, g2, b.Fpart, b.Epart);
+            k_lforce<float, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of,
+                                                     b.Fpart, b.Epart);
     }
     k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3);
     return cudaGetLastError();

@@ -50,7 +50,8 @@ constexpr size_t O_KC = O_KIN + al(sizeof(double) * 3 * NA_MAX_P);
 constexpr size_t O_TOT = O_KC + al(sizeof(KConst) * NA_MAX_P);
 constexpr size_t O_OFF = O_TOT + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
 constexpr size_t O_UTOT = O_OFF + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
-constexpr size_t O_FPART = O_UTOT + al(sizeof(double) * 4 * NA_MAX_P);
+constexpr size_t O_KF = O_UTOT + al(sizeof(double) * 4 * NA_MAX_P);
+constexpr size_t O_FPART = O_KF + al(sizeof(KForce<double>) * NA_MAX_P);
 constexpr size_t O_EPART = O_FPART + al(sizeof(double) * 3 * (size_t)NA_MAX_KS * NA_MAX_N);
 constexpr size_t N_EPART = NA_MAX_KS * NA_MAX_NCH + (NA_MAX_N + 255) / 256 + NA_MAX_P + 8;
 constexpr size_t O_STMP = O_EPART + al(sizeof(double) * N_EPART);
@@ -136,6 +137,7 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     b.k0 = (double *)(S + O_K0); b.qscan = (double *)(S + O_QSCAN);
     b.kc = (KConst *)(S + O_KC); b.kin = (double *)(S + O_KIN);
     b.tot = (double *)(S + O_TOT); b.off = (double *)(S + O_OFF); b.Utot = (double *)(S + O_UTOT);
+    b.kf = S + O_KF;
     b.Epart = (double *)(S + O_EPART);
     const int nch = (N + NA_CH - 1) / NA_CH;
     b.ks = qem_long_ksplit(nch, P, NA_MAX_KS);
