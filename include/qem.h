@@ -163,6 +163,22 @@ qem_status qem_lj_forces(qem_handle *h, int32_t N, const double *xyz, double *F,
 qem_status qem_potential_energy(qem_handle *h, int32_t N, const double *xyz, const double *q, double *energy,
                                 uint32_t terms, int32_t mem, void *stream);
 
+/* Adjoint of qem_forces for L = gE * E + sum_i gF_i . F_i (the backward of the
+ * reference's python_lib autograd use; no reference counterpart in Julia):
+ *   gxyz   3N doubles, dL/dr_i                      (overwritten)
+ *   gq     N doubles or NULL, dL/dq_i               (overwritten)
+ *   ggamma 2 doubles or NULL, dL/dgamma_down, dL/dgamma_up
+ * gF: 3N doubles or NULL (zero).  Always evaluated in FP64, whatever the
+ * handle's precision, with the neighbour-list rules of the forward call and
+ * the handle's current k-set (a k-set is sampled if none exists; with
+ * QEM_RESAMPLE_KSET the backward uses the k-set of the latest forward call).
+ * The derivatives are those of the discretised quantities, so the
+ * quadrature limits' dependence on the image distances (Julia cutoff mode)
+ * is included; the k = 0 force is piecewise constant in z and contributes no
+ * dL/dz. */
+qem_status qem_backward(qem_handle *h, int32_t N, const double *xyz, const double *q, const double *gF, double gE,
+                        double *gxyz, double *gq, double *ggamma, uint32_t terms, int32_t mem, void *stream);
+
 /* Neighbour data of the last short-range build, for bit-exact checks.
  * qem_pair_list: (i, j) pairs with i < j, min-image rho <= r_cutoff
  * (CellListMap.neighborlist set, QEM_short.jl:35); writes min(cap, npairs)

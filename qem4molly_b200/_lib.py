@@ -87,6 +87,7 @@ def load(build: bool = False):
         "qem_long_forces": (C.c_int32, [H, C.c_int32, vp, vp, vp, C.c_int32, vp]),
         "qem_lj_forces": (C.c_int32, [H, C.c_int32, vp, vp, C.c_int32, vp]),
         "qem_potential_energy": (C.c_int32, [H, C.c_int32, vp, vp, dp, C.c_uint32, C.c_int32, vp]),
+        "qem_backward": (C.c_int32, [H, C.c_int32, vp, vp, vp, C.c_double, vp, vp, dp, C.c_uint32, C.c_int32, vp]),
         "qem_pair_list": (C.c_int32, [H, C.c_int32, dp, ip, C.c_int64, C.POINTER(C.c_int64)]),
         "qem_cell_index": (C.c_int32, [H, C.c_int32, dp, ip, ip, C.c_int32, ip, ip]),
         "qem_z_order": (C.c_int32, [H, C.c_int32, dp, ip]),

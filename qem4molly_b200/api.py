@@ -139,6 +139,44 @@ class Engine:
         self._check(st)
         return E.value if energy else None
 
+    def backward(self, xyz, q, gF=None, gE=0.0, terms=L.QEM_TERM_ALL):
+        """Adjoint of forces() for L = gE * E + sum_i gF_i . F_i (host arrays, FP64).
+
+        Returns (dL/dxyz (N x 3), dL/dq (N,), dL/d(gamma_1, gamma_2) (2,))."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+        if q.shape[0] != xyz.shape[0]:
+            raise ValueError("coords and charges differ in length")
+        g = None
+        if gF is not None:
+            g = np.ascontiguousarray(gF, dtype=np.float64).reshape(-1, 3)
+            if g.shape != xyz.shape:
+                raise ValueError("gF must be shaped like xyz")
+        gx = np.zeros_like(xyz)
+        gq = np.zeros_like(q)
+        gg = (C.c_double * 2)()
+        st = self._lib.qem_backward(self._h, xyz.shape[0], xyz.ctypes.data, q.ctypes.data,
+                                    g.ctypes.data if g is not None else None, float(gE), gx.ctypes.data,
+                                    gq.ctypes.data, gg, int(terms), L.QEM_MEM_HOST, None)
+        self._check(st)
+        return gx, gq, np.array([gg[0], gg[1]])
+
+    def backward_device(self, xyz, q, gF, gE, gxyz, gq=None, terms=L.QEM_TERM_ALL, stream=None):
+        """Device version of backward(): torch CUDA float64 tensors, gxyz / gq written in
+        place (gF and gq may be None); returns dL/d(gamma_1, gamma_2) as a numpy array."""
+        import torch
+
+        for t in (xyz, q, gF, gxyz, gq):
+            if t is not None and not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("device tensors must be contiguous float64 CUDA tensors")
+        s = stream if stream is not None else torch.cuda.current_stream(xyz.device).cuda_stream
+        gg = (C.c_double * 2)()
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        st = self._lib.qem_backward(self._h, q.shape[0], ptr(xyz), ptr(q), ptr(gF), float(gE), ptr(gxyz), ptr(gq),
+                                    gg, int(terms), L.QEM_MEM_DEVICE, C.c_void_p(s))
+        self._check(st)
+        return np.array([gg[0], gg[1]])
+
     def energy(self, xyz, q, terms=L.QEM_TERM_SHORT | L.QEM_TERM_LONG):
         return self.forces(xyz, q, terms=terms, energy=True)[1]
 

@@ -1,0 +1,329 @@
+// qem_adjoint.cu -- adjoint (reverse-mode) of the short-range QEM forces,
+// energies and Substrate_LJ walls.
+//
+// For L = gE * E + sum_i gF_i . F_i the pass returns dL/dr_i, dL/dq_i and
+// dL/d(gamma_down, gamma_up).  Each unordered pair's contributions
+// (Force_short.jl:25-78 forces, Energy_short_range_njit.py:34-63 energy) are
+// a function of (dx, dy, z_i, z_j, gamma_down, gamma_up) times q_i q_j: the
+// pair kernel evaluates them in FP64 on Dual<6> numbers, which gives the
+// exact Jacobian of the discretised pair terms (the quadrature limits of the
+// Julia cutoff mode move with the image distances, and that dependence is
+// included), and contracts it with the pair's cotangents
+//   (gF_i - gF_j).(F_x, F_y) + gF_i,z F_z,i + gF_j,z F_z,j + gE U_ij.
+// It writes one record per pair in the forward pass's (owner, other) layout;
+// a per-particle pass sums a particle's own and incoming records in a fixed
+// order, adds the self term (Force_short.jl:82-107, on Dual<3> numbers in
+// (z, gamma_down, gamma_up)) and the walls (Substrate_LJ.jl:19-46,
+// analytic), and reduces the gamma derivatives per block.  No atomics.
+#include "qem_dual.cuh"
+#include "qem_internal.cuh"
+
+namespace {
+
+constexpr int ADJ_BLOCK = 128;
+
+template <class T>
+__device__ __forceinline__ T point_limit_t(const ShortConsts &c, const T &a)
+{
+    if (c.flags & QEM_CUTOFF_PYTHON) return T(a * 0.0 + c.kf_point_py);
+    return sqrt(4.0 * c.alpha * c.alpha * (a * a) + 4.0 * c.alpha * c.neg_lnacc) - 2.0 * c.alpha * a;
+}
+template <class T>
+__device__ __forceinline__ T gauss_limit_t(const ShortConsts &c, const T &a)
+{
+    if (c.flags & QEM_CUTOFF_PYTHON) return T(a * 0.0 + c.kf_gauss_py);
+    return c.neg_lnacc / (a + c.twoLz);
+}
+
+// the FP64 quadrature of one interval (same nodes and integrand as the
+// forward pass): Ir = sum w k G J1, Iz = sum w k G J0, Iu = sum w G J0
+template <class T, bool WITH_J1>
+__device__ void quad_t(const ShortConsts &c, const T &K, const T &ae, double c2, const T &pf, const T &g12,
+                       const T &rho, T &Ir, T &Iz, T &Iu)
+{
+    const T h = 0.5 * K;
+    T r = h * 0.0, z = h * 0.0, u = h * 0.0;
+    for (int n = 0; n < c.Nt; n++) {
+        const T k = h * (1.0 + c.xd[n]);
+        const T w = h * c.wd[n];
+        const T D = 1.0 - g12 * exp(k * (-c.twoLz));
+        const T G = pf * exp(-(k * (ae + k * c2))) / D;
+        const T cw = w * k * G;
+        if (WITH_J1) {
+            T J0, J1;
+            bessel01(k * rho, J0, J1);
+            r += cw * J1;
+            z += cw * J0;
+            u += w * G * J0;
+        } else {
+            z += cw;
+            u += w * G;
+        }
+    }
+    Ir = r; Iz = z; Iu = u;
+}
+
+// unit-charge pair terms of F_short_ij (Force_short.jl:25-78) and the pair
+// energy, in the canonical orientation (i the lower index)
+template <class T>
+__device__ void pair_terms(const ShortConsts &c, const T &dx, const T &dy, const T &dxr, const T &dyr,
+                           const T &zi, const T &zj, const T &g1, const T &g2, T &Fx, T &Fy, T &Fz_i, T &Fz_j,
+                           T &U)
+{
+    const T rho2 = dx * dx + dy * dy;
+    const T rho = sqrt(rho2);
+    const T zn = fabs(zi - zj), zp = zi + zj;
+    const double s = jl_sign(dval(zi) - dval(zj));
+    const T g12 = g1 * g2;
+    T zero = rho * 0.0;
+    T Fr = zero, Fzi = zero, Fzj = zero, Uq = zero, Fp2 = zero, Fz2i = zero, Fz2j = zero, Ub = zero;
+    for (int iv = 0; iv < 8; iv++) {
+        const int l = iv >> 1;
+        const bool gauss = (iv & 1) != 0;
+        const T a = (l == 0) ? zn : (l == 1) ? zp : (l == 2) ? c.twoLz - zp : c.twoLz - zn;
+        const T b = (l == 0) ? zero + 1.0 : (l == 1) ? g1 : (l == 2) ? g2 : g12;
+        const double si = (l == 0) ? -s : (l == 1) ? -1.0 : (l == 2) ? 1.0 : s;
+        const double sj = (l == 1 || l == 2) ? si : -si;
+        T K, ae, pf;
+        double c2;
+        if (gauss) {
+            K = gauss_limit_t(c, a);
+            ae = a;
+            c2 = c.inv4alpha;
+            pf = -0.5 * b;
+        } else {
+            K = point_limit_t(c, a);
+            ae = a + c.twoLz;
+            c2 = 0.0;
+            pf = -0.5 * b * g12;
+        }
+        T Ir, Iz, Iu;
+        quad_t<T, true>(c, K, ae, c2, pf, g12, rho, Ir, Iz, Iu);
+        const double sf = gauss ? 1.0 : -1.0;
+        Fr += sf * Ir;
+        Fzi -= (sf * si) * Iz;
+        Fzj -= (sf * sj) * Iz;
+        Uq += sf * Iu;
+        if (!gauss) {
+            const T r2 = a * a + rho2;
+            const T inv15 = 1.0 / (r2 * sqrt(r2));
+            Fp2 += b * rho * inv15;
+            Fz2i += si * (b * a * inv15);
+            Fz2j += sj * (b * a * inv15);
+            Ub += 0.5 * b / sqrt(r2);
+        }
+    }
+    Fx = zero;
+    Fy = zero;
+    if (dval(rho) != 0.0) {
+        const T Fsr = Fr + 0.5 * Fp2;
+        const bool mi = (c.flags & QEM_DIR_MINIMAGE) != 0;
+        Fx = c.pref * Fsr * (mi ? dx : dxr) / rho;
+        Fy = c.pref * Fsr * (mi ? dy : dyr) / rho;
+    }
+    Fz_i = c.pref * (Fzi - 0.5 * Fz2i);
+    Fz_j = (c.flags & QEM_PAIR_PHYSICAL) ? c.pref * (Fzj - 0.5 * Fz2j) : -Fz_i;
+    U = c.pref * (Uq + Ub);
+}
+
+__device__ __forceinline__ double3 load_g(const double *gF, int i)
+{
+    if (!gF) return make_double3(0, 0, 0);
+    return make_double3(gF[3 * i], gF[3 * i + 1], gF[3 * i + 2]);
+}
+
+// records: RA[2p] = (dL/dx, dL/dy, dL/dz of the owner, dL/dz of the other),
+//          RA[2p+1] = (dL/dq owner, dL/dq other, dL/dgamma_down, dL/dgamma_up)
+__global__ void __launch_bounds__(ADJ_BLOCK) k_short_pair_adj(const int64_t *__restrict__ np, int64_t cap,
+                                                               const int2 *__restrict__ pairs,
+                                                               const double4 *__restrict__ pos,
+                                                               const double *__restrict__ gF, double gE,
+                                                               double4 *__restrict__ RA, const ShortConsts c)
+{
+    typedef Dual<6> D6;
+    const int64_t Np = min(*np, cap);
+    const int64_t p = (int64_t)blockIdx.x * ADJ_BLOCK + threadIdx.x;
+    if (p >= Np) return;
+    const int2 oo = pairs[p];
+    const bool owner_is_i = oo.x < oo.y;
+    const int i = owner_is_i ? oo.x : oo.y, j = owner_is_i ? oo.y : oo.x;
+    const double4 pi = pos[i], pj = pos[j];
+    const double dxr = pi.x - pj.x, dyr = pi.y - pj.y;
+    const double dxm = min_image(dxr, c.Lx, c.invLx), dym = min_image(dyr, c.Ly, c.invLy);
+    if (dxm * dxm + dym * dym > c.rc2) {  // stale-list re-check (Force_short.jl:36-41)
+        RA[2 * p] = make_double4(0, 0, 0, 0);
+        RA[2 * p + 1] = make_double4(0, 0, 0, 0);
+        return;
+    }
+    // tangents: 0 dx, 1 dy, 2 z_i, 3 z_j, 4 gamma_down, 5 gamma_up
+    const D6 dx = dvar<6>(dxm, 0), dy = dvar<6>(dym, 1), dxr_ = dvar<6>(dxr, 0), dyr_ = dvar<6>(dyr, 1);
+    const D6 zi = dvar<6>(pi.z, 2), zj = dvar<6>(pj.z, 3), g1 = dvar<6>(c.g1, 4), g2 = dvar<6>(c.g2, 5);
+    D6 Fx, Fy, Fzi, Fzj, U;
+    pair_terms<D6>(c, dx, dy, dxr_, dyr_, zi, zj, g1, g2, Fx, Fy, Fzi, Fzj, U);
+    const double3 gi = load_g(gF, i), gj = load_g(gF, j);
+    const D6 L = (gi.x - gj.x) * Fx + (gi.y - gj.y) * Fy + gi.z * Fzi + gj.z * Fzj + gE * U;
+    const double qq = pi.w * pj.w;
+    // dL/d(input) = q_i q_j dL~/d(input); dL/dq_i = q_j L~, dL/dq_j = q_i L~
+    const double gdx = qq * L.d[0], gdy = qq * L.d[1], gzi = qq * L.d[2], gzj = qq * L.d[3];
+    const double ggd = qq * L.d[4], ggu = qq * L.d[5];
+    if (owner_is_i) {
+        RA[2 * p] = make_double4(gdx, gdy, gzi, gzj);
+        RA[2 * p + 1] = make_double4(pj.w * L.v, pi.w * L.v, ggd, ggu);
+    } else {
+        RA[2 * p] = make_double4(-gdx, -gdy, gzj, gzi);
+        RA[2 * p + 1] = make_double4(pi.w * L.v, pj.w * L.v, ggd, ggu);
+    }
+}
+
+// unit-charge self image z-force and self energy (Force_short.jl:82-107,
+// Energy_short_range_njit.py:64-81)
+template <class T>
+__device__ void self_terms_t(const ShortConsts &c, const T &z, const T &g1, const T &g2, bool energy, T &Fz, T &E)
+{
+    const T g12 = g1 * g2;
+    const T zero = z * 0.0;
+    T Fs = zero, Uq = zero, Ub = zero;
+    for (int iv = 0; iv < 8; iv++) {
+        const int l = iv >> 1;
+        const bool gauss = (iv & 1) != 0;
+        const bool zterm = (l == 1 || l == 2);
+        if (!energy && !zterm) continue;
+        const T a = (l == 0) ? zero : (l == 1) ? 2.0 * z : (l == 2) ? c.twoLz - 2.0 * z : zero + c.twoLz;
+        const T b = (l == 0) ? zero + 1.0 : (l == 1) ? g1 : (l == 2) ? g2 : g12;
+        const double sa = (l == 1) ? -1.0 : (l == 2) ? 1.0 : 0.0;
+        T K, ae, pf;
+        double c2;
+        if (gauss) {
+            K = gauss_limit_t(c, a);
+            ae = a;
+            c2 = c.inv4alpha;
+            pf = -0.5 * b;
+        } else {
+            K = point_limit_t(c, a);
+            ae = a + c.twoLz;
+            c2 = 0.0;
+            pf = -0.5 * b * g12;
+        }
+        T Ir, Iz, Iu;
+        quad_t<T, false>(c, K, ae, c2, pf, g12, zero, Ir, Iz, Iu);
+        const double sf = gauss ? 1.0 : -1.0;
+        if (zterm) Fs += (sf * sa) * Iz;
+        if (energy) {
+            Uq += sf * Iu;
+            if (!gauss && l > 0) Ub += 0.5 * b / a;
+        }
+    }
+    const T a1 = 2.0 * z, a2 = c.twoLz - 2.0 * z;
+    const T Fp2 = 0.5 * (g2 * a2 / (a2 * a2 * a2) - g1 * a1 / (a1 * a1 * a1));
+    Fz = -c.pref * (Fs + Fp2);
+    E = 0.5 * c.pref * (Uq + Ub);
+}
+
+// per particle: own and incoming pair records (fixed order), self term,
+// walls; writes dL/dr, dL/dq and per-block gamma partials (gam[b], gam[nb + b])
+__global__ void __launch_bounds__(ADJ_BLOCK) k_adj_gather(int N, const double4 *__restrict__ pos,
+                                                           const int *__restrict__ pos_of,
+                                                           const int64_t *__restrict__ poff,
+                                                           const double4 *__restrict__ RA,
+                                                           const int64_t *__restrict__ in_off,
+                                                           const int64_t *__restrict__ in_list, int64_t cap,
+                                                           const double *__restrict__ gF, double gE,
+                                                           const ShortConsts c, double *__restrict__ gxyz,
+                                                           double *__restrict__ gq, double *__restrict__ gam,
+                                                           int do_short, int do_lj)
+{
+    __shared__ double red[2][ADJ_BLOCK / 32];
+    typedef Dual<3> D3;
+    const int i = blockIdx.x * ADJ_BLOCK + threadIdx.x;
+    double gx = 0, gy = 0, gz = 0, gqi = 0, gd = 0, gu = 0;
+    if (i < N) {
+        const double4 p = pos[i];
+        const double3 g = load_g(gF, i);
+        if (do_short) {
+            const int t = pos_of[i];
+            const int64_t pe = min(poff[t + 1], cap);
+            for (int64_t s = min(poff[t], cap); s < pe; s++) {
+                const double4 r0 = RA[2 * s], r1 = RA[2 * s + 1];
+                gx += r0.x; gy += r0.y; gz += r0.z;
+                gqi += r1.x;
+                gd += r1.z; gu += r1.w;
+            }
+            for (int64_t s = in_off[i]; s < in_off[i + 1]; s++) {
+                const int64_t pp = in_list[s];
+                const double4 r0 = RA[2 * pp], r1 = RA[2 * pp + 1];
+                gx -= r0.x; gy -= r0.y; gz += r0.w;
+                gqi += r1.y;
+            }
+            // self: L = q^2 (gF_z Fz~ + gE E~) in (z, gamma_down, gamma_up)
+            D3 Fz, E;
+            self_terms_t<D3>(c, dvar<3>(p.z, 0), dvar<3>(c.g1, 1), dvar<3>(c.g2, 2), gE != 0.0, Fz, E);
+            const D3 Ls = g.z * Fz + gE * E;
+            const double q2 = p.w * p.w;
+            gz += q2 * Ls.d[0];
+            gd += q2 * Ls.d[1];
+            gu += q2 * Ls.d[2];
+            gqi += 2.0 * p.w * Ls.v;
+        }
+        if (do_lj) {
+            for (int w = 0; w < c.n_walls; w++) {
+                const double dz = p.z - c.wall_pos[w];
+                if (!(c.wall_dir[w] * dz > 0)) continue;  // reported by the forward pass
+                if (dz < c.wall_cut[w]) {
+                    // F = dir 24 eps (2 sigma^12 dz^-14 - sigma^6 dz^-8), so
+                    // dF/dz = dir 24 eps dz^-2 (8 s6 - 28 s6^2) / dz
+                    const double invr2 = 1.0 / (dz * dz);
+                    const double s6 = (c.wall_sig2[w] * invr2) * (c.wall_sig2[w] * invr2) * (c.wall_sig2[w] * invr2);
+                    gz += g.z * c.wall_dir[w] * (24.0 * c.wall_eps[w] * invr2) * (8.0 * s6 - 28.0 * s6 * s6) / dz;
+                }
+            }
+        }
+        gxyz[3 * i] = gx;
+        gxyz[3 * i + 1] = gy;
+        gxyz[3 * i + 2] = gz;
+        if (gq) gq[i] = gqi;
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        gd += __shfl_down_sync(0xffffffffu, gd, d);
+        gu += __shfl_down_sync(0xffffffffu, gu, d);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = gd;
+        red[1][threadIdx.x >> 5] = gu;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w = 0; w < ADJ_BLOCK / 32; w++) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        gam[blockIdx.x] = a;
+        gam[gridDim.x + blockIdx.x] = b;
+    }
+}
+
+}  // namespace
+
+int qem_adj_gather_blocks(int N) { return (N + ADJ_BLOCK - 1) / ADJ_BLOCK; }
+
+cudaError_t qem_launch_short_pair_adj(const int64_t *np, int64_t cap, const int2 *pairs, const double4 *pos,
+                                      const double *gF, double gE, double4 *RA, const ShortConsts &c,
+                                      cudaStream_t s)
+{
+    if (cap <= 0) return cudaSuccess;
+    k_short_pair_adj<<<(int)((cap + ADJ_BLOCK - 1) / ADJ_BLOCK), ADJ_BLOCK, 0, s>>>(np, cap, pairs, pos, gF, gE, RA,
+                                                                                   c);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_adj_gather(int N, bool do_short, bool do_lj, const double4 *pos, const int *pos_of,
+                                  const int64_t *poff, const double4 *RA, const int64_t *in_off,
+                                  const int64_t *in_list, int64_t cap, const double *gF, double gE,
+                                  const ShortConsts &c, double *gxyz, double *gq, double *gam, cudaStream_t s)
+{
+    if (N <= 0) return cudaSuccess;
+    k_adj_gather<<<qem_adj_gather_blocks(N), ADJ_BLOCK, 0, s>>>(N, pos, pos_of, poff, RA, in_off, in_list, cap, gF,
+                                                                 gE, c, gxyz, gq, gam, do_short ? 1 : 0,
+                                                                 do_lj ? 1 : 0);
+    return cudaGetLastError();
+}

@@ -139,6 +139,8 @@ struct qem_handle {
         Eout, Fpart, pos_c;
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
+    // adjoint pass
+    DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart;
     cudaStream_t s2 = nullptr;  // side stream of the long range
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     unsigned *h_status = nullptr;
@@ -311,6 +313,91 @@ static void sample_kset(qem_handle *h, int P)
     h->kset_dirty = true;
 }
 
+// device buffers of the long range for N particles, Pk k-vectors, nch chunks
+// and ks k-slices; Ep: energy partials (long-range part at Ep + nbS)
+static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, double *Ep, int nbS, int nb0,
+                               LongBuffers &b)
+{
+    CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
+    CU(grow(h->zperm, sizeof(int) * N));
+    CU(grow(h->ztmp, sizeof(int) * N));
+    CU(grow(h->zkey, sizeof(double) * N));
+    CU(grow(h->zkey2, sizeof(double) * N));
+    CU(grow(h->zx, sizeof(double) * N));
+    CU(grow(h->zy, sizeof(double) * N));
+    CU(grow(h->zhf, sizeof(float) * N));
+    CU(grow(h->zhd, sizeof(double) * N));
+    CU(grow(h->qf, sizeof(float) * N));
+    CU(grow(h->qd, sizeof(double) * N));
+    CU(grow(h->k0, sizeof(double) * N));
+    CU(grow(h->qscan, sizeof(double) * (N + 1)));
+    CU(grow(h->kc, sizeof(KConst) * std::max(Pk, 1)));
+    CU(grow(h->tot, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
+    CU(grow(h->off, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
+    CU(grow(h->Fpart, sizeof(double) * 3 * (size_t)ks * N));
+    CU(grow(h->Utot, sizeof(double) * 4 * std::max(Pk, 1)));
+    CU(grow(h->kf, sizeof(KForce<double>) * std::max(Pk, 1)));
+    CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
+    CU(grow(h->Flong, sizeof(double) * 3 * N));
+    b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
+    b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
+    b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
+    b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
+    b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
+    b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
+    b.kf = h->kf.p;
+    b.Epart = Ep + nbS;
+    b.Eks = Ep + nbS + (size_t)ks * nch + nb0;
+    b.Fpart = ptr<double>(h->Fpart);
+    b.ks = ks;
+    b.stmp = h->scan_tmp2.p; b.stmp_bytes = h->scan_tmp2.cap;
+    return QEM_OK;
+}
+
+// cells, pair list (owner, other) with its per-particle CSR and the incoming
+// lists of every particle (QEM_short.jl:32-36 neighbour build)
+static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s)
+{
+    CU(grow(h->cell_cnt, sizeof(int) * h->ncell));
+    CU(grow(h->cell_start, sizeof(int) * (h->ncell + 1)));
+    CU(grow(h->cell_fill, sizeof(int) * h->ncell));
+    CU(grow(h->cell_list, sizeof(int) * N));
+    CU(grow(h->pos_of, sizeof(int) * N));
+    CU(grow(h->pcount, sizeof(int) * N));
+    CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
+    CU(grow(h->pos_c, sizeof(double4) * N));
+    // pair capacity: last count + 25 %, first time from the mean density; the
+    // count stays on the device (no host round trip inside the call)
+    if (h->pair_cap <= 0) {
+        const double dens = (double)N / (h->p.Lx * h->p.Ly);
+        h->pair_cap = (int64_t)(1.3 * 0.5 * N * QEM_PI * h->p.r_cutoff * h->p.r_cutoff * dens) + 4096;
+    }
+    const int64_t cap = h->pair_cap;
+    CU(grow(h->pairs, sizeof(int2) * cap));
+    CU(grow(h->R, sizeof(double4) * cap));
+    CU(grow(h->Upair, sizeof(double) * cap));
+    CU(grow(h->in_cnt, sizeof(int) * N));
+    CU(grow(h->in_fill, sizeof(int) * N));
+    CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
+    CU(grow(h->in_list, sizeof(int64_t) * cap));
+    CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<double4>(h->pos), ptr<int>(h->cell_cnt),
+                        ptr<int>(h->cell_start), ptr<int>(h->cell_fill), ptr<int>(h->cell_list),
+                        ptr<int>(h->pos_of), ptr<double4>(h->pos_c), h->scan_tmp.p, h->scan_tmp.cap, s));
+    CU(qem_launch_pair_count(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                             ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), s));
+    CU(qem_scan_i32_to_i64(ptr<int>(h->pcount), ptr<int64_t>(h->poff), N, h->scan_tmp.p, h->scan_tmp.cap, s));
+    CU(cudaMemsetAsync(h->in_cnt.p, 0, sizeof(int) * N, s));
+    CU(qem_launch_pair_fill(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
+                            ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
+                            ptr<int2>(h->pairs), cap, ptr<int>(h->in_cnt), st, s));
+    CU(qem_launch_incoming(N, ptr<int64_t>(h->poff) + N, cap, ptr<int2>(h->pairs), ptr<int>(h->in_cnt),
+                           ptr<int64_t>(h->in_off), ptr<int>(h->in_fill), ptr<int64_t>(h->in_list),
+                           h->scan_tmp.p, h->scan_tmp.cap, s));
+    h->pairs_N = N;
+    h->pairs_valid = true;
+    return QEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // one evaluation
 // ---------------------------------------------------------------------------
@@ -385,27 +472,11 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         const int Pk = h->has_kset ? h->P : 0;
         if (prec == QEM_FP32_FIX && Pk > 0 && h->kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
-        CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
-        CU(grow(h->zperm, sizeof(int) * N));
-        CU(grow(h->ztmp, sizeof(int) * N));
-        CU(grow(h->zkey, sizeof(double) * N));
-        CU(grow(h->zkey2, sizeof(double) * N));
-        CU(grow(h->zx, sizeof(double) * N));
-        CU(grow(h->zy, sizeof(double) * N));
-        CU(grow(h->zhf, sizeof(float) * N));
-        CU(grow(h->zhd, sizeof(double) * N));
-        CU(grow(h->qf, sizeof(float) * N));
-        CU(grow(h->qd, sizeof(double) * N));
-        CU(grow(h->k0, sizeof(double) * N));
-        CU(grow(h->qscan, sizeof(double) * (N + 1)));
-        CU(grow(h->kc, sizeof(KConst) * std::max(Pk, 1)));
-        CU(grow(h->tot, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
-        CU(grow(h->off, sizeof(double) * 4 * (size_t)std::max(Pk, 1) * nch));
-        CU(grow(h->Fpart, sizeof(double) * 3 * (size_t)ks * N));
-        CU(grow(h->Utot, sizeof(double) * 4 * std::max(Pk, 1)));
-        CU(grow(h->kf, sizeof(KForce<double>) * std::max(Pk, 1)));
-        CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
-        CU(grow(h->Flong, sizeof(double) * 3 * N));
+        LongBuffers b;  // allocated before any launch or copy that uses them
+        {
+            const qem_status ls = long_buffers(h, N, Pk, nch, ks, Ep, nbS, nb0, b);
+            if (ls != QEM_OK) return ls;
+        }
         if (concurrent) {  // fork after pack (positions) and the energy-partial clear
             CU(cudaEventRecord(h->ev_fork, s));
             CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
@@ -419,19 +490,6 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         CU(cudaMemsetAsync(FL, 0, sizeof(double) * 3 * N, sl));
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
                             ptr<double>(h->zkey2), sl));
-        LongBuffers b;
-        b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
-        b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
-        b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
-        b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
-        b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
-        b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
-        b.kf = h->kf.p;
-        b.Epart = Ep + nbS;
-        b.Eks = Ep + nbS + (size_t)ks * nch + nb0;
-        b.Fpart = ptr<double>(h->Fpart);
-        b.ks = ks;
-        b.stmp = h->scan_tmp2.p; b.stmp_bytes = h->scan_tmp2.cap;
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, FL, nch, st, sl, 0));
         mk_lprep = h->prof.mark(sl);
@@ -447,44 +505,9 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
         const bool rebuild = !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
         if (rebuild) {
-            CU(grow(h->cell_cnt, sizeof(int) * h->ncell));
-            CU(grow(h->cell_start, sizeof(int) * (h->ncell + 1)));
-            CU(grow(h->cell_fill, sizeof(int) * h->ncell));
-            CU(grow(h->cell_list, sizeof(int) * N));
-            CU(grow(h->pos_of, sizeof(int) * N));
-            CU(grow(h->pcount, sizeof(int) * N));
-            CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
-            CU(grow(h->pos_c, sizeof(double4) * N));
-            // pair capacity: last count + 25 %, first time from the mean density; the
-            // count stays on the device (no host round trip inside the call)
-            if (h->pair_cap <= 0) {
-                const double dens = (double)N / (h->p.Lx * h->p.Ly);
-                h->pair_cap = (int64_t)(1.3 * 0.5 * N * QEM_PI * h->p.r_cutoff * h->p.r_cutoff * dens) + 4096;
-            }
-            const int64_t cap = h->pair_cap;
-            CU(grow(h->pairs, sizeof(int2) * cap));
-            CU(grow(h->R, sizeof(double4) * cap));
-            CU(grow(h->Upair, sizeof(double) * cap));
-            CU(grow(h->in_cnt, sizeof(int) * N));
-            CU(grow(h->in_fill, sizeof(int) * N));
-            CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
-            CU(grow(h->in_list, sizeof(int64_t) * cap));
-            CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<double4>(h->pos), ptr<int>(h->cell_cnt),
-                                ptr<int>(h->cell_start), ptr<int>(h->cell_fill), ptr<int>(h->cell_list),
-                                ptr<int>(h->pos_of), ptr<double4>(h->pos_c), h->scan_tmp.p, h->scan_tmp.cap, s));
-            CU(qem_launch_pair_count(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
-                                     ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), s));
-            CU(qem_scan_i32_to_i64(ptr<int>(h->pcount), ptr<int64_t>(h->poff), N, h->scan_tmp.p, h->scan_tmp.cap, s));
-            CU(cudaMemsetAsync(h->in_cnt.p, 0, sizeof(int) * N, s));
-            CU(qem_launch_pair_fill(N, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
-                                    ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
-                                    ptr<int2>(h->pairs), cap, ptr<int>(h->in_cnt), st, s));
-            CU(qem_launch_incoming(N, ptr<int64_t>(h->poff) + N, cap, ptr<int2>(h->pairs), ptr<int>(h->in_cnt),
-                                   ptr<int64_t>(h->in_off), ptr<int>(h->in_fill), ptr<int64_t>(h->in_list),
-                                   h->scan_tmp.p, h->scan_tmp.cap, s));
+            const qem_status bs = build_pairs(h, N, st, s);
+            if (bs != QEM_OK) return bs;
             launches += 16;
-            h->pairs_N = N;
-            h->pairs_valid = true;
         }
         h->short_calls++;
         mk_bin = h->prof.mark(s);
@@ -630,7 +653,9 @@ void qem_destroy(qem_handle *h)
                       &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
                       &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin,
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
-                      &h->pos_c, &h->scan_tmp2, &h->Flong};
+                      &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
+                      &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
+                      &h->lam, &h->ggk, &h->Gpart};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -844,3 +869,165 @@ qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap)
 const char *qem_version(void) { return "qem4molly_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// adjoint: L = gE E + sum_i gF_i . F_i
+// ---------------------------------------------------------------------------
+static qem_status backward_once(qem_handle *h, int N, const double *xyz, const double *q, const double *gF,
+                                double gE, double *gxyz, double *gq, double *ggamma, uint32_t terms, int mem,
+                                cudaStream_t s, bool &retry)
+{
+    retry = false;
+    const bool do_short = terms & QEM_TERM_SHORT;
+    const bool do_long = terms & QEM_TERM_LONG;
+    const bool do_lj = (terms & QEM_TERM_LJ) && h->p.n_walls > 0;
+    CU(grow(h->pos, sizeof(double4) * N));
+    CU(grow(h->cell, sizeof(int) * N));
+    CU(grow(h->status, 64));
+    const double *xyz_d = xyz, *q_d = q, *gF_d = gF;
+    double *gx_d = gxyz, *gq_d = gq;
+    if (mem == QEM_MEM_HOST) {
+        CU(grow(h->xyz, sizeof(double) * 3 * N));
+        CU(grow(h->q, sizeof(double) * N));
+        CU(grow(h->gxyz, sizeof(double) * 3 * N));
+        CU(cudaMemcpyAsync(h->xyz.p, xyz, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(h->q.p, q, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+        xyz_d = ptr<double>(h->xyz);
+        q_d = ptr<double>(h->q);
+        gx_d = ptr<double>(h->gxyz);
+        if (gF) {
+            CU(grow(h->gF, sizeof(double) * 3 * N));
+            CU(cudaMemcpyAsync(h->gF.p, gF, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
+            gF_d = ptr<double>(h->gF);
+        }
+        if (gq) {
+            CU(grow(h->gq, sizeof(double) * N));
+            gq_d = ptr<double>(h->gq);
+        }
+    }
+    unsigned *st = ptr<unsigned>(h->status);
+    CU(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+    CU(qem_launch_pack(N, xyz_d, q_d, ptr<double4>(h->pos), ptr<int>(h->cell), h->geom, st, s));
+    CU(grow(h->gout, sizeof(double) * 8));
+    CU(cudaMemsetAsync(h->gout.p, 0, sizeof(double) * 8, s));
+    double *gout = ptr<double>(h->gout);  // [0, 2): short gamma, [2, 4): long gamma
+    CU(grow(h->scan_tmp, qem_scan_tmp_bytes(std::max(std::max(N, h->ncell), 1)) + 64));
+
+    if (do_short || do_lj) {
+        if (do_short) {
+            const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
+            if (!stale || !h->pairs_valid || h->pairs_N != N) {
+                const qem_status bs = build_pairs(h, N, st, s);
+                if (bs != QEM_OK) return bs;
+            }
+            CU(grow(h->RA, sizeof(double4) * 2 * h->pair_cap));
+            CU(qem_launch_short_pair_adj(ptr<int64_t>(h->poff) + N, h->pair_cap, ptr<int2>(h->pairs),
+                                         ptr<double4>(h->pos), gF_d, gE, ptr<double4>(h->RA), h->sc, s));
+        }
+        const int nb = qem_adj_gather_blocks(N);
+        CU(grow(h->gam, sizeof(double) * 2 * nb));
+        CU(qem_launch_adj_gather(N, do_short, do_lj, ptr<double4>(h->pos), ptr<int>(h->pos_of),
+                                 ptr<int64_t>(h->poff), ptr<double4>(h->RA), ptr<int64_t>(h->in_off),
+                                 ptr<int64_t>(h->in_list), h->pair_cap, gF_d, gE, h->sc, gx_d, gq_d,
+                                 ptr<double>(h->gam), s));
+        CU(qem_launch_reduce_sum(ptr<double>(h->gam), nb, gout, s));
+        CU(qem_launch_reduce_sum(ptr<double>(h->gam) + nb, nb, gout + 1, s));
+    } else {
+        CU(cudaMemsetAsync(gx_d, 0, sizeof(double) * 3 * N, s));
+        if (gq_d) CU(cudaMemsetAsync(gq_d, 0, sizeof(double) * N, s));
+    }
+
+    if (do_long) {
+        if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+        const int Pk = h->has_kset ? h->P : 0;
+        const int LCH = qem_long_chunk();
+        const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;
+        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), 8);
+        CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks * nch + nb0 + std::max(Pk, 1) + 8)));
+        LongBuffers b;
+        {
+            const qem_status ls = long_buffers(h, N, Pk, nch, ks, ptr<double>(h->Epart), nbS, nb0, b);
+            if (ls != QEM_OK) return ls;
+        }
+        if (h->kset_dirty && Pk > 0) {
+            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
+            h->kset_dirty = false;
+        }
+        CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
+                            ptr<double>(h->zkey2), s));
+        CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch, st, s, 0));
+        const size_t P1 = std::max(Pk, 1);
+        CU(grow(h->zgx, sizeof(double) * N));
+        CU(grow(h->zgy, sizeof(double) * N));
+        CU(grow(h->zgz, sizeof(double) * N));
+        CU(grow(h->w1, sizeof(double) * N));
+        CU(grow(h->w2, sizeof(double) * N));
+        CU(grow(h->ws1, sizeof(double) * (N + 1)));
+        CU(grow(h->ws2, sizeof(double) * (N + 1)));
+        CU(grow(h->atot, sizeof(double) * 8 * P1 * nch));
+        CU(grow(h->aoff, sizeof(double) * 4 * P1 * nch));
+        CU(grow(h->lam, sizeof(double) * 4 * P1));
+        CU(grow(h->ggk, sizeof(double) * 2 * P1));
+        CU(grow(h->Gpart, sizeof(double) * 4 * (size_t)ks * N));
+        LongAdjBuffers a;
+        a.zgx = ptr<double>(h->zgx); a.zgy = ptr<double>(h->zgy); a.zgz = ptr<double>(h->zgz);
+        a.w1 = ptr<double>(h->w1); a.w2 = ptr<double>(h->w2); a.s1 = ptr<double>(h->ws1); a.s2 = ptr<double>(h->ws2);
+        a.atot = ptr<double>(h->atot); a.aoff = ptr<double>(h->aoff); a.lam = ptr<double>(h->lam);
+        a.ggk = ptr<double>(h->ggk); a.Gpart = ptr<double>(h->Gpart); a.gam = gout + 2;
+        CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                               h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch, ks, s));
+    }
+    double hg[4] = {0, 0, 0, 0};
+    CU(cudaMemcpyAsync(hg, gout, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    if (mem == QEM_MEM_HOST) {
+        CU(cudaMemcpyAsync(gxyz, gx_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+        if (gq) CU(cudaMemcpyAsync(gq, gq_d, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (do_short)
+        CU(cudaMemcpyAsync(h->h_np, ptr<int64_t>(h->poff) + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    CU(cudaGetLastError());
+    if (do_short) {
+        h->Np = *h->h_np;
+        if (*h->h_status & QEM_ST_OVERFLOW) {
+            h->pair_cap = h->Np + h->Np / 4 + 4096;
+            h->pairs_valid = false;
+            retry = true;
+            return QEM_OK;
+        }
+    }
+    const unsigned stv = *h->h_status;
+    if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
+    if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    if (ggamma) {
+        ggamma[0] = hg[0] + hg[2];
+        ggamma[1] = hg[1] + hg[3];
+    }
+    h->err.clear();
+    return QEM_OK;
+}
+
+extern "C" qem_status qem_backward(qem_handle *h, int32_t N, const double *xyz, const double *q, const double *gF,
+                                   double gE, double *gxyz, double *gq, double *ggamma, uint32_t terms, int32_t mem,
+                                   void *stream)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (N < 0) return fail(h, QEM_ERR_ARG, "N < 0");
+    if (terms & ~QEM_TERM_ALL) return fail(h, QEM_ERR_ARG, "unknown term bit");
+    if (mem != QEM_MEM_HOST && mem != QEM_MEM_DEVICE) return fail(h, QEM_ERR_ARG, "mem must be HOST or DEVICE");
+    if (!std::isfinite(gE)) return fail(h, QEM_ERR_ARG, "gE is not finite");
+    if (N == 0) {
+        if (ggamma) ggamma[0] = ggamma[1] = 0;
+        return QEM_OK;
+    }
+    if (!xyz || !q || !gxyz) return fail(h, QEM_ERR_ARG, "NULL coordinate, charge or gradient pointer");
+    if (cudaSetDevice(h->p.device) != cudaSuccess) return fail(h, QEM_ERR_CUDA, "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    bool retry = false;
+    qem_status st = backward_once(h, N, xyz, q, gF, gE, gxyz, gq, ggamma, terms, mem, s, retry);
+    if (st == QEM_OK && retry) st = backward_once(h, N, xyz, q, gF, gE, gxyz, gq, ggamma, terms, mem, s, retry);
+    if (st == QEM_OK && retry) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list outgrew its capacity twice");
+    return st;
+}

@@ -137,6 +137,33 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
 int qem_long_chunk(void);
 
 cudaError_t qem_launch_reduce_sum(const double *in, int n, double *out, cudaStream_t s);
+
+// ---- adjoint (FP64) --------------------------------------------------------
+// pair records RA (2 double4 per pair) and the per-particle pass writing
+// dL/dr, dL/dq (gq may be NULL) and per-block gamma partials gam[2 * nb]
+int qem_adj_gather_blocks(int N);
+cudaError_t qem_launch_short_pair_adj(const int64_t *np, int64_t cap, const int2 *pairs, const double4 *pos,
+                                      const double *gF, double gE, double4 *RA, const ShortConsts &c,
+                                      cudaStream_t s);
+cudaError_t qem_launch_adj_gather(int N, bool do_short, bool do_lj, const double4 *pos, const int *pos_of,
+                                  const int64_t *poff, const double4 *RA, const int64_t *in_off,
+                                  const int64_t *in_list, int64_t cap, const double *gF, double gE,
+                                  const ShortConsts &c, double *gxyz, double *gq, double *gam, cudaStream_t s);
+struct LongAdjBuffers {
+    double *zgx, *zgy, *zgz;   // cotangents in z order
+    double *w1, *w2, *s1, *s2; // k = 0 adjoint inputs and their exclusive scans (N + 1)
+    double *atot;              // P x nch x 8 chunk totals of a, b, P c1, P c2
+    double *aoff;              // P x nch x 4 scans of a (from above) and b (from below)
+    double *lam;               // P x 4 Lambda_U, Lambda_V
+    double *ggk;               // P x 2 per-k gamma derivatives
+    double *Gpart;             // ks x N x 4 per-slice (dL/dx, dL/dy, dL/dz, dL/dq), z order
+    double *gam;               // 2: gamma derivatives of the long range
+};
+// after stage 0 of qem_launch_long in FP64: adds the long-range dL/dr, dL/dq
+// into gxyz, gq (particle order)
+cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffers &b, const LongAdjBuffers &a,
+                                double Lx, double Ly, double Lz, double g1, double g2, double eps0, const double *gF,
+                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s);
 // out[i] += a[i] for n doubles
 cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s);
 

@@ -433,6 +433,392 @@ __global__ void k_reduce_sum(const double *__restrict__ in, int n, double *__res
 
 inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 
+
+// ---------------------------------------------------------------------------
+// adjoint of the long range (FP64).  With P_i = e^{-i theta_i}, the cotangents
+// w_xy = w_k q (fx gF_x + fy gF_y), w_z = w_k q gF_z of the force pass and
+// c1 = ep (w_z - i w_xy), c2 = -em (w_z + i w_xy), the force part of L is
+//   sum_i Re[P_i (c1 (S1 - C_i / 2) + c2 (S2 - A_i / 2))],
+// so u_m = q ep e^{i theta} collects a_i = -P_i c2_i / 2 from every i above
+// it (through A_i) and v_m collects b_i = -P_i c1_i / 2 from every i below it
+// (through C_i); the sorted energy adds -gE e_k q (em, ep) P / 2 to (a, b),
+// and the totals U, V collect Lambda_U, Lambda_V from S1, S2 and from the
+// split energy term.  Passes: chunk totals of a, b, P c1, P c2 (k_ladj_tot);
+// per k their scans, Lambda and the gamma derivatives (k_ladj_scan); per
+// particle the prefix / suffix sums of u, v, a, b and the gradient
+// (k_ladj); slices + the k = 0 term in particle order (k_ladj_final).
+// ---------------------------------------------------------------------------
+struct AdjIn {
+    const double *zgx, *zgy, *zgz;  // cotangents of F in z order
+    double gE;
+};
+
+// charge-free p1 = P c1 / q, p2 = P c2 / q (w_xy, w_z passed without q) and
+// the scan coefficients a, b (with q)
+__device__ __forceinline__ void adj_coefs(double q, double ep, double em, double c, double s, double wxy, double wz,
+                                          double ekgE, double &ar, double &ai, double &br, double &bi,
+                                          double &p1r, double &p1i, double &p2r, double &p2i)
+{
+    // c1 = ep (wz - i wxy), c2 = -em (wz + i wxy); P = c - i s
+    const double c1r = ep * wz, c1i = -ep * wxy, c2r = -em * wz, c2i = -em * wxy;
+    p1r = c * c1r + s * c1i; p1i = c * c1i - s * c1r;
+    p2r = c * c2r + s * c2i; p2i = c * c2i - s * c2r;
+    // a = -q (P c2 / q + ek gE em P) / 2, b = -q (P c1 / q + ek gE ep P) / 2
+    ar = -0.5 * q * (p2r + ekgE * em * c); ai = -0.5 * q * (p2i - ekgE * em * s);
+    br = -0.5 * q * (p1r + ekgE * ep * c); bi = -0.5 * q * (p1i - ekgE * ep * s);
+}
+
+__global__ void __launch_bounds__(LT) k_ladj_tot(int N, int P, int nch, const double *__restrict__ zx,
+                                                 const double *__restrict__ zy, const double *__restrict__ zh,
+                                                 const double *__restrict__ qv, const KConst *__restrict__ kc,
+                                                 AdjIn in, double *__restrict__ atot)
+{
+    __shared__ double red[8][NW];
+    Quad4<double> P4;
+    const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
+    P4.load(N, m0, zx, zy, zh, qv);
+    double gxy[PPT][2], gzz[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int m = m0 + j;
+        gxy[j][0] = m < N ? in.zgx[m] : 0.0;
+        gxy[j][1] = m < N ? in.zgy[m] : 0.0;
+        gzz[j] = m < N ? in.zgz[m] : 0.0;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int kk = 0; kk < KPB; kk++) {
+        const int kidx = blockIdx.y * KPB + kk;
+        if (kidx >= P) break;
+        const KConst K = kc[kidx];
+        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
+            t -= rint(t);
+            double s, c;
+            sincospi(2.0 * t, &s, &c);
+            const double kz = K.k * P4.z[j], ep = exp(kz), em = exp(-kz), q = P4.q[j];
+            const double wxy = K.wk * (K.fx * gxy[j][0] + K.fy * gxy[j][1]), wz = K.wk * gzz[j];
+            double a[8];
+            adj_coefs(q, ep, em, c, s, wxy, wz, K.ek * in.gE, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]);
+#pragma unroll
+            for (int r = 0; r < 4; r++) v[r] += a[r];
+#pragma unroll
+            for (int r = 4; r < 8; r++) v[r] += q * a[r];
+        }
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) v[r] += __shfl_down_sync(0xffffffffu, v[r], d);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < 8; r++) red[r][w] = v[r];
+        }
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            double sum = 0;
+#pragma unroll
+            for (int ww = 0; ww < NW; ww++) sum += red[threadIdx.x][ww];
+            atot[((int64_t)kidx * nch + blockIdx.x) * 8 + threadIdx.x] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+// one warp per k: suffix scan of the a totals, prefix scan of the b totals,
+// sums of P c1 and P c2; Lambda_U, Lambda_V and the gamma derivatives
+__global__ void k_ladj_scan(int P, int nch, const double *__restrict__ atot, double *__restrict__ aoff,
+                            const double *__restrict__ Utot, const KConst *__restrict__ kc, double g1, double g2,
+                            double gE, double *__restrict__ lam, double *__restrict__ ggk)
+{
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (m >= P) return;
+    const double *T = atot + (int64_t)m * nch * 8;
+    double *O = aoff + (int64_t)m * nch * 4;
+    double s1r = 0, s1i = 0, s2r = 0, s2i = 0;
+    double cr = 0, ci = 0;  // b from below
+    for (int base = 0; base < nch; base += 32) {
+        const int c = base + lane;
+        double r = c < nch ? T[8 * c + 2] : 0.0, i = c < nch ? T[8 * c + 3] : 0.0;
+        s1r += c < nch ? T[8 * c + 4] : 0.0; s1i += c < nch ? T[8 * c + 5] : 0.0;
+        s2r += c < nch ? T[8 * c + 6] : 0.0; s2i += c < nch ? T[8 * c + 7] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double a = __shfl_up_sync(0xffffffffu, r, d), b = __shfl_up_sync(0xffffffffu, i, d);
+            if (lane >= d) { r += a; i += b; }
+        }
+        double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
+        if (lane == 0) { er = 0; ei = 0; }
+        if (c < nch) { O[4 * c + 2] = cr + er; O[4 * c + 3] = ci + ei; }
+        cr += __shfl_sync(0xffffffffu, r, 31);
+        ci += __shfl_sync(0xffffffffu, i, 31);
+    }
+    double dr = 0, di = 0;  // a from above
+    for (int base = 0; base < nch; base += 32) {
+        const int c = nch - 1 - (base + lane);
+        double r = c >= 0 ? T[8 * c] : 0.0, i = c >= 0 ? T[8 * c + 1] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double a = __shfl_up_sync(0xffffffffu, r, d), b = __shfl_up_sync(0xffffffffu, i, d);
+            if (lane >= d) { r += a; i += b; }
+        }
+        double er = __shfl_up_sync(0xffffffffu, r, 1), ei = __shfl_up_sync(0xffffffffu, i, 1);
+        if (lane == 0) { er = 0; ei = 0; }
+        if (c >= 0) { O[4 * c] = dr + er; O[4 * c + 1] = di + ei; }
+        dr += __shfl_sync(0xffffffffu, r, 31);
+        di += __shfl_sync(0xffffffffu, i, 31);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        s1r += __shfl_down_sync(0xffffffffu, s1r, d); s1i += __shfl_down_sync(0xffffffffu, s1i, d);
+        s2r += __shfl_down_sync(0xffffffffu, s2r, d); s2i += __shfl_down_sync(0xffffffffu, s2i, d);
+    }
+    if (lane == 0) {
+        const KConst K = kc[m];
+        const double W = K.W * K.W, g = K.g, g12 = g1 * g2;
+        const double Ur = Utot[4 * m], Ui = Utot[4 * m + 1], Vr = Utot[4 * m + 2], Vi = Utot[4 * m + 3];
+        const double gW = g * W, eg = gE * K.ek * g;
+        // dL = Re[Lambda_U dU + Lambda_V dV]
+        double LUr = gW * (g2 * s1r + g12 * W * s2r), LUi = gW * (g2 * s1i + g12 * W * s2i);
+        double LVr = gW * (g12 * W * s1r + g1 * s2r), LVi = gW * (g12 * W * s1i + g1 * s2i);
+        // split energy e_k g (g2 W |U|^2 + g1 W |V|^2 + g12 W^2 Re(U conj V)): conjugates
+        LUr += eg * (2.0 * g2 * W * Ur + g12 * W * W * Vr); LUi += eg * (-2.0 * g2 * W * Ui - g12 * W * W * Vi);
+        LVr += eg * (2.0 * g1 * W * Vr + g12 * W * W * Ur); LVi += eg * (-2.0 * g1 * W * Vi - g12 * W * W * Ui);
+        lam[4 * m] = LUr; lam[4 * m + 1] = LUi; lam[4 * m + 2] = LVr; lam[4 * m + 3] = LVi;
+        // gamma derivatives: S1 = g W (g2 U + g12 W V), S2 = g W (g12 W U + g1 V),
+        // g = 0.5 / (g12 W^2 - 1), dg/dg12 = -2 W^2 g^2
+        const double dg = -2.0 * W * W * g * g;
+        const double A1r = W * (g2 * Ur + g12 * W * Vr), A1i = W * (g2 * Ui + g12 * W * Vi);  // S1 / g
+        const double A2r = W * (g12 * W * Ur + g1 * Vr), A2i = W * (g12 * W * Ui + g1 * Vi);  // S2 / g
+        // Re[s1 dS1 + s2 dS2] for each gamma (dS = dg A + g W dA)
+        const double base = s1r * A1r - s1i * A1i + s2r * A2r - s2i * A2i;
+        const double dS1d_r = g * W * g2 * W * Vr, dS1d_i = g * W * g2 * W * Vi;  // d(A1)/dg1 * g W
+        const double dS2d_r = g * W * (g2 * W * Ur + Vr), dS2d_i = g * W * (g2 * W * Ui + Vi);
+        const double dS1u_r = g * W * (Ur + g1 * W * Vr), dS1u_i = g * W * (Ui + g1 * W * Vi);
+        const double dS2u_r = g * W * g1 * W * Ur, dS2u_i = g * W * g1 * W * Ui;
+        double gd = dg * g2 * base + (s1r * dS1d_r - s1i * dS1d_i + s2r * dS2d_r - s2i * dS2d_i);
+        double gu = dg * g1 * base + (s1r * dS1u_r - s1i * dS1u_i + s2r * dS2u_r - s2i * dS2u_i);
+        const double UU = Ur * Ur + Ui * Ui, VV = Vr * Vr + Vi * Vi, UV = Ur * Vr + Ui * Vi;
+        const double sig = g2 * W * UU + g1 * W * VV + g12 * W * W * UV;
+        gd += gE * K.ek * (dg * g2 * sig + g * (W * VV + g2 * W * W * UV));
+        gu += gE * K.ek * (dg * g1 * sig + g * (W * UU + g1 * W * W * UV));
+        ggk[2 * m] = gd;
+        ggk[2 * m + 1] = gu;
+    }
+}
+
+// exclusive block scans of NV values per thread: forward (from lower
+// threads) where FWD bit v is set, backward (from higher threads) otherwise
+template <int NV, unsigned FWD>
+__device__ __forceinline__ void block_excl(double (&v)[NV], double (*sh)[NW])
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            const bool f = (FWD >> r) & 1u;
+            const double up = __shfl_up_sync(0xffffffffu, v[r], d), dn = __shfl_down_sync(0xffffffffu, v[r], d);
+            if (f ? lane >= d : lane + d < 32) v[r] += f ? up : dn;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NV; r++) {
+        const bool f = (FWD >> r) & 1u;
+        if (f ? lane == 31 : lane == 0) sh[r][w] = v[r];
+        const double up = __shfl_up_sync(0xffffffffu, v[r], 1), dn = __shfl_down_sync(0xffffffffu, v[r], 1);
+        v[r] = f ? (lane == 0 ? 0.0 : up) : (lane == 31 ? 0.0 : dn);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NV; r++) {
+        const bool f = (FWD >> r) & 1u;
+#pragma unroll
+        for (int ww = 0; ww < NW; ww++)
+            if (f ? ww < w : ww > w) v[r] += sh[r][ww];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(LT) k_ladj(int N, int P, int nch, int ks_n, const double *__restrict__ zx,
+                                             const double *__restrict__ zy, const double *__restrict__ zh,
+                                             const double *__restrict__ qv, const KConst *__restrict__ kc,
+                                             const double *__restrict__ kin, const KForce<double> *__restrict__ kf,
+                                             const double *__restrict__ off, const double *__restrict__ aoff,
+                                             const double *__restrict__ lam, AdjIn in, double *__restrict__ Gpart)
+{
+    __shared__ double sh[8][NW];
+    Quad4<double> P4;
+    const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
+    P4.load(N, m0, zx, zy, zh, qv);
+    double gxy[PPT][2], gzz[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int m = m0 + j;
+        gxy[j][0] = m < N ? in.zgx[m] : 0.0;
+        gxy[j][1] = m < N ? in.zgy[m] : 0.0;
+        gzz[j] = m < N ? in.zgz[m] : 0.0;
+    }
+    const int ks = blockIdx.y;
+    const int kb = (int)((int64_t)P * ks / ks_n), ke = (int)((int64_t)P * (ks + 1) / ks_n);
+    double Gx[PPT], Gy[PPT], Gz[PPT], Gq[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) { Gx[j] = 0; Gy[j] = 0; Gz[j] = 0; Gq[j] = 0; }
+    for (int kidx = kb; kidx < ke; kidx++) {
+        const KConst K = kc[kidx];
+        const KForce<double> F = kf[kidx];
+        const double kx = kin[3 * kidx], ky = kin[3 * kidx + 1], ekgE = K.ek * in.gE;
+        double c[PPT], s[PPT], ep[PPT], em[PPT];
+        double u[PPT][8];  // u, v, a, b (complex) per particle
+        double pc1[PPT][2], pc2[PPT][2];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
+            t -= rint(t);
+            sincospi(2.0 * t, &s[j], &c[j]);
+            const double kz = K.k * P4.z[j], q = P4.q[j];
+            ep[j] = exp(kz);
+            em[j] = exp(-kz);
+            u[j][0] = q * ep[j] * c[j]; u[j][1] = q * ep[j] * s[j];
+            u[j][2] = q * em[j] * c[j]; u[j][3] = q * em[j] * s[j];
+            const double wxy = K.wk * (K.fx * gxy[j][0] + K.fy * gxy[j][1]), wz = K.wk * gzz[j];
+            adj_coefs(q, ep[j], em[j], c[j], s[j], wxy, wz, ekgE, u[j][4], u[j][5], u[j][6], u[j][7], pc1[j][0],
+                      pc1[j][1], pc2[j][0], pc2[j][1]);
+        }
+        // thread-local exclusive sums: u (0,1) and b (6,7) from below; v (2,3) and a (4,5) from above
+        double loc[PPT][8], tot[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const bool fwd = (r < 2) || (r >= 6);
+            double acc = 0;
+            if (fwd) {
+#pragma unroll
+                for (int j = 0; j < PPT; j++) { loc[j][r] = acc; acc += u[j][r]; }
+            } else {
+#pragma unroll
+                for (int j = PPT - 1; j >= 0; j--) { loc[j][r] = acc; acc += u[j][r]; }
+            }
+            tot[r] = acc;
+        }
+        block_excl<8, 0xC3u>(tot, sh);
+        const double *O = off + ((int64_t)kidx * nch + blockIdx.x) * 4;
+        const double *OA = aoff + ((int64_t)kidx * nch + blockIdx.x) * 4;
+        const double base[8] = {O[0] + tot[0], O[1] + tot[1], O[2] + tot[2], O[3] + tot[3],
+                                OA[0] + tot[4], OA[1] + tot[5], OA[2] + tot[6], OA[3] + tot[7]};
+        const double LUr = lam[4 * kidx], LUi = lam[4 * kidx + 1], LVr = lam[4 * kidx + 2], LVi = lam[4 * kidx + 3];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const double q = P4.q[j];
+            const double Ar = base[0] + loc[j][0], Ai = base[1] + loc[j][1];
+            const double Cr = base[2] + loc[j][2], Ci = base[3] + loc[j][3];
+            const double SAr = base[4] + loc[j][4], SAi = base[5] + loc[j][5];
+            const double PBr = base[6] + loc[j][6], PBi = base[7] + loc[j][7];
+            // through u = q ep E and v = q em E (E = c + i s): ubar = Lambda_U + SA, vbar = Lambda_V + PB
+            const double ubr = LUr + SAr, ubi = LUi + SAi, vbr = LVr + PBr, vbi = LVi + PBi;
+            const double uur = ubr * u[j][0] - ubi * u[j][1], uui = ubr * u[j][1] + ubi * u[j][0];
+            const double vvr = vbr * u[j][2] - vbi * u[j][3], vvi = vbr * u[j][3] + vbi * u[j][2];
+            double gth = -(uui + vvi);
+            double gz = K.k * (uur - vvr);
+            double gq = (ep[j] * (ubr * c[j] - ubi * s[j]) + em[j] * (vbr * c[j] - vbi * s[j]));
+            // direct: Re[P (c1 alpha + c2 beta)], alpha = S1 - C/2, beta = S2 - A/2
+            const double alr = F.s1r - 0.5 * Cr, ali = F.s1i - 0.5 * Ci;
+            const double ber = F.s2r - 0.5 * Ar, bei = F.s2i - 0.5 * Ai;
+            const double x1r = pc1[j][0] * alr - pc1[j][1] * ali, x1i = pc1[j][0] * ali + pc1[j][1] * alr;
+            const double x2r = pc2[j][0] * ber - pc2[j][1] * bei, x2i = pc2[j][0] * bei + pc2[j][1] * ber;
+            gth += q * (x1i + x2i);
+            gz += q * K.k * (x1r - x2r);
+            gq += x1r + x2r;
+            // sorted energy: gE e_k (-q^2 - q Re[P (em A + ep C)]) / 2, P = c - i s
+            const double zr = em[j] * Ar + ep[j] * Cr, zi = em[j] * Ai + ep[j] * Ci;
+            const double pzr = c[j] * zr + s[j] * zi, pzi = c[j] * zi - s[j] * zr;
+            const double yr = ep[j] * Cr - em[j] * Ar, yi = ep[j] * Ci - em[j] * Ai;
+            gth += -0.5 * ekgE * q * pzi;
+            gz += -0.5 * ekgE * q * K.k * (c[j] * yr + s[j] * yi);
+            gq += 0.5 * ekgE * (-2.0 * q - pzr);
+            Gx[j] += kx * gth;
+            Gy[j] += ky * gth;
+            Gz[j] += gz;
+            Gq[j] += gq;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int m = m0 + j;
+        if (m < N) {
+            double *o = Gpart + ((int64_t)ks * N + m) * 4;
+            o[0] = Gx[j]; o[1] = Gy[j]; o[2] = Gz[j]; o[3] = Gq[j];
+        }
+    }
+}
+
+// z-ordered cotangents and the k = 0 adjoint inputs: w1 = gF_z q, w2 = q z
+__global__ void k_ladj_prep(int N, const double *__restrict__ gF, const int *__restrict__ zperm,
+                            const double *__restrict__ qd, const double *__restrict__ zhd, double h,
+                            double *__restrict__ zgx, double *__restrict__ zgy, double *__restrict__ zgz,
+                            double *__restrict__ w1, double *__restrict__ w2)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    const int i = zperm[m];
+    const double gx = gF ? gF[3 * i] : 0.0, gy = gF ? gF[3 * i + 1] : 0.0, gz = gF ? gF[3 * i + 2] : 0.0;
+    zgx[m] = gx; zgy[m] = gy; zgz[m] = gz;
+    w1[m] = gz * qd[m];
+    w2[m] = qd[m] * (zhd[m] + h);
+}
+
+// gamma derivatives of the long range: sums over k in a fixed order
+__global__ void k_ladj_gsum(int P, const double *__restrict__ ggk, double *__restrict__ out)
+{
+    __shared__ double red[2][8];
+    double a = 0, b = 0;
+    for (int m = threadIdx.x; m < P; m += blockDim.x) { a += ggk[2 * m]; b += ggk[2 * m + 1]; }
+    for (int d = 16; d > 0; d >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, d);
+        b += __shfl_down_sync(0xffffffffu, b, d);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = a; red[1][threadIdx.x >> 5] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0, y = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) { x += red[0][w]; y += red[1][w]; }
+        out[0] = x;
+        out[1] = y;
+    }
+}
+
+// slices + k = 0 term (Force_long.jl:130-161, Energy_long_range_njit.py:25-44),
+// added in particle order
+__global__ void k_ladj_final(int N, int ks_n, const double *__restrict__ Gpart, const int *__restrict__ zperm,
+                             const double *__restrict__ qd, const double *__restrict__ zhd, double h,
+                             const double *__restrict__ qscan, const double *__restrict__ zgz,
+                             const double *__restrict__ w1, const double *__restrict__ s1,
+                             const double *__restrict__ w2, const double *__restrict__ s2, double fs, double es,
+                             double gE, double *__restrict__ gxyz, double *__restrict__ gq)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double gx = 0, gy = 0, gz = 0, gqm = 0;
+    for (int ks = 0; ks < ks_n; ks++) {
+        const double *o = Gpart + ((int64_t)ks * N + m) * 4;
+        gx += o[0]; gy += o[1]; gz += o[2]; gqm += o[3];
+    }
+    const double q = qd[m], Z = zhd[m] + h, Qb = qscan[m], Qa = (qscan[N] - Qb) - q;
+    // forces: F0_i = q_i (Q_below - Q_above) fs
+    const double w1_above = (s1[N] - s1[m]) - w1[m], w1_below = s1[m];
+    gqm += zgz[m] * (Qb - Qa) * fs + fs * (w1_above - w1_below);
+    // energy: E0_i = 2 q_i z_i (2 Q_below + q_i) es
+    const double w2_above = (s2[N] - s2[m]) - w2[m];
+    gz += gE * 2.0 * q * (2.0 * Qb + q) * es;
+    gqm += gE * es * (2.0 * Z * (2.0 * Qb + q) + 2.0 * q * Z + 4.0 * w2_above);
+    const int i = zperm[m];
+    gxyz[3 * i] += gx;
+    gxyz[3 * i + 1] += gy;
+    gxyz[3 * i + 2] += gz;
+    if (gq) gq[i] += gqm;
+}
+
 }  // namespace
 
 int qem_long_chunk(void) { return LCH; }
@@ -513,5 +899,30 @@ cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s)
 cudaError_t qem_launch_reduce_sum(const double *in, int n, double *out, cudaStream_t s)
 {
     k_reduce_sum<<<1, 1024, 0, s>>>(in, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffers &b, const LongAdjBuffers &a,
+                                double Lx, double Ly, double Lz, double g1, double g2, double eps0, const double *gF,
+                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s)
+{
+    if (N <= 0) return cudaSuccess;
+    const double h = 0.5 * Lz;
+    k_ladj_prep<<<nblk(N, 256), 256, 0, s>>>(N, gF, zperm, b.qd, b.zhd, h, a.zgx, a.zgy, a.zgz, a.w1, a.w2);
+    cudaError_t e = qem_scan_f64_excl(a.w1, a.s1, N, b.stmp, b.stmp_bytes, s);
+    if (e == cudaSuccess) e = qem_scan_f64_excl(a.w2, a.s2, N, b.stmp, b.stmp_bytes, s);
+    if (e != cudaSuccess) return e;
+    AdjIn in;
+    in.zgx = a.zgx; in.zgy = a.zgy; in.zgz = a.zgz; in.gE = gE;
+    if (P > 0) {
+        k_ladj_tot<<<dim3(nch, nblk(P, KPB)), LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, in, a.atot);
+        k_ladj_scan<<<nblk(P, 4), 128, 0, s>>>(P, nch, a.atot, a.aoff, b.Utot, b.kc, g1, g2, gE, a.lam, a.ggk);
+    }
+    k_ladj<<<dim3(nch, ks), LT, 0, s>>>(N, P, nch, ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.kin,
+                                        (const KForce<double> *)b.kf, b.off, a.aoff, a.lam, in, a.Gpart);
+    const double fs = 1.0 / (2.0 * Lx * Ly * eps0), es = -1.0 / (4.0 * eps0 * Lx * Ly);
+    k_ladj_final<<<nblk(N, 256), 256, 0, s>>>(N, ks, a.Gpart, zperm, b.qd, b.zhd, h, b.qscan, a.zgz, a.w1, a.s1,
+                                              a.w2, a.s2, fs, es, gE, gxyz, gq);
+    k_ladj_gsum<<<1, 256, 0, s>>>(P, a.ggk, a.gam);
     return cudaGetLastError();
 }

@@ -4,9 +4,10 @@
 
 xyz: (N, 3) float64 CUDA tensor, q: (N,) float64 CUDA tensor.  The forward
 evaluates the QEM energy and forces in one fused call on the tensors' device
-and stream (QEM_MEM_DEVICE: no host round trip).  The backward gives
-dL/dxyz = -dL/dE * F (forces are minus the energy gradient); gradients that
-flow into F itself need the second-derivative (adjoint) kernels and raise.
+and stream (QEM_MEM_DEVICE: no host round trip).  The backward runs the
+library's adjoint kernels (qem_backward) for L = gE * E + sum_i gF_i . F_i
+and returns dL/dxyz and dL/dq; it is the backward of the reference's
+python_lib use of these terms inside a torch model.
 """
 from __future__ import annotations
 
@@ -25,19 +26,17 @@ class QEMEnergyForces(torch.autograd.Function):
         qq = q.detach().to(torch.float64).contiguous()
         F = torch.empty_like(x)
         E = engine.forces_device(x, qq, F, terms=terms, energy=True)
-        ctx.save_for_backward(F)
+        ctx.save_for_backward(x, qq)
+        ctx.engine, ctx.terms = engine, terms
         Et = torch.tensor(E, dtype=torch.float64, device=xyz.device)
-        ctx.mark_non_differentiable(F)
         return Et, F
 
     @staticmethod
     def backward(ctx, gE, gF):
-        (F,) = ctx.saved_tensors
-        if gF is not None and bool(torch.any(gF != 0)):
-            raise NotImplementedError("gradients through the forces need the adjoint kernels")
-        gx = None
-        if ctx.needs_input_grad[0]:
-            gx = -gE * F
-        if ctx.needs_input_grad[1]:
-            raise NotImplementedError("charge gradients need the adjoint kernels")
-        return gx, None, None, None
+        x, qq = ctx.saved_tensors
+        gFc = gF.detach().to(torch.float64).contiguous() if gF is not None else None
+        gEv = float(gE) if gE is not None else 0.0
+        gx = torch.empty_like(x)
+        gq = torch.empty_like(qq) if ctx.needs_input_grad[1] else None
+        ctx.engine.backward_device(x, qq, gFc, gEv, gx, gq, terms=ctx.terms)
+        return (gx if ctx.needs_input_grad[0] else None), gq, None, None

@@ -101,3 +101,35 @@ def rel_err(F, Fref):
     nref = np.linalg.norm(Fref)
     rms = nref / np.sqrt(max(len(Fref), 1))
     return float(np.linalg.norm(d) / nref), float(np.max(np.linalg.norm(d, axis=1)) / rms)
+
+
+def main(argv=None):
+    """Run a few force evaluations of a workload on cuda:0 (profiling target).
+
+    python -m qem4molly_b200.workloads --config 2 --evals 3 --precision fp32
+    """
+    import argparse
+
+    import torch
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--config", type=int, default=2, choices=(1, 2, 3, 5))
+    ap.add_argument("--evals", type=int, default=3)
+    ap.add_argument("--precision", default="fp32", choices=("fp32", "fp64"))
+    ap.add_argument("--N", type=int, default=None, help="particle count (configs 2, 3, 5)")
+    a = ap.parse_args(argv)
+    make = {1: config1, 2: config2, 3: config3, 5: config5}[a.config]
+    cfg = make(N=a.N) if (a.N and a.config != 1) else make()
+    e = engine_for(cfg, a.precision)
+    dev = torch.device("cuda", 0)
+    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
+    q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
+    F = torch.empty_like(x)
+    for _ in range(a.evals):
+        e.forces_device(x, q, F)
+    torch.cuda.synchronize()
+    print(f"config {a.config}: N={len(cfg['q'])}, {a.evals} {a.precision} evaluations, |F|_max={F.abs().max().item():.6e}")
+
+
+if __name__ == "__main__":
+    main()
