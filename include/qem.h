@@ -205,8 +205,12 @@ qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
  * own pool, real-time loops).  Same result as qem_long_forces for the same
  * k-set: F (3N, overwritten) = Molly.forces(::QEM_long) with the rows k3
  * (P x (kx, ky, k), host memory) and normaliser sum_K.  xyz, q and F are
- * device memory of device p->device; work is ordered on `stream` and the call
- * synchronises it before returning.  Scratch lives in one fixed
+ * device memory of device p->device; work is ordered on `stream`.  Outside a
+ * stream capture the call synchronises the stream before returning and
+ * reports non-finite inputs; while `stream` is being captured it only
+ * enqueues its work (no read-back), so the call can be recorded in a graph;
+ * k3 must then be page-locked host memory (pageable copies cannot be
+ * captured).  Scratch lives in one fixed
  * QEM_NOALLOC_SCRATCH_BYTES device array inside libqem.so that every GPU
  * loading the library holds until exit; larger N or P are rejected with
  * QEM_ERR_ARG.  The first call on a device looks up that array's address and
@@ -217,6 +221,40 @@ qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
 #define QEM_NOALLOC_SCRATCH_BYTES (8u << 20)
 qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, const double *xyz, const double *q, int32_t P,
                                    const double *k3, double sum_K, double *F, void *stream);
+
+/* ---- batches of independent systems (many small slabs, one launch graph) ----
+ * A batch groups B handles (same device), system s with N[s] particles.  The
+ * batch calls take device arrays laid end to end: system s owns particles
+ * [off[s], off[s] + N[s]) of xyz (3 per particle), q, F and v, with off the
+ * exclusive prefix sum of N.  The handles stay owned by the caller.
+ *
+ * qem_batch_forces: forces of every system (terms as in qem_forces).  The
+ *   first call (and the first after a change of terms) runs each system
+ *   synchronously to size its buffers and upload its k-set; later calls only
+ *   enqueue work on `stream` (a pool of streams forked from it), allocate
+ *   nothing and can be captured into a CUDA graph.  Device status (pair-list
+ *   overflow, non-finite input, particle out of the slab) accumulates and is
+ *   reported by qem_batch_check, which synchronises `stream`.
+ * qem_batch_md: nsteps velocity-Verlet steps of every system (unit masses,
+ *   x += v dt + F dt^2 / 2, v += (F + F') dt / 2, x and y wrapped into the
+ *   box), with one step recorded once as a CUDA graph and replayed.  On
+ *   return xyz and v hold the final state and F the final forces; the call
+ *   synchronises and checks the status.  Neighbour lists are rebuilt every
+ *   step and each system keeps its current k-set for the whole run.
+ * qem_batch_autotune: times the graph-replayed force evaluation for stream
+ *   pool widths 1, 2, 4, ... up to min(B, 128) and keeps the fastest;
+ *   returns the width and its time per batch evaluation (ms). */
+typedef struct qem_batch qem_batch;
+qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t *N, qem_batch **out);
+void qem_batch_destroy(qem_batch *b);
+const char *qem_batch_last_error(const qem_batch *b);
+qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                            void *stream);
+qem_status qem_batch_check(qem_batch *b, void *stream);
+qem_status qem_batch_md(qem_batch *b, int32_t nsteps, double dt, double *xyz, double *v, const double *q, double *F,
+                        uint32_t terms, void *stream);
+qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                              void *stream, int32_t *width, double *ms_per_eval);
 
 /* Library identity (version string and the compiled CUDA architecture). */
 const char *qem_version(void);

@@ -296,6 +296,81 @@ class System:
     charges: np.ndarray
 
 
+class Batch:
+    """Independent systems evaluated together (qem_batch_* of libqem): one Engine
+    per system, device arrays laid end to end (system s owns particles
+    [off[s], off[s] + N[s])).  Keeps its engines alive."""
+
+    def __init__(self, engines, N):
+        self._lib = L.load()
+        self.engines = list(engines)
+        self.N = [int(n) for n in N]
+        if len(self.N) != len(self.engines):
+            raise ValueError("one particle count per engine")
+        self.off = np.concatenate([[0], np.cumsum(self.N)[:-1]]).astype(np.int64)
+        hs = (C.c_void_p * len(self.engines))(*[e._h.value for e in self.engines])
+        ns = (C.c_int32 * len(self.N))(*self.N)
+        b = C.c_void_p()
+        st = self._lib.qem_batch_create(len(self.engines), hs, ns, C.byref(b))
+        if st != 0:
+            raise L.QemError(st, "qem_batch_create failed")
+        self._b = b
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.qem_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise L.QemError(st, self._lib.qem_batch_last_error(self._b).decode())
+
+    @staticmethod
+    def _ptr(t):
+        import torch
+
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise ValueError("device tensors must be contiguous float64 CUDA tensors")
+        return C.c_void_p(t.data_ptr())
+
+    @staticmethod
+    def _stream(t, stream):
+        import torch
+
+        return C.c_void_p(stream if stream is not None else torch.cuda.current_stream(t.device).cuda_stream)
+
+    def forces(self, xyz, q, F, terms=L.QEM_TERM_ALL, stream=None):
+        """Batched forces into F (asynchronous after the first call; see check())."""
+        self._check(self._lib.qem_batch_forces(self._b, self._ptr(xyz), self._ptr(q), self._ptr(F), int(terms),
+                                               self._stream(xyz, stream)))
+
+    def check(self, stream=None):
+        """Synchronises the stream and raises on any device status recorded since the last check."""
+        import torch
+
+        s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        self._check(self._lib.qem_batch_check(self._b, s))
+
+    def md(self, nsteps, dt, xyz, v, q, F, terms=L.QEM_TERM_ALL, stream=None):
+        """nsteps graph-replayed velocity-Verlet steps (unit masses) in place."""
+        self._check(self._lib.qem_batch_md(self._b, int(nsteps), float(dt), self._ptr(xyz), self._ptr(v),
+                                           self._ptr(q), self._ptr(F), int(terms), self._stream(xyz, stream)))
+
+    def autotune(self, xyz, q, F, terms=L.QEM_TERM_ALL, stream=None):
+        """Chooses the stream-pool width; returns (width, ms per batch evaluation)."""
+        w = C.c_int32()
+        ms = C.c_double()
+        self._check(self._lib.qem_batch_autotune(self._b, self._ptr(xyz), self._ptr(q), self._ptr(F), int(terms),
+                                                 self._stream(xyz, stream), C.byref(w), C.byref(ms)))
+        return w.value, ms.value
+
+
 def forces(inter, sys, neighbors=None):
     """Molly.forces(inter, sys, neighbors) for QEM_short / QEM_long / Substrate_LJ (N x 3)."""
     xyz, q = np.asarray(sys.coords, dtype=np.float64), np.asarray(sys.charges, dtype=np.float64)

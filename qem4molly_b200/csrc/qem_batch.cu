@@ -1,0 +1,341 @@
+// qem_batch.cu -- batches of independent systems: asynchronous batched force
+// evaluation on a pool of streams, a velocity-Verlet step recorded once as a
+// CUDA graph and replayed, and an autotuner for the stream-pool width.
+//
+// Reference: the MD setups of test/QEM_test.jl:40-60 (Molly VelocityVerlet
+// over QEM_short + QEM_long + Substrate_LJ) run one system at a time; the
+// batch runs many small slabs together.  Each system keeps its own handle
+// (parameters, k-set, neighbour list); the systems' kernels are small (a few
+// thousand particles), so the batch's speed comes from running their
+// pipelines concurrently and from replaying one recorded graph per MD step
+// instead of issuing some forty launches per system from the host.
+#include <algorithm>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "qem_internal.cuh"
+
+namespace {
+
+// x += v dt + F dt^2 / 2 (unit masses), x and y wrapped into [0, L)
+__global__ void k_vv_drift(int n, double *__restrict__ x, const double *__restrict__ v,
+                           const double *__restrict__ F, double dt, const int *__restrict__ sys,
+                           const double *__restrict__ box)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = sys[i];
+    for (int c = 0; c < 3; c++) x[3 * i + c] += dt * v[3 * i + c] + 0.5 * dt * dt * F[3 * i + c];
+    const double Lx = box[2 * s], Ly = box[2 * s + 1];
+    x[3 * i] -= Lx * floor(x[3 * i] / Lx);
+    x[3 * i + 1] -= Ly * floor(x[3 * i + 1] / Ly);
+}
+
+// v += (F + F') dt / 2, F = F'
+__global__ void k_vv_kick(int n3, double *__restrict__ v, double *__restrict__ F, const double *__restrict__ Fn,
+                          double dt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    const double fn = Fn[i];
+    v[i] += 0.5 * dt * (F[i] + fn);
+    F[i] = fn;
+}
+
+}  // namespace
+
+struct qem_batch {
+    int B = 0, Ntot = 0, device = 0;
+    std::vector<qem_handle *> h;
+    std::vector<int> N, off;
+    int W = 1;                          // stream-pool width in use
+    std::vector<cudaStream_t> pool;     // up to min(B, 128) streams
+    std::vector<cudaEvent_t> ev_done;
+    cudaEvent_t ev_start = nullptr;
+    cudaStream_t cap = nullptr;         // private stream the graphs are recorded on
+    bool warm = false;
+    uint32_t warm_terms = 0;
+    int *sys = nullptr;                 // particle -> system
+    double *box = nullptr;              // (Lx, Ly) per system
+    double *Fn = nullptr;               // forces at the new positions (MD)
+    cudaGraphExec_t md_exec = nullptr;  // one recorded MD step
+    const void *md_key[4] = {nullptr, nullptr, nullptr, nullptr};
+    double md_dt = 0;
+    uint32_t md_terms = 0;
+    int md_W = 0;
+    std::string err;
+};
+
+static qem_status bfail(qem_batch *b, qem_status s, const std::string &m)
+{
+    b->err = m;
+    return s;
+}
+
+#define BCU(call)                                                                                \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return bfail(b, QEM_ERR_CUDA, std::string(#call) + " -> " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// enqueue every system's evaluation on the pool, forked from and joined to s
+static qem_status enqueue_forces(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                                 cudaStream_t s)
+{
+    BCU(cudaEventRecord(b->ev_start, s));
+    for (int w = 0; w < b->W; w++) BCU(cudaStreamWaitEvent(b->pool[w], b->ev_start, 0));
+    for (int i = 0; i < b->B; i++) {
+        const size_t o = (size_t)b->off[i];
+        const qem_status st =
+            qem_forces_async(b->h[i], b->N[i], xyz + 3 * o, q + o, F + 3 * o, terms, b->pool[i % b->W]);
+        if (st != QEM_OK)
+            return bfail(b, st, "system " + std::to_string(i) + ": " + qem_handle_error(b->h[i]));
+    }
+    for (int w = 0; w < b->W; w++) {
+        BCU(cudaEventRecord(b->ev_done[w], b->pool[w]));
+        BCU(cudaStreamWaitEvent(s, b->ev_done[w], 0));
+    }
+    return QEM_OK;
+}
+
+static void drop_md_graph(qem_batch *b)
+{
+    if (b->md_exec) cudaGraphExecDestroy(b->md_exec);
+    b->md_exec = nullptr;
+}
+
+extern "C" {
+
+qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t *N, qem_batch **out)
+{
+    if (!out || B <= 0 || !handles || !N) return QEM_ERR_ARG;
+    *out = nullptr;
+    qem_batch *b = new qem_batch();
+    b->B = B;
+    b->device = qem_handle_params(handles[0])->device;
+    int64_t tot = 0;
+    for (int i = 0; i < B; i++) {
+        if (!handles[i] || N[i] < 0 || qem_handle_params(handles[i])->device != b->device) {
+            delete b;
+            return QEM_ERR_ARG;
+        }
+        b->h.push_back(handles[i]);
+        b->N.push_back(N[i]);
+        b->off.push_back((int)tot);
+        tot += N[i];
+    }
+    if (tot > (1 << 30)) {
+        delete b;
+        return QEM_ERR_ARG;
+    }
+    b->Ntot = (int)tot;
+    if (cudaSetDevice(b->device) != cudaSuccess) {
+        delete b;
+        return QEM_ERR_CUDA;
+    }
+    const int np = std::min(B, 128);
+    bool ok = cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) == cudaSuccess;
+    for (int w = 0; ok && w < np; w++) {
+        cudaStream_t s;
+        cudaEvent_t e;
+        ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+        if (ok) b->pool.push_back(s);
+        ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+        if (ok) b->ev_done.push_back(e);
+    }
+    std::vector<int> sys(std::max(b->Ntot, 1));
+    std::vector<double> box(2 * B);
+    for (int i = 0; i < B; i++) {
+        for (int k = 0; k < N[i]; k++) sys[b->off[i] + k] = i;
+        box[2 * i] = qem_handle_params(handles[i])->Lx;
+        box[2 * i + 1] = qem_handle_params(handles[i])->Ly;
+    }
+    ok = ok && cudaMalloc(&b->sys, sizeof(int) * sys.size()) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->box, sizeof(double) * box.size()) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->Fn, sizeof(double) * 3 * std::max(b->Ntot, 1)) == cudaSuccess;
+    ok = ok && cudaMemcpy(b->sys, sys.data(), sizeof(int) * sys.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && cudaMemcpy(b->box, box.data(), sizeof(double) * box.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        qem_batch_destroy(b);
+        return QEM_ERR_CUDA;
+    }
+    b->W = np;
+    *out = b;
+    return QEM_OK;
+}
+
+void qem_batch_destroy(qem_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    drop_md_graph(b);
+    for (cudaStream_t s : b->pool) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    for (cudaEvent_t e : b->ev_done) cudaEventDestroy(e);
+    if (b->ev_start) cudaEventDestroy(b->ev_start);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->sys) cudaFree(b->sys);
+    if (b->box) cudaFree(b->box);
+    if (b->Fn) cudaFree(b->Fn);
+    delete b;
+}
+
+const char *qem_batch_last_error(const qem_batch *b) { return b ? b->err.c_str() : "NULL batch"; }
+
+qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                            void *stream)
+{
+    if (!b || !xyz || !q || !F || (terms & ~QEM_TERM_ALL)) return b ? bfail(b, QEM_ERR_ARG, "bad argument") : QEM_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->warm || b->warm_terms != terms) {
+        // size every system's buffers and upload its k-set (synchronous)
+        for (int i = 0; i < b->B; i++) {
+            const size_t o = (size_t)b->off[i];
+            const qem_status st =
+                qem_forces(b->h[i], b->N[i], xyz + 3 * o, q + o, F + 3 * o, nullptr, terms, QEM_MEM_DEVICE, s);
+            if (st != QEM_OK) return bfail(b, st, "system " + std::to_string(i) + ": " + qem_handle_error(b->h[i]));
+        }
+        b->warm = true;
+        b->warm_terms = terms;
+        drop_md_graph(b);
+        return QEM_OK;
+    }
+    return enqueue_forces(b, xyz, q, F, terms, s);
+}
+
+qem_status qem_batch_check(qem_batch *b, void *stream)
+{
+    if (!b) return QEM_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    BCU(cudaStreamSynchronize(s));
+    for (int i = 0; i < b->B; i++) {
+        const qem_status st = qem_status_check(b->h[i], s);
+        if (st != QEM_OK) return bfail(b, st, "system " + std::to_string(i) + ": " + qem_handle_error(b->h[i]));
+    }
+    b->err.clear();
+    return QEM_OK;
+}
+
+qem_status qem_batch_md(qem_batch *b, int32_t nsteps, double dt, double *xyz, double *v, const double *q, double *F,
+                        uint32_t terms, void *stream)
+{
+    if (!b || nsteps < 0 || !xyz || !v || !q || !F || !(dt == dt)) return b ? bfail(b, QEM_ERR_ARG, "bad argument") : QEM_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    // forces at the initial positions (sizes the buffers on the first call)
+    qem_status st = qem_batch_forces(b, xyz, q, F, terms, s);
+    if (st != QEM_OK) return st;
+    if (b->warm_terms != terms) return bfail(b, QEM_ERR_ARG, "terms changed");
+    const void *key[4] = {xyz, v, q, F};
+    if (b->md_exec && (!std::equal(key, key + 4, b->md_key) || b->md_dt != dt || b->md_terms != terms || b->md_W != b->W))
+        drop_md_graph(b);
+    if (!b->md_exec && nsteps > 0) {
+        const int n = b->Ntot, T = 256;
+        // recorded on the batch's own stream (the caller's may be the legacy
+        // default stream, which cannot be captured) and launched on s
+        cudaStream_t c = b->cap;
+        cudaGraph_t g = nullptr;
+        BCU(cudaStreamSynchronize(s));
+        BCU(cudaStreamBeginCapture(c, cudaStreamCaptureModeThreadLocal));
+        k_vv_drift<<<(n + T - 1) / T, T, 0, c>>>(n, xyz, v, F, dt, b->sys, b->box);
+        st = enqueue_forces(b, xyz, q, b->Fn, terms, c);
+        k_vv_kick<<<(3 * n + T - 1) / T, T, 0, c>>>(3 * n, v, F, b->Fn, dt);
+        const cudaError_t ec = cudaStreamEndCapture(c, &g);
+        if (st != QEM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (ec != cudaSuccess) return bfail(b, QEM_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&b->md_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            b->md_exec = nullptr;
+            return bfail(b, QEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        std::copy(key, key + 4, b->md_key);
+        b->md_dt = dt;
+        b->md_terms = terms;
+        b->md_W = b->W;
+    }
+    for (int k = 0; k < nsteps; k++) BCU(cudaGraphLaunch(b->md_exec, s));
+    return qem_batch_check(b, stream);
+}
+
+qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                              void *stream, int32_t *width, double *ms_per_eval)
+{
+    if (!b) return QEM_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    qem_status st = qem_batch_forces(b, xyz, q, F, terms, s);
+    if (st != QEM_OK) return st;
+    const int wmax = (int)b->pool.size();
+    std::vector<int> cand;
+    for (int w = 1; w < wmax; w *= 2) cand.push_back(w);
+    cand.push_back(wmax);
+    cudaEvent_t t0, t1;
+    BCU(cudaEventCreate(&t0));
+    BCU(cudaEventCreate(&t1));
+    int best_w = b->W;
+    float best = 1e30f;
+    const int W0 = b->W;
+    for (int w : cand) {
+        b->W = w;
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        BCU(cudaStreamSynchronize(s));
+        BCU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_forces(b, xyz, q, F, terms, b->cap);
+        const cudaError_t ec = cudaStreamEndCapture(b->cap, &g);
+        if (st != QEM_OK || ec != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            b->W = W0;
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            return st != QEM_OK ? st : bfail(b, QEM_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ec));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            b->W = W0;
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            return bfail(b, QEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        const int reps = 5;
+        cudaError_t e = cudaGraphLaunch(ex, s);  // warm-up
+        e = e == cudaSuccess ? cudaEventRecord(t0, s) : e;
+        for (int r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(ex, s);
+        e = e == cudaSuccess ? cudaEventRecord(t1, s) : e;
+        e = e == cudaSuccess ? cudaEventSynchronize(t1) : e;
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+        cudaGraphExecDestroy(ex);
+        if (e != cudaSuccess) {
+            b->W = W0;
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            return bfail(b, QEM_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(e));
+        }
+        ms /= reps;
+        if (ms < best) {
+            best = ms;
+            best_w = w;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    b->W = best_w;
+    drop_md_graph(b);
+    if (width) *width = best_w;
+    if (ms_per_eval) *ms_per_eval = best;
+    return qem_batch_check(b, stream);
+}
+
+}  // extern "C"

@@ -17,9 +17,14 @@ struct DevBuf {
     size_t cap = 0;
 };
 
+// set while enqueuing asynchronous (capturable) work: a buffer that would
+// have to grow is an error there, as cudaMalloc / cudaFree cannot be captured
+thread_local bool g_no_alloc = false;
+
 cudaError_t grow(DevBuf &b, size_t bytes)
 {
     if (bytes <= b.cap && b.p) return cudaSuccess;
+    if (g_no_alloc) return cudaErrorMemoryAllocation;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
@@ -403,8 +408,15 @@ static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s
 // ---------------------------------------------------------------------------
 // retry = true asks the caller to evaluate again (the pair list outgrew its
 // capacity, which has been enlarged).
+//
+// async = true enqueues the evaluation only (device memory, no energy): no
+// host synchronisation, no allocation, no k-set sampling or upload and a
+// pair-list rebuild on every call, so that the work can be captured into a
+// CUDA graph; the device status word then accumulates over calls and is
+// checked (and cleared) by qem_batch_check.  A synchronous call of the same
+// size must have run first.
 static qem_status run_once(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
-                           uint32_t terms, int mem, cudaStream_t s, bool &retry)
+                           uint32_t terms, int mem, cudaStream_t s, bool &retry, bool async = false)
 {
     retry = false;
     if (!h) return QEM_ERR_ARG;
@@ -421,8 +433,22 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         return QEM_OK;
     }
     if (!xyz || !q || !F) return fail(h, QEM_ERR_ARG, "NULL coordinate, charge or force pointer");
+    if (async && (mem != QEM_MEM_DEVICE || energy)) return fail(h, QEM_ERR_ARG, "async evaluation: device memory, no energy");
     CU(cudaSetDevice(h->p.device));
     const int prec = h->p.precision;
+    const bool prof_on = h->prof.on;
+    if (async) h->prof.on = false;
+    struct Restore {
+        qem_handle *h;
+        bool prof;
+        bool async;
+        ~Restore()
+        {
+            h->prof.on = prof;
+            if (async) g_no_alloc = false;
+        }
+    } restore{h, prof_on, async};
+    if (async) g_no_alloc = true;
     h->prof.begin();
     int launches = 0;
     const int mk0 = h->prof.mark(s);
@@ -444,7 +470,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         F_d = ptr<double>(h->F);
     }
     unsigned *st = ptr<unsigned>(h->status);
-    CU(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+    if (!async) CU(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
     const int mk_in = h->prof.mark(s);
     CU(qem_launch_pack(N, xyz_d, q_d, ptr<double4>(h->pos), ptr<int>(h->cell), h->geom, st, s));
     launches++;
@@ -467,8 +493,14 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     int mk_lstart = -1, mk_lprep = -1, mk_lforce = -1;
     h->counts[2] = 0;
     if (do_long) {
-        if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
-        else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+        if (async) {
+            if ((h->p.rbe_p > 0 && !h->has_kset) || h->kset_dirty)
+                return fail(h, QEM_ERR_NO_KSET, "async evaluation: the k-set must be on the device (synchronous call first)");
+        } else if (!h->has_kset && h->p.rbe_p > 0) {
+            sample_kset(h, h->p.rbe_p);
+        } else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) {
+            sample_kset(h, h->p.rbe_p);
+        }
         const int Pk = h->has_kset ? h->P : 0;
         if (prec == QEM_FP32_FIX && Pk > 0 && h->kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
@@ -503,7 +535,8 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     int mk_bin = -1, mk_pair = -1, mk_gather = -1;
     if (do_short) {
         const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
-        const bool rebuild = !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
+        const bool rebuild =
+            async || !stale || !h->pairs_valid || h->pairs_N != N || (h->short_calls % h->p.iter_period) == 0;
         if (rebuild) {
             const qem_status bs = build_pairs(h, N, st, s);
             if (bs != QEM_OK) return bs;
@@ -538,6 +571,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         launches++;
         CU(cudaMemcpyAsync(h->h_E, h->Eout.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
+    if (async) return QEM_OK;
     if (mem == QEM_MEM_HOST) CU(cudaMemcpyAsync(F, F_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     if (do_short)
@@ -1031,3 +1065,30 @@ extern "C" qem_status qem_backward(qem_handle *h, int32_t N, const double *xyz, 
     if (st == QEM_OK && retry) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list outgrew its capacity twice");
     return st;
 }
+
+// ---------------------------------------------------------------------------
+// internal hooks of the batch API (qem_batch.cu)
+// ---------------------------------------------------------------------------
+qem_status qem_forces_async(qem_handle *h, int N, const double *xyz, const double *q, double *F, uint32_t terms,
+                            cudaStream_t s)
+{
+    bool retry = false;
+    return run_once(h, N, xyz, q, F, nullptr, terms, QEM_MEM_DEVICE, s, retry, true);
+}
+
+qem_status qem_status_check(qem_handle *h, cudaStream_t s)
+{
+    if (!h->status.p) return QEM_OK;
+    CU(cudaSetDevice(h->p.device));
+    CU(cudaMemcpyAsync(h->h_status, h->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemsetAsync(h->status.p, 0, sizeof(unsigned), s));
+    CU(cudaStreamSynchronize(s));
+    const unsigned stv = *h->h_status;
+    if (stv & QEM_ST_OVERFLOW) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list outgrew its capacity in an asynchronous call");
+    if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
+    if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    return QEM_OK;
+}
+
+const qem_params *qem_handle_params(const qem_handle *h) { return &h->p; }
+const char *qem_handle_error(const qem_handle *h) { return h->err.c_str(); }

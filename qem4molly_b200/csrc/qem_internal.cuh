@@ -138,6 +138,15 @@ int qem_long_chunk(void);
 
 cudaError_t qem_launch_reduce_sum(const double *in, int n, double *out, cudaStream_t s);
 
+// ---- batch API hooks (defined in qem_capi.cu) -------------------------------
+// capturable evaluation on device memory (see run_once in qem_capi.cu)
+qem_status qem_forces_async(qem_handle *h, int N, const double *xyz, const double *q, double *F, uint32_t terms,
+                            cudaStream_t s);
+// synchronises s, reads and clears the handle's device status word
+qem_status qem_status_check(qem_handle *h, cudaStream_t s);
+const qem_params *qem_handle_params(const qem_handle *h);
+const char *qem_handle_error(const qem_handle *h);
+
 // ---- adjoint (FP64) --------------------------------------------------------
 // pair records RA (2 double4 per pair) and the per-particle pass writing
 // dL/dr, dL/dq (gq may be NULL) and per-block gamma partials gam[2 * nb]
