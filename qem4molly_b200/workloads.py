@@ -15,6 +15,35 @@ def _slab(rng, N, Lx, Ly, zlo, zhi):
     return np.stack([rng.random(N) * Lx, rng.random(N) * Ly, zlo + rng.random(N) * (zhi - zlo)], axis=1)
 
 
+def _hard_core_slab(rng, N, Lx, Ly, zlo, zhi, dmin):
+    """Uniform slab positions, each redrawn until it is at least dmin (3-D,
+    minimum image in x and y) from every earlier particle."""
+    xyz = _slab(rng, N, Lx, Ly, zlo, zhi)
+    cell = max(dmin, 1e-9)
+    grid = {}
+    for i in range(N):
+        while True:
+            p = xyz[i]
+            cx, cy, cz = int(p[0] // cell), int(p[1] // cell), int(p[2] // cell)
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        for j in grid.get(((cx + dx) % max(1, int(Lx // cell)), (cy + dy) % max(1, int(Ly // cell)),
+                                           cz + dz), ()):
+                            d = xyz[j] - p
+                            d[0] -= Lx * np.rint(d[0] / Lx)
+                            d[1] -= Ly * np.rint(d[1] / Ly)
+                            if d @ d < dmin * dmin:
+                                ok = False
+            if ok:
+                break
+            xyz[i] = _slab(rng, 1, Lx, Ly, zlo, zhi)[0]
+        key = (cx % max(1, int(Lx // cell)), cy % max(1, int(Ly // cell)), cz)
+        grid.setdefault(key, []).append(i)
+    return xyz
+
+
 def _pm_charges(N):
     q = np.ones(N)
     q[N // 2:] = -1.0
@@ -58,7 +87,10 @@ def config3(seed=None, N=20_000):
 
 def config4(seed=None, n_systems=256):
     """256 independent slabs, N ~ U[200, 5000], Lz ~ U[5, 20], Lx=Ly from density 0.01,
-    gamma pairs ~ U(-0.95, 0.95)^2, alpha=0.1, r_c=10, P=200."""
+    gamma pairs ~ U(-0.95, 0.95)^2, alpha=0.1, r_c=10, P=200.  Positions are uniform
+    with a hard core of 1.0 (no two particles closer), so that the bare +-1 charges
+    (no Lennard-Jones core between particles) do not collapse onto each other within
+    a 1000-step, dt = 1e-3 velocity-Verlet run."""
     rng = np.random.default_rng(SEED0 + 4 if seed is None else seed)
     out = []
     for s in range(n_systems):
@@ -66,7 +98,7 @@ def config4(seed=None, n_systems=256):
         Lz = float(rng.uniform(5, 20))
         L = float(np.sqrt(N / 0.01))
         gu, gd = rng.uniform(-0.95, 0.95, 2)
-        out.append(dict(name=f"config4_sys{s}", N=N, L=(L, L, Lz), xyz=_slab(rng, N, L, L, 0.5, Lz - 0.5),
+        out.append(dict(name=f"config4_sys{s}", N=N, L=(L, L, Lz), xyz=_hard_core_slab(rng, N, L, L, 0.5, Lz - 0.5, 1.0),
                         q=_pm_charges(N), alpha=0.1, r_cutoff=10.0, gamma_up=float(gu), gamma_down=float(gd),
                         N_t=30, accuracy=1e-6, P=200, walls=[]))
     return out

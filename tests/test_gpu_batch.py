@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 def _setup(n_sys, prec="fp64", seed=None):
     import torch
 
-    cfgs = W.config4(seed=seed)[:n_sys]
+    cfgs = W.config4(seed=seed, n_systems=n_sys)
     engines = [W.engine_for(c, prec, seed=100 + i) for i, c in enumerate(cfgs)]
     N = [c["N"] for c in cfgs]
     dev = torch.device("cuda", 0)
