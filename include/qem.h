@@ -222,6 +222,16 @@ qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
 qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, const double *xyz, const double *q, int32_t P,
                                    const double *k3, double sum_K, double *F, void *stream);
 
+/* Sharding one system over `world` ranks (one GPU each): with rank r set, a
+ * call evaluates the pairs [Np r / W, Np (r + 1) / W) of the neighbour list,
+ * the k-set rows [P r / W, P (r + 1) / W) (weighted by the full sum_K / P),
+ * and, on rank 0 only, the self image terms, the walls and the k = 0 term;
+ * forces and energies of the W ranks then sum to the unsharded result (the
+ * caller's one exchange step: an all-reduce of F and E).  Every rank must
+ * hold the same positions, charges and k-set.  qem_backward ignores the
+ * shard and evaluates the whole system.  Default rank 0 of 1. */
+qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
+
 /* ---- batches of independent systems (many small slabs, one launch graph) ----
  * A batch groups B handles (same device), system s with N[s] particles.  The
  * batch calls take device arrays laid end to end: system s owns particles

@@ -97,6 +97,7 @@ def load(build: bool = False):
         "qem_version": (C.c_char_p, []),
         "qem_measure_peaks": (C.c_int32, [C.c_int32, dp, dp]),
         "qem_long_forces_noalloc": (C.c_int32, [PP, C.c_int32, vp, vp, C.c_int32, dp, C.c_double, vp, vp]),
+        "qem_set_shard": (C.c_int32, [H, C.c_int32, C.c_int32]),
         "qem_batch_create": (C.c_int32, [C.c_int32, C.POINTER(H), ip, C.POINTER(vp)]),
         "qem_batch_destroy": (None, [vp]),
         "qem_batch_last_error": (C.c_char_p, [vp]),

@@ -86,6 +86,11 @@ class Engine:
         if st != 0:
             raise L.QemError(st, self._lib.qem_last_error(self._h).decode())
 
+    def set_shard(self, rank, world):
+        """Evaluate this rank's share of one system (see qem_set_shard); the W
+        ranks' forces and energies sum to the unsharded result."""
+        self._check(self._lib.qem_set_shard(self._h, int(rank), int(world)))
+
     # -- k-set -----------------------------------------------------------------
     def set_kset(self, k3, sum_K):
         k3 = np.ascontiguousarray(k3, dtype=np.float64).reshape(-1, 3)

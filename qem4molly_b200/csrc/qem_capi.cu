@@ -128,6 +128,9 @@ struct qem_handle {
     double sum_K = 0;
     int P = 0;
     bool has_kset = false, kset_dirty = true;
+    int kin_lo = 0, kin_hi = -1;  // rows of the k-set currently in the device copy
+    // sharding of one system over ranks (qem_set_shard)
+    int shard_rank = 0, shard_world = 1;
     uint64_t rng = 0x51ed5eedULL;
     std::vector<double> cdfx, cdfy;
     long mxmax = 0, mymax = 0;
@@ -232,6 +235,8 @@ static void build_consts(qem_handle *h)
     const qem_params &p = h->p;
     ShortConsts &c = h->sc;
     memset(&c, 0, sizeof(c));
+    c.shard_rank = h->shard_rank;
+    c.shard_world = h->shard_world;
     c.Lx = p.Lx; c.Ly = p.Ly; c.invLx = 1.0 / p.Lx; c.invLy = 1.0 / p.Ly;
     c.Lz = p.Lz; c.twoLz = 2.0 * p.Lz;
     c.alpha = p.alpha; c.inv4alpha = 1.0 / (4.0 * p.alpha);
@@ -501,32 +506,43 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         } else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) {
             sample_kset(h, h->p.rbe_p);
         }
-        const int Pk = h->has_kset ? h->P : 0;
-        if (prec == QEM_FP32_FIX && Pk > 0 && h->kmax * h->p.Lz > 120.0)
+        const int Pall = h->has_kset ? h->P : 0;
+        if (prec == QEM_FP32_FIX && Pall > 0 && h->kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
+        // this rank's rows of the k-set, weighted as part of all Pall rows
+        const int k_lo = (int)((int64_t)Pall * h->shard_rank / h->shard_world);
+        const int k_hi = (int)((int64_t)Pall * (h->shard_rank + 1) / h->shard_world);
+        const int Pk = k_hi - k_lo;
+        const double sumK_eff = Pall > 0 ? h->sum_K * Pk / Pall : 0.0;
+        if (async && (h->kin_lo != k_lo || h->kin_hi != k_hi))
+            return fail(h, QEM_ERR_NO_KSET, "async evaluation: the k-set rows must be on the device (synchronous call first)");
         LongBuffers b;  // allocated before any launch or copy that uses them
         {
             const qem_status ls = long_buffers(h, N, Pk, nch, ks, Ep, nbS, nb0, b);
             if (ls != QEM_OK) return ls;
         }
+        b.skip_k0 = h->shard_rank != 0;
         if (concurrent) {  // fork after pack (positions) and the energy-partial clear
             CU(cudaEventRecord(h->ev_fork, s));
             CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
         }
         mk_lstart = h->prof.mark(sl);
-        if (h->kset_dirty && Pk > 0) {
-            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, sl));
+        if ((h->kset_dirty || h->kin_lo != k_lo || h->kin_hi != k_hi) && Pk > 0) {
+            CU(cudaMemcpyAsync(h->kin.p, h->kset.data() + 3 * (size_t)k_lo, sizeof(double) * 3 * Pk,
+                               cudaMemcpyHostToDevice, sl));
             h->kset_dirty = false;
+            h->kin_lo = k_lo;
+            h->kin_hi = k_hi;
         }
         double *FL = concurrent ? ptr<double>(h->Flong) : F_d;
         CU(cudaMemsetAsync(FL, 0, sizeof(double) * 3 * N, sl));
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
                             ptr<double>(h->zkey2), sl));
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
-                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, FL, nch, st, sl, 0));
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 0));
         mk_lprep = h->prof.mark(sl);
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
-                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, FL, nch, st, sl, 1));
+                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 1));
         mk_lforce = h->prof.mark(sl);
         launches += 22;
         h->counts[2] = Pk;
@@ -983,9 +999,11 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
             const qem_status ls = long_buffers(h, N, Pk, nch, ks, ptr<double>(h->Epart), nbS, nb0, b);
             if (ls != QEM_OK) return ls;
         }
-        if (h->kset_dirty && Pk > 0) {
+        if ((h->kset_dirty || h->kin_lo != 0 || h->kin_hi != Pk) && Pk > 0) {
             CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
             h->kset_dirty = false;
+            h->kin_lo = 0;
+            h->kin_hi = Pk;
         }
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
                             ptr<double>(h->zkey2), s));
@@ -1092,3 +1110,16 @@ qem_status qem_status_check(qem_handle *h, cudaStream_t s)
 
 const qem_params *qem_handle_params(const qem_handle *h) { return &h->p; }
 const char *qem_handle_error(const qem_handle *h) { return h->err.c_str(); }
+
+extern "C" qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (world < 1 || world > 4096 || rank < 0 || rank >= world)
+        return fail(h, QEM_ERR_ARG, "shard rank must be in 0 .. world - 1, world in 1 .. 4096");
+    h->shard_rank = rank;
+    h->shard_world = world;
+    h->sc.shard_rank = rank;
+    h->sc.shard_world = world;
+    h->err.clear();
+    return QEM_OK;
+}

@@ -29,13 +29,14 @@ struct ShortConsts {
     int Nt;
     uint32_t flags;       // QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL
     int n_walls;
-    int pad;
+    int shard_rank;       // this rank evaluates pairs [Np r / W, Np (r + 1) / W) of the list
+
     double wall_cut[2], wall_sig2[2], wall_eps[2], wall_pos[2], wall_dir[2];
     // Gauss-Legendre nodes/weights on [-1, 1]: FP32 as node pairs (2m, 2m+1)
     // for the packed FP32x2 loop, an odd N_t padded with (x = -1, w = 0),
     // i.e. a node at k = 0 of weight zero; FP64 as plain arrays
     int Nt2;              // (N_t + 1) / 2
-    int pad2;
+    int shard_world;      // W >= 1; the self terms and walls belong to rank 0
     float2 xf2[QEM_MAX_NT / 2], wf2[QEM_MAX_NT / 2];
     double xd[QEM_MAX_NT], wd[QEM_MAX_NT];
 };
@@ -126,6 +127,7 @@ struct LongBuffers {
     int ks;               // number of k slices of the force pass
     void *stmp;           // scan scratch
     size_t stmp_bytes;
+    int skip_k0 = 0;      // 1: leave out the k = 0 term (sharded ranks other than 0)
 };
 // number of k slices for nch chunks and P k-vectors (at most max_ks)
 int qem_long_ksplit(int nch, int P, int max_ks);

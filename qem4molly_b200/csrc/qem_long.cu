@@ -844,8 +844,8 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd);
         cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
         if (e != cudaSuccess) return e;
-        const double fscale = 1.0 / (2.0 * Lx * Ly * eps0);
-        const double escale = -1.0 / (4.0 * eps0 * Lx * Ly);
+        const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
+        const double escale = b.skip_k0 ? 0.0 : -1.0 / (4.0 * eps0 * Lx * Ly);
         k_k0<<<nblk(N, 256), 256, 0, s>>>(N, b.qd, b.zhd, h, b.qscan, fscale, escale, b.k0, b.Epart + b.ks * nch,
                                           energy ? 1 : 0);
         if (P > 0) {

@@ -192,11 +192,13 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
     __shared__ int sidx[PAIR_BLOCK];
     const int64_t Np = min(*np, cap);
     if ((int64_t)blockIdx.x * PAIR_BLOCK >= Np) return;  // whole block: before any barrier
+    // this rank's block of the pair list (all of it unless sharded)
+    const int64_t lo = Np * c.shard_rank / c.shard_world, hi = Np * (c.shard_rank + 1) / c.shard_world;
     // 1. every thread loads one pair and its rho^2; order the block's pairs by rho^2
     {
         const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + threadIdx.x;
         double key = 1e300;
-        if (p < Np) {
+        if (p >= lo && p < hi) {
             const int2 ij = pairs[p];
             const double4 pi = pos[ij.x], pj = pos[ij.y];
             const double dx = min_image(pi.x - pj.x, c.Lx, c.invLx), dy = min_image(pi.y - pj.y, c.Ly, c.invLy);
@@ -224,6 +226,11 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
     }
     const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + sidx[threadIdx.x];
     if (p >= Np) return;
+    if (p < lo || p >= hi) {  // another rank's pair
+        R[p] = make_double4(0, 0, 0, 0);
+        if (ENERGY) Upair[p] = 0;
+        return;
+    }
     // stored as (owner, other); evaluated as F_short_ij with i the lower index
     // (the canonical orientation of QEM_short.jl:41-47), recorded for the owner
     const int2 oo = pairs[p];
@@ -345,12 +352,14 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
                 const double4 r = R[in_list[s]];
                 Fx -= r.x; Fy -= r.y; Fz += r.w;
             }
-            double fz_self = 0, e_self = 0;
-            self_terms<PREC, ENERGY>(c, pi.z, pi.w, fz_self, e_self);
-            Fz += fz_self;
-            if (ENERGY) E += e_self;
+            if (c.shard_rank == 0) {
+                double fz_self = 0, e_self = 0;
+                self_terms<PREC, ENERGY>(c, pi.z, pi.w, fz_self, e_self);
+                Fz += fz_self;
+                if (ENERGY) E += e_self;
+            }
         }
-        if (do_lj) {
+        if (do_lj && c.shard_rank == 0) {
             for (int w = 0; w < c.n_walls; w++) {
                 const double dz = pi.z - c.wall_pos[w];
                 if (!(c.wall_dir[w] * dz > 0)) {  // Substrate_LJ.jl:37
