@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_gather(int N, const double4 *
                                                            const int64_t *__restrict__ poff,
                                                            const double4 *__restrict__ RA,
                                                            const int64_t *__restrict__ in_off,
-                                                           const int64_t *__restrict__ in_list, int64_t cap,
+                                                           const int *__restrict__ in_list, int64_t cap,
                                                            const double *__restrict__ gF, double gE,
                                                            const ShortConsts c, double *__restrict__ gxyz,
                                                            double *__restrict__ gq, double *__restrict__ gam,
@@ -318,7 +318,7 @@ cudaError_t qem_launch_short_pair_adj(const int64_t *np, int64_t cap, const int2
 
 cudaError_t qem_launch_adj_gather(int N, bool do_short, bool do_lj, const double4 *pos, const int *pos_of,
                                   const int64_t *poff, const double4 *RA, const int64_t *in_off,
-                                  const int64_t *in_list, int64_t cap, const double *gF, double gE,
+                                  const int *in_list, int64_t cap, const double *gF, double gE,
                                   const ShortConsts &c, double *gxyz, double *gq, double *gam, cudaStream_t s)
 {
     if (N <= 0) return cudaSuccess;

@@ -239,12 +239,15 @@ __global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__res
 // pair list (j > i, minimum-image rho^2 <= r_c^2)
 // ---------------------------------------------------------------------------
 // rho^2 with explicitly rounded operations so that the in/out decision is
-// bit-identical to an unfused CPU evaluation of the same expression.
+// bit-identical to an unfused CPU evaluation of the same expression.  The
+// image shift n = rint(d / L) is taken as rint(d * (1 / L)): the two differ
+// only where d / L lies within rounding of +-1/2, i.e. |d| ~ L / 2 > r_c,
+// where both shifts leave the pair out of range.
 __device__ __forceinline__ double rho2_exact(double4 a, double4 b, const CellGeom &g)
 {
     double dx = __dsub_rn(a.x, b.x), dy = __dsub_rn(a.y, b.y);
-    dx = __dsub_rn(dx, __dmul_rn(g.Lx, rint(dx / g.Lx)));
-    dy = __dsub_rn(dy, __dmul_rn(g.Ly, rint(dy / g.Ly)));
+    dx = __dsub_rn(dx, __dmul_rn(g.Lx, rint(dx * g.invLx)));
+    dy = __dsub_rn(dy, __dmul_rn(g.Ly, rint(dy * g.invLy)));
     return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
 }
 
@@ -318,21 +321,21 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__r
 // the pair count lives on the device (*np = poff[N]); grids are sized for
 // the capacity and threads beyond the count return
 __global__ void k_in_fill(const int64_t *__restrict__ np, int64_t cap, const int2 *__restrict__ pairs,
-                          const int64_t *__restrict__ off, int *fill, int64_t *__restrict__ list)
+                          const int64_t *__restrict__ off, int *fill, int *__restrict__ list)
 {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= *np || p >= cap) return;
     const int j = pairs[p].y;
-    list[off[j] + atomicAdd(&fill[j], 1)] = p;
+    list[off[j] + atomicAdd(&fill[j], 1)] = (int)p;
 }
 
 // incoming lists in ascending pair order; one warp per particle
-__global__ void k_in_sort(int N, const int64_t *__restrict__ off, int64_t *__restrict__ list)
+__global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restrict__ list)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= N) return;
-    warp_sort_segment<long long>((long long *)list, off[i], off[i + 1], lane, 0x7fffffffffffffffLL);
+    warp_sort_segment<int>(list, off[i], off[i + 1], lane, 0x7fffffff);
 }
 
 // ---------------------------------------------------------------------------
@@ -501,7 +504,7 @@ cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, c
 }
 
 cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
-                                int64_t *in_off, int *in_fill, int64_t *in_list, void *scan_tmp,
+                                int64_t *in_off, int *in_fill, int *in_list, void *scan_tmp,
                                 size_t scan_tmp_bytes, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(in_fill, 0, sizeof(int) * N, s);

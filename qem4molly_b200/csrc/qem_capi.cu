@@ -389,7 +389,8 @@ static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s
     CU(grow(h->in_cnt, sizeof(int) * N));
     CU(grow(h->in_fill, sizeof(int) * N));
     CU(grow(h->in_off, sizeof(int64_t) * (N + 1)));
-    CU(grow(h->in_list, sizeof(int64_t) * cap));
+    if (cap > INT32_MAX) return fail(h, QEM_ERR_NB_OVERFLOW, "more than 2^31 - 1 pairs");
+    CU(grow(h->in_list, sizeof(int) * cap));
     CU(qem_launch_cells(N, h->ncell, ptr<int>(h->cell), ptr<double4>(h->pos), ptr<int>(h->cell_cnt),
                         ptr<int>(h->cell_start), ptr<int>(h->cell_fill), ptr<int>(h->cell_list),
                         ptr<int>(h->pos_of), ptr<double4>(h->pos_c), h->scan_tmp.p, h->scan_tmp.cap, s));
@@ -401,7 +402,7 @@ static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s
                             ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int64_t>(h->poff),
                             ptr<int2>(h->pairs), cap, ptr<int>(h->in_cnt), st, s));
     CU(qem_launch_incoming(N, ptr<int64_t>(h->poff) + N, cap, ptr<int2>(h->pairs), ptr<int>(h->in_cnt),
-                           ptr<int64_t>(h->in_off), ptr<int>(h->in_fill), ptr<int64_t>(h->in_list),
+                           ptr<int64_t>(h->in_off), ptr<int>(h->in_fill), ptr<int>(h->in_list),
                            h->scan_tmp.p, h->scan_tmp.cap, s));
     h->pairs_N = N;
     h->pairs_valid = true;
@@ -568,7 +569,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     if (do_short || do_lj) {
         CU(qem_launch_short_gather(prec, want_E, do_short, do_lj, N, ptr<double4>(h->pos), ptr<int>(h->pos_of),
                                    ptr<int64_t>(h->poff), ptr<double4>(h->R), ptr<double>(h->Upair),
-                                   ptr<int64_t>(h->in_off), ptr<int64_t>(h->in_list), h->pair_cap, h->sc, F_d, Ep,
+                                   ptr<int64_t>(h->in_off), ptr<int>(h->in_list), h->pair_cap, h->sc, F_d, Ep,
                                    st, s));
         launches++;
     } else if (!do_long) {  // (a long-only call has already zeroed F_d in front of its kernels)
@@ -978,7 +979,7 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         CU(grow(h->gam, sizeof(double) * 2 * nb));
         CU(qem_launch_adj_gather(N, do_short, do_lj, ptr<double4>(h->pos), ptr<int>(h->pos_of),
                                  ptr<int64_t>(h->poff), ptr<double4>(h->RA), ptr<int64_t>(h->in_off),
-                                 ptr<int64_t>(h->in_list), h->pair_cap, gF_d, gE, h->sc, gx_d, gq_d,
+                                 ptr<int>(h->in_list), h->pair_cap, gF_d, gE, h->sc, gx_d, gq_d,
                                  ptr<double>(h->gam), s));
         CU(qem_launch_reduce_sum(ptr<double>(h->gam), nb, gout, s));
         CU(qem_launch_reduce_sum(ptr<double>(h->gam) + nb, nb, gout + 1, s));

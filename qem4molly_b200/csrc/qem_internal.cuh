@@ -88,7 +88,7 @@ cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, c
                                  int64_t cap, int *in_cnt, unsigned *status, cudaStream_t s);
 // np: device pointer to the pair count (poff[N])
 cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
-                                int64_t *in_off, int *in_fill, int64_t *in_list, void *scan_tmp,
+                                int64_t *in_off, int *in_fill, int *in_list, void *scan_tmp,
                                 size_t scan_tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
@@ -100,7 +100,7 @@ cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np
                                    cudaStream_t s);
 cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, bool do_lj, int N,
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
-                                    const double *Upair, const int64_t *in_off, const int64_t *in_list, int64_t cap,
+                                    const double *Upair, const int64_t *in_off, const int *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s);
 
@@ -158,7 +158,7 @@ cudaError_t qem_launch_short_pair_adj(const int64_t *np, int64_t cap, const int2
                                       cudaStream_t s);
 cudaError_t qem_launch_adj_gather(int N, bool do_short, bool do_lj, const double4 *pos, const int *pos_of,
                                   const int64_t *poff, const double4 *RA, const int64_t *in_off,
-                                  const int64_t *in_list, int64_t cap, const double *gF, double gE,
+                                  const int *in_list, int64_t cap, const double *gF, double gE,
                                   const ShortConsts &c, double *gxyz, double *gq, double *gam, cudaStream_t s);
 struct LongAdjBuffers {
     double *zgx, *zgy, *zgz;   // cotangents in z order

@@ -44,6 +44,14 @@ constexpr int LKB = 8;          // k-vectors per FP32 accumulation batch of the 
 #endif
 constexpr int LF_MINB = QEM_LF_MINB;  // resident FP32 force-pass blocks per SM (register budget)
 
+// t - round(t) for |t| < 2^51 turns: rounding by adding and subtracting
+// 1.5 * 2^52 (two FP64 adds)
+__device__ __forceinline__ double frac_turns(double t)
+{
+    const double M = 6755399441055744.0;
+    return t - ((t + M) - M);
+}
+
 template <typename Real>
 struct LM;
 template <>
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
             double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
-            t -= rint(t);
+            t = frac_turns(t);
             Real s, c;
             LM<Real>::sc(t, s, c);
             const Real kz = (Real)K.k * P4.z[j];
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(LT, sizeof(Real) == 4 ? LF_MINB : 4) k_lforce(
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
             double t = fma(kx2, P4.x[j], ky2 * P4.y[j]);
-            t -= rint(t);
+            t = frac_turns(t);
             LM<Real>::sc(t, s[j], c[j]);
             const Real kz = K.k * P4.z[j];
             ep[j] = LM<Real>::ex(kz);
@@ -494,7 +502,7 @@ __global__ void __launch_bounds__(LT) k_ladj_tot(int N, int P, int nch, const do
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
             double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
-            t -= rint(t);
+            t = frac_turns(t);
             double s, c;
             sincospi(2.0 * t, &s, &c);
             const double kz = K.k * P4.z[j], ep = exp(kz), em = exp(-kz), q = P4.q[j];
@@ -676,7 +684,7 @@ __global__ void __launch_bounds__(LT) k_ladj(int N, int P, int nch, int ks_n, co
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
             double t = fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]);
-            t -= rint(t);
+            t = frac_turns(t);
             sincospi(2.0 * t, &s[j], &c[j]);
             const double kz = K.k * P4.z[j], q = P4.q[j];
             ep[j] = exp(kz);

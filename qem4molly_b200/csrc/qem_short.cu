@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
                                                        const int *__restrict__ pos_of, const int64_t *__restrict__ poff,
                                                        const double4 *__restrict__ R, const double *__restrict__ Upair,
                                                        const int64_t *__restrict__ in_off,
-                                                       const int64_t *__restrict__ in_list, int64_t cap,
+                                                       const int *__restrict__ in_list, int64_t cap,
                                                        const ShortConsts c, double *__restrict__ F3,
                                                        double *__restrict__ Epart, unsigned *status, int do_short,
                                                        int do_lj)
@@ -412,7 +412,7 @@ cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np
 
 cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, bool do_lj, int N,
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
-                                    const double *Upair, const int64_t *in_off, const int64_t *in_list, int64_t cap,
+                                    const double *Upair, const int64_t *in_off, const int *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s)
 {
