@@ -398,6 +398,169 @@ __global__ void __launch_bounds__(LT, sizeof(Real) == 4 ? LF_MINB : 4) k_lforce(
     }
 }
 
+// FP32 force pass, same terms as k_lforce: the thread's four particles run as
+// two packed FP32x2 pairs (0, 1), (2, 3) through the per-particle algebra,
+// and the next k-vector's constants are fetched while the current one is
+// processed.
+template <bool ENERGY>
+__global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nch, int ks_n,
+                                                           const double *__restrict__ zx,
+                                                           const double *__restrict__ zy,
+                                                           const float *__restrict__ zh, const float *__restrict__ qv,
+                                                           const KConst *__restrict__ kc,
+                                                           const KForce<float> *__restrict__ kf,
+                                                           const float *__restrict__ off, double *__restrict__ Fpart,
+                                                           double *__restrict__ Epart)
+{
+    static_assert(PPT == 4, "two packed particle pairs per thread");
+    constexpr float LOG2E = 1.4426950408889634f;
+    __shared__ float wsh[2][4][NW];
+    __shared__ double ered[NW];
+    Quad4<float> P4;
+    const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
+    P4.load(N, m0, zx, zy, zh, qv);
+    const float2 z2[2] = {f2(P4.z[0], P4.z[1]), f2(P4.z[2], P4.z[3])};
+    const float2 q2[2] = {f2(P4.q[0], P4.q[1]), f2(P4.q[2], P4.q[3])};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ks = blockIdx.y;
+    const int ng = (P + LKB - 1) / LKB;
+    const int kb = LKB * (int)((int64_t)ng * ks / ks_n);
+    const int ke = min(P, LKB * (int)((int64_t)ng * (ks + 1) / ks_n));
+    double Fx[PPT], Fy[PPT], Fz[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) { Fx[j] = 0; Fy[j] = 0; Fz[j] = 0; }
+    float2 bx[2] = {f2s(0.f), f2s(0.f)}, by[2] = {f2s(0.f), f2s(0.f)}, bz[2] = {f2s(0.f), f2s(0.f)};
+    double E = 0;
+    // constants of k = kidx, fetched one iteration ahead
+    double kxn = 0, kyn = 0, ekn = 0;
+    float4 Kan = make_float4(0, 0, 0, 0), Kbn = Kan, On = Kan;
+    auto fetch = [&](int k) {
+        kxn = kc[k].kx_2pi;
+        kyn = kc[k].ky_2pi;
+        if (ENERGY) ekn = kc[k].ek;
+        const float4 *kk = reinterpret_cast<const float4 *>(kf + k);
+        Kan = kk[0];  // k, wfx, wfy, wk
+        Kbn = kk[1];  // s1r, s1i, s2r, s2i
+        On = *reinterpret_cast<const float4 *>(off + ((int64_t)k * nch + blockIdx.x) * 4);
+    };
+    if (kb < ke) fetch(kb);
+    for (int kidx = kb; kidx < ke; kidx++) {
+        const double kx2 = kxn, ky2 = kyn, ek = ekn;
+        const float4 Ka = Kan, Kb = Kbn, O = On;
+        if (kidx + 1 < ke) fetch(kidx + 1);
+        const int buf = (kidx - kb) & 1;
+        float2 c2[2], s2[2], ep2[2], em2[2], ur[2], ui[2], vr[2], vi[2];
+        const float2 kl = f2s(Ka.x * LOG2E);
+#pragma unroll
+        for (int pp = 0; pp < 2; pp++) {
+            float cc[2], ss[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int j = 2 * pp + h;
+                const double t = frac_turns(fma(kx2, P4.x[j], ky2 * P4.y[j]));
+                __sincosf((float)t * 6.28318530717958648f, &ss[h], &cc[h]);
+            }
+            c2[pp] = f2(cc[0], cc[1]);
+            s2[pp] = f2(ss[0], ss[1]);
+            const float2 e = mul2(kl, z2[pp]);
+            ep2[pp] = f2(ex2_approx(e.x), ex2_approx(e.y));
+            em2[pp] = f2(ex2_approx(-e.x), ex2_approx(-e.y));
+            const float2 qp = mul2(q2[pp], ep2[pp]), qm = mul2(q2[pp], em2[pp]);
+            ur[pp] = mul2(qp, c2[pp]);
+            ui[pp] = mul2(qp, s2[pp]);
+            vr[pp] = mul2(qm, c2[pp]);
+            vi[pp] = mul2(qm, s2[pp]);
+        }
+        // exclusive prefix of u over the particles 0..3 (from below) and
+        // exclusive suffix of v (from above), as packed pairs
+        const float s01r = ur[0].x + ur[0].y, s01i = ui[0].x + ui[0].y;
+        const float2 Arl[2] = {f2(0.f, ur[0].x), f2(s01r, s01r + ur[1].x)};
+        const float2 Ail[2] = {f2(0.f, ui[0].x), f2(s01i, s01i + ui[1].x)};
+        const float tr = Arl[1].y + ur[1].y, ti = Ail[1].y + ui[1].y;
+        const float s23r = vr[1].y + vr[1].x, s23i = vi[1].y + vi[1].x;
+        const float2 Crl[2] = {f2(s23r + vr[0].y, s23r), f2(vr[1].y, 0.f)};
+        const float2 Cil[2] = {f2(s23i + vi[0].y, s23i), f2(vi[1].y, 0.f)};
+        const float br = Crl[0].x + vr[0].x, bi = Cil[0].x + vi[0].x;
+        // warp inclusive scans of the thread totals: forward for u, backward for v
+        float fr = tr, fi = ti, gr = br, gi = bi;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const float a1 = __shfl_up_sync(0xffffffffu, fr, d), a2 = __shfl_up_sync(0xffffffffu, fi, d);
+            const float b1 = __shfl_down_sync(0xffffffffu, gr, d), b2 = __shfl_down_sync(0xffffffffu, gi, d);
+            if (lane >= d) { fr += a1; fi += a2; }
+            if (lane + d < 32) { gr += b1; gi += b2; }
+        }
+        if (lane == 31) { wsh[buf][0][w] = fr; wsh[buf][1][w] = fi; }
+        if (lane == 0) { wsh[buf][2][w] = gr; wsh[buf][3][w] = gi; }
+        float xr = __shfl_up_sync(0xffffffffu, fr, 1), xi = __shfl_up_sync(0xffffffffu, fi, 1);
+        float yr = __shfl_down_sync(0xffffffffu, gr, 1), yi = __shfl_down_sync(0xffffffffu, gi, 1);
+        if (lane == 0) { xr = 0; xi = 0; }
+        if (lane == 31) { yr = 0; yi = 0; }
+        __syncthreads();
+#pragma unroll
+        for (int ww = 0; ww < NW; ww++) {
+            if (ww < w) { xr += wsh[buf][0][ww]; xi += wsh[buf][1][ww]; }
+            if (ww > w) { yr += wsh[buf][2][ww]; yi += wsh[buf][3][ww]; }
+        }
+        const float2 bAr = f2s(O.x + xr), bAi = f2s(O.y + xi), bCr = f2s(O.z + yr), bCi = f2s(O.w + yi);
+        const float2 mh = f2s(-0.5f), m1 = f2s(-1.f);
+#pragma unroll
+        for (int pp = 0; pp < 2; pp++) {
+            const float2 Ar = add2(bAr, Arl[pp]), Ai = add2(bAi, Ail[pp]);
+            const float2 Cr = add2(bCr, Crl[pp]), Ci = add2(bCi, Cil[pp]);
+            const float2 ar = fma2(Cr, mh, f2s(Kb.x)), ai = fma2(Ci, mh, f2s(Kb.y));
+            const float2 br_ = fma2(Ar, mh, f2s(Kb.z)), bi_ = fma2(Ai, mh, f2s(Kb.w));
+            const float2 pr = mul2(ep2[pp], ar), pi = mul2(ep2[pp], ai);
+            const float2 mr = mul2(em2[pp], br_), mi = mul2(em2[pp], bi_);
+            const float2 x1r = add2(pr, mr), x1i = add2(pi, mi);
+            const float2 x2r = fma2(mr, m1, pr), x2i = fma2(mi, m1, pi);
+            const float2 im1 = fma2(mul2(s2[pp], m1), x1r, mul2(c2[pp], x1i));  // Im[e^{-i theta} X1]
+            const float2 re2 = fma2(s2[pp], x2i, mul2(c2[pp], x2r));           // Re[e^{-i theta} X2]
+            bx[pp] = fma2(f2s(Ka.y), im1, bx[pp]);
+            by[pp] = fma2(f2s(Ka.z), im1, by[pp]);
+            bz[pp] = fma2(f2s(Ka.w), re2, bz[pp]);
+            if (ENERGY) {
+                // Energy_long_range_njit.py:10-24 (sorted part), Re[e^{-i theta}(em A + ep C)]
+                const float2 zr = fma2(em2[pp], Ar, mul2(ep2[pp], Cr)), zi = fma2(em2[pp], Ai, mul2(ep2[pp], Ci));
+                const float2 pz = fma2(c2[pp], zr, mul2(s2[pp], zi));
+                const float2 q = q2[pp];
+                E += ek * 0.5 * ((double)(-q.x * q.x - q.x * pz.x) + (double)(-q.y * q.y - q.y * pz.y));
+            }
+        }
+        if ((kidx + 1) % LKB == 0) {
+#pragma unroll
+            for (int pp = 0; pp < 2; pp++) {
+                Fx[2 * pp] += (double)bx[pp].x; Fx[2 * pp + 1] += (double)bx[pp].y;
+                Fy[2 * pp] += (double)by[pp].x; Fy[2 * pp + 1] += (double)by[pp].y;
+                Fz[2 * pp] += (double)bz[pp].x; Fz[2 * pp + 1] += (double)bz[pp].y;
+                bx[pp] = f2s(0.f); by[pp] = f2s(0.f); bz[pp] = f2s(0.f);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int m = m0 + j;
+        const float2 bxv = bx[j >> 1], byv = by[j >> 1], bzv = bz[j >> 1];
+        if (m < N) {
+            const double q = (double)P4.q[j];
+            double *o = Fpart + ((int64_t)ks * N + m) * 3;
+            o[0] = q * (Fx[j] + (double)((j & 1) ? bxv.y : bxv.x));
+            o[1] = q * (Fy[j] + (double)((j & 1) ? byv.y : byv.x));
+            o[2] = q * (Fz[j] + (double)((j & 1) ? bzv.y : bzv.x));
+        }
+    }
+    if (ENERGY) {
+        for (int d = 16; d > 0; d >>= 1) E += __shfl_down_sync(0xffffffffu, E, d);
+        if (lane == 0) ered[w] = E;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0;
+            for (int ww = 0; ww < NW; ww++) sum += ered[ww];
+            Epart[(int64_t)ks * nch + blockIdx.x] = sum;
+        }
+    }
+}
+
 // F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term
 __global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, const double *__restrict__ k0,
                          const int *__restrict__ zperm, double *__restrict__ F3)
@@ -887,11 +1050,11 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const KForce<float> *kf = (const KForce<float> *)b.kf;
         const float *of = (const float *)b.off;
         if (energy)
-            k_lforce<float, true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of,
-                                                    b.Fpart, b.Epart);
+            k_lforce_f32<true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
+                                                 b.Epart);
         else
-            k_lforce<float, false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of,
-                                                     b.Fpart, b.Epart);
+            k_lforce_f32<false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
+                                                  b.Epart);
     }
     k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3);
     return cudaGetLastError();
