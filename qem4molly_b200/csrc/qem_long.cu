@@ -40,7 +40,7 @@ constexpr int NW = LT / 32;     // warps per block
 constexpr int KPB = 16;         // k-vectors per block in the totals pass
 constexpr int LKB = 8;          // k-vectors per FP32 accumulation batch of the force pass
 #ifndef QEM_LF_MINB
-#define QEM_LF_MINB 6
+#define QEM_LF_MINB 8
 #endif
 constexpr int LF_MINB = QEM_LF_MINB;  // resident FP32 force-pass blocks per SM (register budget)
 
@@ -416,6 +416,7 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     constexpr float LOG2E = 1.4426950408889634f;
     __shared__ float wsh[2][4][NW];
     __shared__ double ered[NW];
+    __shared__ double Facc[3 * PPT][LT];  // FP64 sums of the FP32 batches (registers stay free)
     Quad4<float> P4;
     const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
     P4.load(N, m0, zx, zy, zh, qv);
@@ -426,9 +427,8 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     const int ng = (P + LKB - 1) / LKB;
     const int kb = LKB * (int)((int64_t)ng * ks / ks_n);
     const int ke = min(P, LKB * (int)((int64_t)ng * (ks + 1) / ks_n));
-    double Fx[PPT], Fy[PPT], Fz[PPT];
 #pragma unroll
-    for (int j = 0; j < PPT; j++) { Fx[j] = 0; Fy[j] = 0; Fz[j] = 0; }
+    for (int r = 0; r < 3 * PPT; r++) Facc[r][threadIdx.x] = 0.0;
     float2 bx[2] = {f2s(0.f), f2s(0.f)}, by[2] = {f2s(0.f), f2s(0.f)}, bz[2] = {f2s(0.f), f2s(0.f)};
     double E = 0;
     // constants of k = kidx, fetched one iteration ahead
@@ -530,9 +530,12 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
         if ((kidx + 1) % LKB == 0) {
 #pragma unroll
             for (int pp = 0; pp < 2; pp++) {
-                Fx[2 * pp] += (double)bx[pp].x; Fx[2 * pp + 1] += (double)bx[pp].y;
-                Fy[2 * pp] += (double)by[pp].x; Fy[2 * pp + 1] += (double)by[pp].y;
-                Fz[2 * pp] += (double)bz[pp].x; Fz[2 * pp + 1] += (double)bz[pp].y;
+                Facc[6 * pp + 0][threadIdx.x] += (double)bx[pp].x;
+                Facc[6 * pp + 1][threadIdx.x] += (double)bx[pp].y;
+                Facc[6 * pp + 2][threadIdx.x] += (double)by[pp].x;
+                Facc[6 * pp + 3][threadIdx.x] += (double)by[pp].y;
+                Facc[6 * pp + 4][threadIdx.x] += (double)bz[pp].x;
+                Facc[6 * pp + 5][threadIdx.x] += (double)bz[pp].y;
                 bx[pp] = f2s(0.f); by[pp] = f2s(0.f); bz[pp] = f2s(0.f);
             }
         }
@@ -540,13 +543,14 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int m = m0 + j;
-        const float2 bxv = bx[j >> 1], byv = by[j >> 1], bzv = bz[j >> 1];
+        const int pp = j >> 1, h = j & 1;
+        const float2 bxv = bx[pp], byv = by[pp], bzv = bz[pp];
         if (m < N) {
             const double q = (double)P4.q[j];
             double *o = Fpart + ((int64_t)ks * N + m) * 3;
-            o[0] = q * (Fx[j] + (double)((j & 1) ? bxv.y : bxv.x));
-            o[1] = q * (Fy[j] + (double)((j & 1) ? byv.y : byv.x));
-            o[2] = q * (Fz[j] + (double)((j & 1) ? bzv.y : bzv.x));
+            o[0] = q * (Facc[6 * pp + 0 + h][threadIdx.x] + (double)(h ? bxv.y : bxv.x));
+            o[1] = q * (Facc[6 * pp + 2 + h][threadIdx.x] + (double)(h ? byv.y : byv.x));
+            o[2] = q * (Facc[6 * pp + 4 + h][threadIdx.x] + (double)(h ? bzv.y : bzv.x));
         }
     }
     if (ENERGY) {
@@ -994,9 +998,25 @@ __global__ void k_ladj_final(int N, int ks_n, const double *__restrict__ Gpart, 
 
 int qem_long_chunk(void) { return LCH; }
 
+// streaming multiprocessors of the current device (cached per device)
+static int sm_count()
+{
+    static int cached[64] = {0};
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return 148;
+    if (cached[d] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess || n <= 0) n = 148;
+        cached[d] = n;
+    }
+    return cached[d];
+}
+
 int qem_long_ksplit(int nch, int P, int max_ks)
 {
-    int ks = (4 * 148 + nch - 1) / nch;  // enough blocks for every SM
+    // as many whole k-slices of the nch chunks as fit in one wave of resident
+    // force-pass blocks
+    int ks = sm_count() * LF_MINB / (nch > 0 ? nch : 1);
     ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
     const int pm = P > LKB ? (P + LKB - 1) / LKB : 1;  // at most one slice per k group
     return ks < pm ? ks : pm;
