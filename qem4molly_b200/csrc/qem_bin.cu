@@ -329,13 +329,69 @@ __global__ void k_in_fill(const int64_t *__restrict__ np, int64_t cap, const int
     list[off[j] + atomicAdd(&fill[j], 1)] = (int)p;
 }
 
-// incoming lists in ascending pair order; one warp per particle
+// ascending order of M register values (bitonic network; every index is a
+// compile-time constant after unrolling, so the array stays in registers)
+template <int M>
+__device__ __forceinline__ void reg_sort(int (&v)[M])
+{
+#pragma unroll
+    for (int size = 2; size <= M; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+            for (int a = 0; a < M; a++) {
+                const int b = a ^ stride;
+                if (b > a) {
+                    const bool up = (a & size) == 0;
+                    const int x = v[a], y = v[b];
+                    v[a] = up ? min(x, y) : max(x, y);
+                    v[b] = up ? max(x, y) : min(x, y);
+                }
+            }
+        }
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void sort_small_segment(int *list, int64_t b, int n)
+{
+    int v[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) v[k] = k < n ? list[b + k] : 0x7fffffff;
+    reg_sort<M>(v);
+#pragma unroll
+    for (int k = 0; k < M; k++)
+        if (k < n) list[b + k] = v[k];
+}
+
+// incoming lists in ascending pair order; one thread per particle, the
+// segment sorted in registers (segments of more than 64 entries, which a
+// cutoff disc at these densities practically never holds, by insertion in
+// place)
 __global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restrict__ list)
 {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    warp_sort_segment<int>(list, off[i], off[i + 1], lane, 0x7fffffff);
+    const int64_t b = off[i], e = off[i + 1];
+    const int64_t n = e - b;
+    if (n <= 1) return;
+    if (n <= 16) {
+        sort_small_segment<16>(list, b, (int)n);
+    } else if (n <= 32) {
+        sort_small_segment<32>(list, b, (int)n);
+    } else if (n <= 64) {
+        sort_small_segment<64>(list, b, (int)n);
+    } else {
+        for (int64_t s = b + 1; s < e; s++) {
+            const int v = list[s];
+            int64_t t = s - 1;
+            while (t >= b && list[t] > v) {
+                list[t + 1] = list[t];
+                t--;
+            }
+            list[t + 1] = v;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -512,7 +568,7 @@ cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int
     e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s);
     if (e != cudaSuccess) return e;
     if (cap > 0) k_in_fill<<<nblk(cap, 256), 256, 0, s>>>(np, cap, pairs, in_off, in_fill, in_list);
-    k_in_sort<<<nblk((int64_t)N * 32, 256), 256, 0, s>>>(N, in_off, in_list);
+    k_in_sort<<<nblk(N, 128), 128, 0, s>>>(N, in_off, in_list);
     return cudaGetLastError();
 }
 

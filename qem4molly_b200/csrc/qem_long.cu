@@ -55,14 +55,6 @@ __device__ __forceinline__ double frac_turns(double t)
 template <typename Real>
 struct LM;
 template <>
-struct LM<float> {
-    static __device__ __forceinline__ float ex(float x) { return __expf(x); }
-    static __device__ __forceinline__ void sc(double turns, float &s, float &c)
-    {
-        __sincosf((float)turns * 6.28318530717958648f, &s, &c);
-    }
-};
-template <>
 struct LM<double> {
     static __device__ __forceinline__ double ex(double x) { return exp(x); }
     static __device__ __forceinline__ void sc(double turns, double &s, double &c) { sincospi(2.0 * turns, &s, &c); }
@@ -192,6 +184,55 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
             tot[((int64_t)kidx * nch + blockIdx.x) * 4 + threadIdx.x] = sum;
         }
         __syncthreads();
+    }
+}
+
+// FP32 chunk totals, same sums as k_ltot<float>: each thread keeps its four
+// particles' sums for the block's KPB k-vectors in shared memory, and one
+// tree reduction over the block's threads finishes all KPB x 4 totals (one
+// barrier per tree level instead of two barriers and a warp reduction per k).
+__global__ void __launch_bounds__(LT) k_ltot_f32(int N, int P, int nch, const double *__restrict__ zx,
+                                                 const double *__restrict__ zy, const float *__restrict__ zh,
+                                                 const float *__restrict__ qv, const KConst *__restrict__ kc,
+                                                 double *__restrict__ tot)
+{
+    constexpr float LOG2E = 1.4426950408889634f;
+    __shared__ float part[KPB * 4][LT + 1];  // +1: rows on different banks
+    Quad4<float> P4;
+    P4.load(N, blockIdx.x * LCH + threadIdx.x * PPT, zx, zy, zh, qv);
+    const int k0 = blockIdx.y * KPB;
+    const int nk = min(KPB, P - k0);
+    for (int kk = 0; kk < nk; kk++) {
+        const KConst K = kc[k0 + kk];
+        const float kl = (float)K.k * LOG2E;
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const double t = frac_turns(fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]));
+            float s, c;
+            __sincosf((float)t * 6.28318530717958648f, &s, &c);
+            const float e = kl * P4.z[j];
+            const float ep = P4.q[j] * ex2_approx(e), em = P4.q[j] * ex2_approx(-e);
+            v[0] = fmaf(ep, c, v[0]);
+            v[1] = fmaf(ep, s, v[1]);
+            v[2] = fmaf(em, c, v[2]);
+            v[3] = fmaf(em, s, v[3]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) part[4 * kk + r][threadIdx.x] = v[r];
+    }
+    __syncthreads();
+    const int rows = 4 * nk;
+    for (int stride = LT / 2; stride > 0; stride >>= 1) {
+        for (int idx = threadIdx.x; idx < rows * stride; idx += LT) {
+            const int row = idx / stride, col = idx - row * stride;
+            part[row][col] += part[row][col + stride];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < rows) {
+        const int kk = threadIdx.x >> 2, r = threadIdx.x & 3;
+        tot[((int64_t)(k0 + kk) * nch + blockIdx.x) * 4 + r] = (double)part[threadIdx.x][0];
     }
 }
 
@@ -1047,7 +1088,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
-                k_ltot<float><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
+                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
