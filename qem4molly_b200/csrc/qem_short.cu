@@ -40,7 +40,10 @@
 
 namespace {
 
-constexpr int PAIR_BLOCK = 256;
+#ifndef QEM_PAIR_BLOCK
+#define QEM_PAIR_BLOCK 256
+#endif
+constexpr int PAIR_BLOCK = QEM_PAIR_BLOCK;  // pairs per block, ordered by rho in shared memory
 // resident pair blocks per SM requested from the register allocator, and the
 // unroll factor of the FP32 node loop (tuning knobs; measured defaults)
 #ifndef QEM_PAIR_MINB

@@ -310,3 +310,19 @@ def test_config2_full_size_properties():
     sh[:, 1] = (sh[:, 1] + 654.321) % cfg["L"][1]
     Fb = em.forces(sh, cfg["q"], terms=L.QEM_TERM_SHORT)
     assert W.rel_err(Fb, Fa)[0] <= 1e-10
+
+
+def test_pair_list_overflow_retry_matches_oracle():
+    """Particles packed into a 20 x 20 patch of a 200 x 200 box: the first
+    pair-capacity estimate (from the mean density) is ~20 times too small, the
+    call overflows, grows the capacity and evaluates again; the forces equal
+    the oracle's and a second call repeats them bit for bit."""
+    rng = np.random.default_rng(77)
+    N, Lb = 1500, (200.0, 200.0, 10.0)
+    xyz = np.stack([50 + 20 * rng.random(N), 80 + 20 * rng.random(N), 0.5 + 9 * rng.random(N)], 1)
+    q = np.where(np.arange(N) < N // 2, 1.0, -1.0)
+    e = Engine(L_box=Lb, alpha=0.1, r_cutoff=10.0, gamma_1=0.5, gamma_2=-0.4, rbe_p=0)
+    F = e.forces(xyz, q, terms=L.QEM_TERM_SHORT)
+    Fref = O.short_forces(oparams(Lb, 0.1, 10.0, 0.5, -0.4), xyz, q)
+    assert W.rel_err(F, Fref)[0] <= 1e-11
+    assert np.array_equal(e.forces(xyz, q, terms=L.QEM_TERM_SHORT), F)
