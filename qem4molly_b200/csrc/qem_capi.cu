@@ -2,6 +2,7 @@
 // validation, device scratch, k-set sampling and the per-call orchestration of
 // the binning, short-range and long-range kernels.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,11 +21,15 @@ struct DevBuf {
 // set while enqueuing asynchronous (capturable) work: a buffer that would
 // have to grow is an error there, as cudaMalloc / cudaFree cannot be captured
 thread_local bool g_no_alloc = false;
+// counts device (re)allocations of handle buffers: a recorded evaluation graph
+// holds buffer addresses and is replayed only while this is unchanged
+std::atomic<uint64_t> g_alloc_epoch{0};
 
 cudaError_t grow(DevBuf &b, size_t bytes)
 {
     if (bytes <= b.cap && b.p) return cudaSuccess;
     if (g_no_alloc) return cudaErrorMemoryAllocation;
+    g_alloc_epoch++;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
@@ -131,6 +136,7 @@ struct qem_handle {
     int kin_lo = 0, kin_hi = -1;  // rows of the k-set currently in the device copy
     // sharding of one system over ranks (qem_set_shard)
     int shard_rank = 0, shard_world = 1;
+    uint64_t cfg_version = 0;  // bumped by k-set and shard changes
     uint64_t rng = 0x51ed5eedULL;
     std::vector<double> cdfx, cdfy;
     long mxmax = 0, mymax = 0;
@@ -161,6 +167,24 @@ struct qem_handle {
     int64_t short_calls = 0;
     Prof prof;
     int64_t counts[4] = {0, 0, 0, 0};
+    // replay of a recorded device-memory evaluation (run())
+    struct GraphKey {
+        int N = -1;
+        const void *xyz = nullptr, *q = nullptr, *F = nullptr;
+        uint32_t terms = 0;
+        int64_t cap = 0;
+        int P = 0;
+        uint64_t cfg = 0, epoch = 0;
+        bool operator==(const GraphKey &o) const
+        {
+            return N == o.N && xyz == o.xyz && q == o.q && F == o.F && terms == o.terms && cap == o.cap && P == o.P &&
+                   cfg == o.cfg && epoch == o.epoch;
+        }
+    };
+    GraphKey gkey, gwarm;
+    bool gwarm_valid = false;
+    cudaStream_t gcap = nullptr;
+    cudaGraphExec_t gexec = nullptr;
 };
 
 static const char *status_str(qem_status s)
@@ -321,6 +345,7 @@ static void sample_kset(qem_handle *h, int P)
     h->kmax = kmax;
     h->has_kset = true;
     h->kset_dirty = true;
+    h->cfg_version++;
 }
 
 // device buffers of the long range for N particles, Pk k-vectors, nch chunks
@@ -626,13 +651,124 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     return QEM_OK;
 }
 
+// Device-memory force calls (no energy, no profiling, neighbour list rebuilt
+// and k-set kept every call) repeat the same launches on the same buffers, so
+// after one ordinary call of a configuration the evaluation is recorded once
+// as a CUDA graph on the handle's private stream and then replayed on the
+// caller's stream: the host issues one launch instead of some forty.  The key
+// covers everything the recorded launches depend on (sizes, pointers, terms,
+// pair capacity, k-set and shard, and every buffer address through the
+// allocation count); the status word and the pair count are read back after
+// each replay as in an ordinary call, and a pair-list overflow drops the
+// graph and re-runs the call the ordinary way.
+static void drop_graph(qem_handle *h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+}
+
+static bool graph_eligible(const qem_handle *h, int N, const double *xyz, const double *q, const double *F,
+                           const double *energy, uint32_t terms, int mem)
+{
+    return mem == QEM_MEM_DEVICE && !energy && !h->prof.on && N > 0 && xyz && q && F && !(terms & ~QEM_TERM_ALL) &&
+           !(h->p.mode_flags & (QEM_STALE_NEIGHBORS | QEM_RESAMPLE_KSET));
+}
+
+static qem_handle::GraphKey graph_key(const qem_handle *h, int N, const double *xyz, const double *q,
+                                      const double *F, uint32_t terms)
+{
+    qem_handle::GraphKey k;
+    k.N = N; k.xyz = xyz; k.q = q; k.F = F; k.terms = terms;
+    k.cap = h->pair_cap;
+    k.P = h->has_kset ? h->P : 0;
+    k.cfg = h->cfg_version;
+    k.epoch = g_alloc_epoch.load();
+    return k;
+}
+
+// replays (recording first if needed); fallback = true asks for an ordinary call
+static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const double *xyz, const double *q,
+                            double *F, uint32_t terms, cudaStream_t s, bool &fallback)
+{
+    fallback = false;
+    const int N = k.N;
+    CU(cudaSetDevice(h->p.device));
+    if (!h->gexec || !(h->gkey == k)) {
+        drop_graph(h);
+        if (!h->gcap) CU(cudaStreamCreateWithFlags(&h->gcap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(h->gcap, cudaStreamCaptureModeThreadLocal));
+        bool retry = false;
+        const qem_status st = run_once(h, N, xyz, q, F, nullptr, terms, QEM_MEM_DEVICE, h->gcap, retry, true);
+        const cudaError_t ec = cudaStreamEndCapture(h->gcap, &g);
+        cudaGraphExec_t ex = nullptr;
+        const bool ok = st == QEM_OK && ec == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (!ok || !(graph_key(h, N, xyz, q, F, terms) == k)) {
+            if (ex) cudaGraphExecDestroy(ex);
+            h->gwarm_valid = false;
+            fallback = true;
+            return QEM_OK;
+        }
+        h->gexec = ex;
+        h->gkey = k;
+    }
+    const bool do_short = terms & QEM_TERM_SHORT;
+    unsigned *st = ptr<unsigned>(h->status);
+    CU(cudaMemsetAsync(st, 0, sizeof(unsigned), s));
+    CU(cudaGraphLaunch(h->gexec, s));
+    CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (do_short)
+        CU(cudaMemcpyAsync(h->h_np, ptr<int64_t>(h->poff) + N, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const unsigned stv = *h->h_status;
+    if (do_short) {
+        h->Np = *h->h_np;
+        if (stv & QEM_ST_OVERFLOW) {  // grow and evaluate the ordinary way
+            h->pair_cap = h->Np + h->Np / 4 + 4096;
+            h->pairs_valid = false;
+            drop_graph(h);
+            h->gwarm_valid = false;
+            fallback = true;
+            return QEM_OK;
+        }
+        if (h->Np > h->pair_cap - h->pair_cap / 8) {  // grow at the next (ordinary) build
+            h->pair_cap = h->Np + h->Np / 4 + 4096;
+            h->gwarm_valid = false;
+        }
+    }
+    h->counts[0] = do_short ? h->Np : 0;
+    h->counts[1] = N;
+    h->counts[3] = 1;
+    if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
+    if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    h->err.clear();
+    return QEM_OK;
+}
+
 static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, double *F, double *energy,
                       uint32_t terms, int mem, cudaStream_t s)
 {
+    if (!h) return QEM_ERR_ARG;
+    const bool eligible = graph_eligible(h, N, xyz, q, F, energy, terms, mem);
+    if (eligible && h->gwarm_valid && !h->kset_dirty) {
+        const qem_handle::GraphKey k = graph_key(h, N, xyz, q, F, terms);
+        if (k == h->gwarm) {
+            bool fallback = false;
+            const qem_status st = run_graph(h, k, xyz, q, F, terms, s, fallback);
+            if (!fallback) return st;
+        }
+    }
+    const int64_t cap0 = h->pair_cap;
     bool retry = false;
     qem_status st = run_once(h, N, xyz, q, F, energy, terms, mem, s, retry);
     if (st == QEM_OK && retry) st = run_once(h, N, xyz, q, F, energy, terms, mem, s, retry);
     if (st == QEM_OK && retry) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list grew past its capacity twice");
+    // a configuration is recorded once an ordinary call ran it with buffers
+    // that are already large enough for the next call
+    h->gwarm_valid = st == QEM_OK && eligible && h->pair_cap == cap0;
+    if (h->gwarm_valid) h->gwarm = graph_key(h, N, xyz, q, F, terms);
     return st;
 }
 
@@ -710,6 +846,8 @@ void qem_destroy(qem_handle *h)
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->gcap) cudaStreamDestroy(h->gcap);
     if (h->s2) {
         cudaStreamSynchronize(h->s2);
         cudaStreamDestroy(h->s2);
@@ -742,6 +880,7 @@ qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K
     h->kmax = kmax;
     h->has_kset = true;
     h->kset_dirty = true;
+    h->cfg_version++;
     return QEM_OK;
 }
 
@@ -1119,6 +1258,7 @@ extern "C" qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world)
         return fail(h, QEM_ERR_ARG, "shard rank must be in 0 .. world - 1, world in 1 .. 4096");
     h->shard_rank = rank;
     h->shard_world = world;
+    h->cfg_version++;
     h->sc.shard_rank = rank;
     h->sc.shard_world = world;
     h->err.clear();
