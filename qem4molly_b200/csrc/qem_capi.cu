@@ -169,7 +169,7 @@ struct qem_handle {
     int64_t counts[4] = {0, 0, 0, 0};
     // replay of a recorded device-memory evaluation (run())
     struct GraphKey {
-        int N = -1;
+        int N = -1, mem = -1;
         const void *xyz = nullptr, *q = nullptr, *F = nullptr;
         uint32_t terms = 0;
         int64_t cap = 0;
@@ -177,8 +177,8 @@ struct qem_handle {
         uint64_t cfg = 0, epoch = 0;
         bool operator==(const GraphKey &o) const
         {
-            return N == o.N && xyz == o.xyz && q == o.q && F == o.F && terms == o.terms && cap == o.cap && P == o.P &&
-                   cfg == o.cfg && epoch == o.epoch;
+            return N == o.N && mem == o.mem && xyz == o.xyz && q == o.q && F == o.F && terms == o.terms &&
+                   cap == o.cap && P == o.P && cfg == o.cfg && epoch == o.epoch;
         }
     };
     GraphKey gkey, gwarm;
@@ -651,13 +651,16 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     return QEM_OK;
 }
 
-// Device-memory force calls (no energy, no profiling, neighbour list rebuilt
-// and k-set kept every call) repeat the same launches on the same buffers, so
-// after one ordinary call of a configuration the evaluation is recorded once
-// as a CUDA graph on the handle's private stream and then replayed on the
-// caller's stream: the host issues one launch instead of some forty.  The key
-// covers everything the recorded launches depend on (sizes, pointers, terms,
-// pair capacity, k-set and shard, and every buffer address through the
+// Force calls without energy or profiling whose neighbour list is rebuilt and
+// whose k-set is kept every call repeat the same launches on the same
+// buffers, so after one ordinary call of a configuration the evaluation is
+// recorded once as a CUDA graph on the handle's private stream and then
+// replayed on the caller's stream: the host issues one launch instead of some
+// forty.  Device buffers qualify, and so do page-locked host buffers, whose
+// host-to-device and device-to-host copies are then part of the graph
+// (pageable host memory cannot be copied inside a graph).  The key covers
+// everything the recorded launches depend on (sizes, pointers, memory kind,
+// terms, pair capacity, k-set and shard, and every buffer address through the
 // allocation count); the status word and the pair count are read back after
 // each replay as in an ordinary call, and a pair-list overflow drops the
 // graph and re-runs the call the ordinary way.
@@ -667,18 +670,37 @@ static void drop_graph(qem_handle *h)
     h->gexec = nullptr;
 }
 
+// first and last byte of [p, p + bytes) in page-locked host memory
+static bool host_locked(const void *p, size_t bytes)
+{
+    const char *c = static_cast<const char *>(p);
+    for (const char *a : {c, c + bytes - 1}) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, a) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (at.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
+
 static bool graph_eligible(const qem_handle *h, int N, const double *xyz, const double *q, const double *F,
                            const double *energy, uint32_t terms, int mem)
 {
-    return mem == QEM_MEM_DEVICE && !energy && !h->prof.on && N > 0 && xyz && q && F && !(terms & ~QEM_TERM_ALL) &&
-           !(h->p.mode_flags & (QEM_STALE_NEIGHBORS | QEM_RESAMPLE_KSET));
+    if (energy || h->prof.on || N <= 0 || !xyz || !q || !F || (terms & ~QEM_TERM_ALL) ||
+        (h->p.mode_flags & (QEM_STALE_NEIGHBORS | QEM_RESAMPLE_KSET)))
+        return false;
+    if (mem == QEM_MEM_DEVICE) return true;
+    const size_t n3 = sizeof(double) * 3 * (size_t)N;
+    return mem == QEM_MEM_HOST && host_locked(xyz, n3) && host_locked(q, sizeof(double) * N) && host_locked(F, n3);
 }
 
 static qem_handle::GraphKey graph_key(const qem_handle *h, int N, const double *xyz, const double *q,
-                                      const double *F, uint32_t terms)
+                                      const double *F, uint32_t terms, int mem)
 {
     qem_handle::GraphKey k;
-    k.N = N; k.xyz = xyz; k.q = q; k.F = F; k.terms = terms;
+    k.N = N; k.mem = mem; k.xyz = xyz; k.q = q; k.F = F; k.terms = terms;
     k.cap = h->pair_cap;
     k.P = h->has_kset ? h->P : 0;
     k.cfg = h->cfg_version;
@@ -696,16 +718,35 @@ static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const 
     if (!h->gexec || !(h->gkey == k)) {
         drop_graph(h);
         if (!h->gcap) CU(cudaStreamCreateWithFlags(&h->gcap, cudaStreamNonBlocking));
+        // host buffers: staged through the handle's device copies, which the
+        // ordinary call of this configuration has already sized
+        const bool host = k.mem == QEM_MEM_HOST;
+        const size_t n3 = sizeof(double) * 3 * (size_t)N;
+        if (host && (h->xyz.cap < n3 || h->q.cap < sizeof(double) * N || h->F.cap < n3)) {
+            h->gwarm_valid = false;
+            fallback = true;
+            return QEM_OK;
+        }
+        const double *xd = host ? ptr<double>(h->xyz) : xyz, *qd = host ? ptr<double>(h->q) : q;
+        double *Fd = host ? ptr<double>(h->F) : F;
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(h->gcap, cudaStreamCaptureModeThreadLocal));
+        cudaError_t ce = cudaSuccess;
+        if (host) {
+            ce = cudaMemcpyAsync(h->xyz.p, xyz, n3, cudaMemcpyHostToDevice, h->gcap);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(h->q.p, q, sizeof(double) * N, cudaMemcpyHostToDevice, h->gcap);
+        }
         bool retry = false;
-        const qem_status st = run_once(h, N, xyz, q, F, nullptr, terms, QEM_MEM_DEVICE, h->gcap, retry, true);
+        qem_status st = QEM_ERR_CUDA;
+        if (ce == cudaSuccess) st = run_once(h, N, xd, qd, Fd, nullptr, terms, QEM_MEM_DEVICE, h->gcap, retry, true);
+        if (st == QEM_OK && host) ce = cudaMemcpyAsync(F, Fd, n3, cudaMemcpyDeviceToHost, h->gcap);
         const cudaError_t ec = cudaStreamEndCapture(h->gcap, &g);
         cudaGraphExec_t ex = nullptr;
-        const bool ok = st == QEM_OK && ec == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+        const bool ok = st == QEM_OK && ce == cudaSuccess && ec == cudaSuccess && g &&
+                        cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
-        if (!ok || !(graph_key(h, N, xyz, q, F, terms) == k)) {
+        if (!ok || !(graph_key(h, N, xyz, q, F, terms, k.mem) == k)) {
             if (ex) cudaGraphExecDestroy(ex);
             h->gwarm_valid = false;
             fallback = true;
@@ -753,7 +794,7 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
     if (!h) return QEM_ERR_ARG;
     const bool eligible = graph_eligible(h, N, xyz, q, F, energy, terms, mem);
     if (eligible && h->gwarm_valid && !h->kset_dirty) {
-        const qem_handle::GraphKey k = graph_key(h, N, xyz, q, F, terms);
+        const qem_handle::GraphKey k = graph_key(h, N, xyz, q, F, terms, mem);
         if (k == h->gwarm) {
             bool fallback = false;
             const qem_status st = run_graph(h, k, xyz, q, F, terms, s, fallback);
@@ -768,7 +809,7 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
     // a configuration is recorded once an ordinary call ran it with buffers
     // that are already large enough for the next call
     h->gwarm_valid = st == QEM_OK && eligible && h->pair_cap == cap0;
-    if (h->gwarm_valid) h->gwarm = graph_key(h, N, xyz, q, F, terms);
+    if (h->gwarm_valid) h->gwarm = graph_key(h, N, xyz, q, F, terms, mem);
     return st;
 }
 

@@ -1,8 +1,9 @@
-"""Device-memory force calls are recorded once as a CUDA graph and replayed
-(qem_forces, QEM_MEM_DEVICE, no energy): replays must give the ordinary
-call's result bit for bit and follow every change the recorded launches do
-not capture -- coordinates in the same buffer, a new k-set, another output
-buffer, a pair list that outgrows its capacity, a non-finite input."""
+"""Force calls on device buffers or page-locked host buffers are recorded once
+as a CUDA graph and replayed (qem_forces without energy): replays must give
+the ordinary call's result bit for bit and follow every change the recorded
+launches do not capture -- coordinates in the same buffer, a new k-set,
+another output buffer, a pair list that outgrows its capacity, a non-finite
+input."""
 import numpy as np
 import pytest
 
@@ -22,7 +23,7 @@ def _dev(a):
 def test_replays_equal_the_ordinary_call(prec):
     cfg = W.config3(N=4000)
     e = W.engine_for(cfg, prec)
-    ref = e.forces(cfg["xyz"], cfg["q"])           # host memory: never replayed
+    ref = e.forces(cfg["xyz"], cfg["q"])           # pageable host memory: never replayed
     x, q = _dev(cfg["xyz"]), _dev(cfg["q"])
     F = _dev(np.zeros_like(cfg["xyz"]))
     for _ in range(4):                              # ordinary, record + replay, replay, replay
@@ -89,3 +90,32 @@ def test_replay_overflow_and_status():
     x.copy_(_dev(packed))
     e.forces_device(x, q, F)
     assert np.array_equal(F.cpu().numpy(), fresh.forces(packed, qh))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_pinned_host_buffers_replay(prec):
+    import torch
+
+    cfg = W.config3(N=4000)
+    e = W.engine_for(cfg, prec)
+    ref = e.forces(cfg["xyz"], cfg["q"])
+    xh = torch.tensor(cfg["xyz"], dtype=torch.float64).pin_memory()
+    qh = torch.tensor(cfg["q"], dtype=torch.float64).pin_memory()
+    Fh = torch.empty_like(xh).pin_memory()
+    for _ in range(4):                              # ordinary, record + replay, replay, replay
+        Fh.fill_(float("nan"))
+        e.forces(xh.numpy(), qh.numpy(), out=Fh.numpy())
+        assert np.array_equal(Fh.numpy(), ref)
+    rng = np.random.default_rng(9)
+    xyz2 = cfg["xyz"] + rng.normal(scale=0.05, size=cfg["xyz"].shape)
+    xyz2[:, 2] = np.clip(xyz2[:, 2], 0.6, 9.4)
+    xh.copy_(torch.tensor(xyz2))                    # new coordinates in the same page-locked buffer
+    e.forces(xh.numpy(), qh.numpy(), out=Fh.numpy())
+    got = Fh.numpy().copy()
+    assert np.array_equal(got, e.forces(xyz2, cfg["q"]))
+    # the device-memory graph of the same handle and the host one agree
+    x, q = _dev(xyz2), _dev(cfg["q"])
+    F = torch.empty_like(x)
+    for _ in range(3):
+        e.forces_device(x, q, F)
+    assert np.array_equal(F.cpu().numpy(), got)
