@@ -316,6 +316,163 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__r
 }
 
 // ---------------------------------------------------------------------------
+// pair list, at least 3 cells along x and y: one warp per owner cell
+// ---------------------------------------------------------------------------
+// The five cells of the half stencil in visiting order: own cell, then
+// (0,+1), (+1,-1), (+1,0), (+1,+1) -- the order of k_pairs.
+__device__ __forceinline__ void half_offset(int d, int &ox, int &oy)
+{
+    ox = d >= 2 ? 1 : 0;
+    oy = d == 0 ? 0 : (d == 1 ? 1 : d - 3);
+}
+
+__device__ __forceinline__ int wrap_cell(int n, int m) { return n < 0 ? n + m : (n >= m ? n - m : n); }
+
+// The lanes hold 32 consecutive candidates of the concatenated stencil cells
+// and the warp walks the cell's owners in order: a ballot per owner gives
+// each hit its pair index (the owner's next index plus the hits of lower
+// lanes), which reproduces k_pairs' order exactly, and each lane counts the
+// hits on its candidate, i.e. the candidate's incoming entries from this
+// owner cell in owner order.  The count pass stores, per owner, its number
+// of pairs and, per (candidate, stencil direction), its number of incoming
+// pairs from that owner cell (`in_slot`, indexed by cell-order position).
+// k_in_base turns those into slot bases; the fill pass then writes every
+// incoming entry straight to its final slot, so the incoming lists come out
+// in ascending pair order without atomics or a sort.  A (candidate,
+// direction) entry belongs to exactly one owner cell, hence to one warp, and
+// owner blocks of more than 32 owners carry it over in place.
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__restrict__ pos_c,
+                                                    const int *__restrict__ cstart, const int *__restrict__ clist,
+                                                    CellGeom g, double rc2, int *__restrict__ pcount,
+                                                    const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
+                                                    int64_t cap, int *__restrict__ in_slot,
+                                                    const int64_t *__restrict__ in_off, int *__restrict__ in_list,
+                                                    unsigned *status)
+{
+    const int c = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (c >= ncell) return;  // c is the same for the whole warp
+    const int cx = c / g.ncy, cy = c - cx * g.ncy;
+    int sb[5], sl[5], tot = 0;
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+        int ox, oy;
+        half_offset(d, ox, oy);
+        const int cc = wrap_cell(cx + ox, g.ncx) * g.ncy + wrap_cell(cy + oy, g.ncy);
+        sb[d] = cstart[cc];
+        sl[d] = cstart[cc + 1] - sb[d];
+        tot += sl[d];
+    }
+    const int ob = sb[0], nown = sl[0];
+    const unsigned below = (1u << lane) - 1u;
+    // the count pass also visits an empty cell once, to zero its candidates' entries
+    const int nblkown = nown > 0 ? (nown + 31) >> 5 : (FILL ? 0 : 1);
+    for (int blk = 0; blk < nblkown; blk++) {
+        const int o0 = ob + 32 * blk;
+        const int no = max(0, min(32, ob + nown - o0));
+        int my_i = 0, my_cnt = 0;
+        int64_t my_next = 0;  // fill: pair index of this lane's owner's next pair
+        if (lane < no) {
+            my_i = clist[o0 + lane];
+            if (FILL) my_next = poff[o0 + lane];
+        }
+        for (int v0 = 0; v0 < tot; v0 += 32) {
+            const int v = v0 + lane;
+            int d = -1, s = 0;
+            {
+                int acc = 0;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    if (d < 0 && v < acc + sl[k]) {
+                        d = k;
+                        s = sb[k] + (v - acc);
+                    }
+                    acc += sl[k];
+                }
+            }
+            const bool valid = d >= 0;
+            double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
+            int j = 0;
+            int64_t slot = 0;
+            if (valid) {
+                pj = pos_c[s];
+                j = clist[s];
+                if (FILL) slot = in_off[j] + in_slot[(size_t)5 * s + d];
+            }
+            int r = 0;
+            for (int k = 0; k < no; k++) {
+                const int t = o0 + k;
+                const bool hit = valid && (d != 0 || s > t) && rho2_exact(pos_c[t], pj, g) <= rc2;
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (FILL) {
+                    const int64_t base = __shfl_sync(0xffffffffu, my_next, k);
+                    const int io = __shfl_sync(0xffffffffu, my_i, k);
+                    if (hit) {
+                        const int64_t p = base + __popc(m & below);
+                        if (p < cap) {
+                            pairs[p] = make_int2(io, j);
+                            if (slot + r < cap) in_list[slot + r] = (int)p;
+                        } else {
+                            atomicOr(status, QEM_ST_OVERFLOW);
+                        }
+                    }
+                    if (lane == k) my_next += __popc(m);
+                } else if (lane == k) {
+                    my_cnt += __popc(m);
+                }
+                r += hit;
+            }
+            if (valid) {
+                int &w = in_slot[(size_t)5 * s + d];
+                w = (FILL || blk > 0) ? w + r : r;
+            }
+        }
+        if (!FILL && lane < no) pcount[o0 + lane] = my_cnt;
+    }
+}
+
+// Per cell-order position s of particle j: the owner cells of j's incoming
+// pairs are the five cells j - offset(d); pair indices ascend with the owner's
+// cell index, so ordering the five cells by index turns the per-direction
+// counts into slot bases.  Also j's number of incoming pairs -- zero for
+// every particle when the pairs do not fit the capacity (the evaluation is
+// then repeated with a larger list), so that in_off[N] <= cap and every
+// entry of in_list below in_off[N] names a stored pair.
+__global__ void k_in_base(int N, const int *__restrict__ clist, const int *__restrict__ cell, CellGeom g,
+                          const int64_t *__restrict__ np, int64_t cap, int *__restrict__ in_slot,
+                          int *__restrict__ in_cnt, unsigned *status)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const int j = clist[s];
+    if (*np > cap) {
+        in_cnt[j] = 0;
+        if (s == 0) atomicOr(status, QEM_ST_OVERFLOW);
+        return;
+    }
+    const int c = cell[j];
+    const int cx = c / g.ncy, cy = c - cx * g.ncy;
+    int cc[5], n[5], tot = 0;
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+        int ox, oy;
+        half_offset(d, ox, oy);
+        cc[d] = wrap_cell(cx - ox, g.ncx) * g.ncy + wrap_cell(cy - oy, g.ncy);
+        n[d] = in_slot[(size_t)5 * s + d];
+        tot += n[d];
+    }
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+        int b = 0;
+#pragma unroll
+        for (int e = 0; e < 5; e++) b += cc[e] < cc[d] ? n[e] : 0;
+        in_slot[(size_t)5 * s + d] = b;
+    }
+    in_cnt[j] = tot;
+}
+
+// ---------------------------------------------------------------------------
 // incoming pairs per particle (CSR over the second index), sorted by pair id
 // ---------------------------------------------------------------------------
 // the pair count lives on the device (*np = poff[N]); grids are sized for
@@ -542,32 +699,35 @@ cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *p
     return cudaGetLastError();
 }
 
-cudaError_t qem_launch_pair_count(int N, const double4 *pos_c, const int *cell, const int *cell_start,
-                                  const int *cell_list, CellGeom g, double rc2, int *pcount, cudaStream_t s)
+cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const int *cell, const int *cell_start,
+                                 const int *cell_list, CellGeom g, double rc2, int *pcount, int64_t *poff,
+                                 int2 *pairs, int64_t cap, int *in_cnt, int *in_slot, int64_t *in_off, int *in_list,
+                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
 {
+    if (N <= 0) return cudaSuccess;
+    cudaError_t e;
+    if (g.ncx >= 3 && g.ncy >= 3) {
+        const int nb = nblk((int64_t)ncell * 32, 128);
+        k_pairs_cell<false><<<nb, 128, 0, s>>>(ncell, pos_c, cell_start, cell_list, g, rc2, pcount, nullptr, nullptr,
+                                               0, in_slot, nullptr, nullptr, nullptr);
+        if ((e = scan_impl<int, int64_t>(pcount, poff, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
+        k_in_base<<<nblk(N, 256), 256, 0, s>>>(N, cell_list, cell, g, poff + N, cap, in_slot, in_cnt, status);
+        if ((e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
+        k_pairs_cell<true><<<nb, 128, 0, s>>>(ncell, pos_c, cell_start, cell_list, g, rc2, nullptr, poff, pairs, cap,
+                                              in_slot, in_off, in_list, status);
+        return cudaGetLastError();
+    }
+    // fewer than 3 cells along x or y: one thread per owner over the full
+    // deduplicated stencil, incoming entries scattered with atomics and sorted
     k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
                                                  nullptr, 0, nullptr, nullptr);
-    return cudaGetLastError();
-}
-
-cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, const int *cell_start,
-                                 const int *cell_list, CellGeom g, double rc2, const int64_t *poff, int2 *pairs,
-                                 int64_t cap, int *in_cnt, unsigned *status, cudaStream_t s)
-{
+    if ((e = scan_impl<int, int64_t>(pcount, poff, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(in_cnt, 0, sizeof(int) * N, s)) != cudaSuccess) return e;
     k_pairs<true><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, nullptr, poff, pairs,
                                                 cap, in_cnt, status);
-    return cudaGetLastError();
-}
-
-cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
-                                int64_t *in_off, int *in_fill, int *in_list, void *scan_tmp,
-                                size_t scan_tmp_bytes, cudaStream_t s)
-{
-    cudaError_t e = cudaMemsetAsync(in_fill, 0, sizeof(int) * N, s);
-    if (e != cudaSuccess) return e;
-    e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s);
-    if (e != cudaSuccess) return e;
-    if (cap > 0) k_in_fill<<<nblk(cap, 256), 256, 0, s>>>(np, cap, pairs, in_off, in_fill, in_list);
+    if ((e = cudaMemsetAsync(in_slot, 0, sizeof(int) * N, s)) != cudaSuccess) return e;
+    if ((e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
+    if (cap > 0) k_in_fill<<<nblk(cap, 256), 256, 0, s>>>(poff + N, cap, pairs, in_off, in_slot, in_list);
     k_in_sort<<<nblk(N, 128), 128, 0, s>>>(N, in_off, in_list);
     return cudaGetLastError();
 }

@@ -79,17 +79,15 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
 cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *pos, int *cell_cnt, int *cell_start,
                              int *cell_fill, int *cell_list, int *pos_of, double4 *pos_c, void *scan_tmp,
                              size_t scan_tmp_bytes, cudaStream_t s);
-cudaError_t qem_launch_pair_count(int N, const double4 *pos_c, const int *cell, const int *cell_start,
-                                  const int *cell_list, CellGeom g, double rc2, int *pcount, cudaStream_t s);
-// fills at most cap pairs (QEM_ST_OVERFLOW beyond) and counts incoming pairs
-// per particle into in_cnt (zeroed by the caller)
-cudaError_t qem_launch_pair_fill(int N, const double4 *pos_c, const int *cell, const int *cell_start,
-                                 const int *cell_list, CellGeom g, double rc2, const int64_t *poff, int2 *pairs,
-                                 int64_t cap, int *in_cnt, unsigned *status, cudaStream_t s);
-// np: device pointer to the pair count (poff[N])
-cudaError_t qem_launch_incoming(int N, const int64_t *np, int64_t cap, const int2 *pairs, const int *in_cnt,
-                                int64_t *in_off, int *in_fill, int *in_list, void *scan_tmp,
-                                size_t scan_tmp_bytes, cudaStream_t s);
+// pair list (owner, other) in poff order and the incoming lists: pcount and
+// poff per cell-order position (poff[N] = number of pairs, on the device), at
+// most cap pairs stored (QEM_ST_OVERFLOW beyond), in_cnt / in_off per
+// particle with in_list in ascending pair order and in_off[N] <= cap (no
+// incoming entries at all after an overflow); in_slot is scratch of 5 N ints
+cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const int *cell, const int *cell_start,
+                                 const int *cell_list, CellGeom g, double rc2, int *pcount, int64_t *poff,
+                                 int2 *pairs, int64_t cap, int *in_cnt, int *in_slot, int64_t *in_off, int *in_list,
+                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
