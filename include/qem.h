@@ -145,6 +145,34 @@ qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K
 qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P);
 qem_status qem_get_kset(const qem_handle *h, double *k3_out, int32_t cap, int32_t *P, double *sum_K);
 
+/* Most k-vectors of one k-set (the k-space passes put 16 k-vectors per block
+ * along a grid dimension of at most 65535 blocks). */
+#define QEM_MAX_KSET 1048560
+
+/* Exact (non-random-batch) k-sum, F_long's rbe_mode = false branch
+ * (Force_long.jl:220-233; python_lib Force_long_range_njit_exact.py:10-45):
+ * every lattice vector k = 2 pi (m / Lx, n / Ly) with 0 < |k| < k_cutoff, each
+ * weighted by exp(-|k|^2 / 4 alpha) in place of the random batch's sum_K / P.
+ * Two typos of the Julia branch are fixed: the lattice bound is
+ * trunc(k_cutoff L / 2 pi) (written k_cutoff * L_x / 2 * pi, lines 221-222)
+ * and |k| = sqrt(kx^2 + ky^2) (written sqrt(k_x^2 + k_y), line 227); the k = 0
+ * lattice point, which that loop would also visit, is the separate k = 0 term.
+ * QEM_inter (Quasi_Ewald_Method.jl:16) takes k_cutoff = 2 s sqrt(alpha).
+ *
+ * qem_exact_kset_rows writes up to cap rows (kx, ky, |k|) and weights in the
+ * Julia loop order (m outer, n inner) and the full count (host only; no GPU
+ * needed).  qem_set_kset_weighted feeds any k-set with per-row weights (sum_K
+ * then reports the sum of the weights); qem_set_kset_exact generates and feeds
+ * the exact set of the handle's box and alpha.  qem_set_kset and
+ * qem_sample_kset return the handle to uniform sum_K / P weights, and so does
+ * QEM_RESAMPLE_KSET at its next draw.  qem_get_kset_weights reports P = 0 for
+ * a uniform k-set. */
+qem_status qem_exact_kset_rows(double Lx, double Ly, double alpha, double k_cutoff, double *k3, double *w,
+                               int64_t cap, int64_t *count);
+qem_status qem_set_kset_weighted(qem_handle *h, const double *k3, const double *w, int32_t P);
+qem_status qem_set_kset_exact(qem_handle *h, double k_cutoff, int32_t *P);
+qem_status qem_get_kset_weights(const qem_handle *h, double *w_out, int32_t cap, int32_t *P);
+
 /* Fused evaluation: short range (+ self terms) + long range + walls.
  * F: 3N doubles (overwritten).  energy: NULL or one double receiving the QEM
  * short + long energy (Substrate_LJ has no energy in the reference). */

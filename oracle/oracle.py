@@ -94,6 +94,9 @@ def lib():
             "qo_pairs_eval": (None, [P, dp, dp, C.c_long, ip, dp, C.c_int]),
             "qo_self_eval": (None, [P, C.c_int, dp, dp, dp, C.c_int]),
             "qo_max_threads": (C.c_int, []),
+            "qo_exact_kset": (C.c_long, [C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, C.c_long]),
+            "qo_F_long_w": (None, [P, C.c_int, dp, dp, ip, C.c_int, dp, dp, dp, C.c_int]),
+            "qo_energy_long_w": (C.c_double, [P, C.c_int, dp, dp, ip, C.c_int, dp, dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -262,6 +265,35 @@ def F_long(p, xyz, q, kset, sum_K, zlist=None, nthreads=0):
     zl = None if zlist is None else _i(zlist)[1]
     lib().qo_F_long(C.byref(p), xyz.shape[0], px, _d(q)[1], zl, kset.shape[0], pk, sum_K, _d(F)[1], nthreads)
     return F
+
+
+def exact_kset(L, alpha, k_cutoff):
+    """Exact-sum k-set (Force_long.jl:220-233, typos fixed): rows (kx, ky, k) of every
+    lattice vector with 0 < k < k_cutoff in the Julia loop order, and weights e^{-k^2/4 alpha}."""
+    n = lib().qo_exact_kset(L[0], L[1], alpha, k_cutoff, None, None, 0)
+    k3 = np.zeros((n, 3))
+    w = np.zeros(n)
+    lib().qo_exact_kset(L[0], L[1], alpha, k_cutoff, _d(k3)[1], _d(w)[1], n)
+    return k3, w
+
+
+def F_long_weighted(p, xyz, q, kset, w, zlist=None, nthreads=0):
+    """F_long with a per-k weight w[m] in place of sum_K / P (exact k-sum: w = e^{-k^2/4 alpha})."""
+    xyz, px = _d(xyz)
+    kset, pk = _d(kset)
+    w, pw = _d(w)
+    F = np.zeros_like(xyz)
+    zl = None if zlist is None else _i(zlist)[1]
+    lib().qo_F_long_w(C.byref(p), xyz.shape[0], px, _d(q)[1], zl, kset.shape[0], pk, pw, _d(F)[1], nthreads)
+    return F
+
+
+def energy_long_weighted(p, xyz, q, kset, w, zlist=None):
+    xyz, px = _d(xyz)
+    kset, pk = _d(kset)
+    w, pw = _d(w)
+    zl = None if zlist is None else _i(zlist)[1]
+    return lib().qo_energy_long_w(C.byref(p), xyz.shape[0], px, _d(q)[1], zl, kset.shape[0], pk, pw)
 
 
 def energy_short(p, xyz, q, pair_list=None, nthreads=0):

@@ -805,6 +805,78 @@ double qo_energy_long(const qo_params *p, int N, const double *xyz, const double
 }
 
 /* ------------------------------------------------------------------ */
+/* Exact (non-random-batch) k-sum, Force_long.jl:220-233 with its two    */
+/* typos fixed: the lattice bound trunc(k_c L / (2 pi)) (written         */
+/* k_cutoff * L_x / 2 * pi at 221-222) and k = sqrt(k_x^2 + k_y^2)        */
+/* (written sqrt(k_x^2 + k_y) at 227).  The k = 0 lattice point, which    */
+/* the loop would pass to F_l_total (k_x / k = 0 / 0), is left out: the   */
+/* k = 0 term is Flz_sort_k0.  Every k carries the weight e^{-k^2/4a}     */
+/* (232), as in the python exact path (Force_long_range_njit_exact.py:    */
+/* 19-34, whose KCAR shells cut at k <= k_f1).                            */
+/* ------------------------------------------------------------------ */
+/* rows in the Julia loop order (n_x outer, n_y inner); returns the count
+ * (rows written up to cap; k3 / w may be NULL to count only) */
+long qo_exact_kset(double Lx, double Ly, double alpha, double k_cutoff, double *k3, double *w, long cap)
+{
+    const long nx = (long)(k_cutoff * Lx / (2 * QO_PI)), ny = (long)(k_cutoff * Ly / (2 * QO_PI));
+    long n = 0;
+    for (long a = -nx; a <= nx; a++)
+        for (long b = -ny; b <= ny; b++) {
+            if (a == 0 && b == 0) continue;
+            const double kx = 2 * QO_PI * a / Lx, ky = 2 * QO_PI * b / Ly;
+            const double k = sqrt(kx * kx + ky * ky);
+            if (!(k < k_cutoff)) continue;
+            if (n < cap) {
+                if (k3) {
+                    k3[3 * n] = kx;
+                    k3[3 * n + 1] = ky;
+                    k3[3 * n + 2] = k;
+                }
+                if (w) w[n] = exp(-k * k / (4 * alpha));
+            }
+            n++;
+        }
+    return n;
+}
+
+/* F_long with a per-k weight w[m] in place of sum_K / P (Force_long.jl:232) */
+void qo_F_long_w(const qo_params *p, int N, const double *xyz, const double *q, const int *zlist_in, int P,
+                 const double *kset, const double *w, double *F, int nthreads)
+{
+    int *zlist = malloc(sizeof(int) * (N > 0 ? N : 1));
+    if (zlist_in) memcpy(zlist, zlist_in, sizeof(int) * N);
+    else qo_sortperm_z(N, xyz, zlist);
+    double *t = malloc(sizeof(double) * 3 * (size_t)(N > 0 ? N : 1));
+    qo_Flz_sort_k0(N, zlist, q, t);
+    double den0 = 2 * p->Lx * p->Ly * p->eps_0;
+    for (int i = 0; i < 3 * N; i++) F[i] = 0 + t[i] / den0;
+    for (int m = 0; m < P; m++) {
+        qo_F_l_total(p, kset + 3 * m, N, xyz, q, zlist, t, nthreads);
+        for (int i = 0; i < 3 * N; i++) F[i] += t[i] * w[m];
+    }
+    free(t);
+    free(zlist);
+}
+
+/* energy_long with a per-k weight w[m] in place of sum_K / P */
+double qo_energy_long_w(const qo_params *p, int N, const double *xyz, const double *q, const int *zlist_in, int P,
+                        const double *kset, const double *w)
+{
+    int *zlist = malloc(sizeof(int) * (N > 0 ? N : 1));
+    if (zlist_in) memcpy(zlist, zlist_in, sizeof(int) * N);
+    else qo_sortperm_z(N, xyz, zlist);
+    double Es = 0, Ens = 0;
+    for (int m = 0; m < P; m++) {
+        Es += -w[m] * qo_sigma_s(kset + 3 * m, N, xyz, q, p->gamma_1, p->gamma_2, p->Lz) /
+              (2 * p->eps_0 * p->Lx * p->Ly);
+        Ens += -w[m] * qo_sigma_ns(kset + 3 * m, N, xyz, q, zlist) / (2 * p->eps_0 * p->Lx * p->Ly);
+    }
+    double E = Es + Ens + qo_energy_k0(p, N, xyz, q, zlist);
+    free(zlist);
+    return E;
+}
+
+/* ------------------------------------------------------------------ */
 /* Bounded-sample drivers for the timed CPU baseline (bench.py).        */
 /* ------------------------------------------------------------------ */
 /* F_short_ij for npairs pairs (4 doubles per pair, see qo_F_short_ij). */

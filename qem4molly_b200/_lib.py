@@ -25,6 +25,7 @@ QEM_FP64, QEM_FP32_FIX = 0, 1
 QEM_TERM_SHORT, QEM_TERM_LONG, QEM_TERM_LJ, QEM_TERM_ALL = 0x1, 0x2, 0x4, 0x7
 QEM_MEM_HOST, QEM_MEM_DEVICE = 0, 1
 QEM_NOALLOC_MAX_N, QEM_NOALLOC_MAX_P = 32768, 512
+QEM_MAX_KSET = 1048560
 
 
 class QemError(RuntimeError):
@@ -82,6 +83,11 @@ def load(build: bool = False):
         "qem_set_kset": (C.c_int32, [H, dp, C.c_int32, C.c_double]),
         "qem_sample_kset": (C.c_int32, [H, C.c_uint64, C.c_int32]),
         "qem_get_kset": (C.c_int32, [H, dp, C.c_int32, ip, dp]),
+        "qem_exact_kset_rows": (C.c_int32, [C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64,
+                                            C.POINTER(C.c_int64)]),
+        "qem_set_kset_weighted": (C.c_int32, [H, dp, dp, C.c_int32]),
+        "qem_set_kset_exact": (C.c_int32, [H, C.c_double, ip]),
+        "qem_get_kset_weights": (C.c_int32, [H, dp, C.c_int32, ip]),
         "qem_forces": (C.c_int32, [H, C.c_int32, vp, vp, vp, dp, C.c_uint32, C.c_int32, vp]),
         "qem_short_forces": (C.c_int32, [H, C.c_int32, vp, vp, vp, C.c_int32, vp]),
         "qem_long_forces": (C.c_int32, [H, C.c_int32, vp, vp, vp, C.c_int32, vp]),

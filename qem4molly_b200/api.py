@@ -100,6 +100,33 @@ class Engine:
     def sample_kset(self, seed, P):
         self._check(self._lib.qem_sample_kset(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(P)))
 
+    def set_kset_weighted(self, k3, w):
+        """k-set rows (kx, ky, |k|) with a weight per row in place of sum_K / P."""
+        k3 = np.ascontiguousarray(k3, dtype=np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+        if w.shape[0] != k3.shape[0]:
+            raise ValueError("one weight per k-vector")
+        self._check(self._lib.qem_set_kset_weighted(self._h, k3.ctypes.data_as(C.POINTER(C.c_double)),
+                                                    w.ctypes.data_as(C.POINTER(C.c_double)), k3.shape[0]))
+
+    def set_kset_exact(self, k_cutoff):
+        """Exact (non-random-batch) k-sum: every lattice k with 0 < |k| < k_cutoff, weight
+        exp(-k^2 / 4 alpha) (Force_long.jl:220-233).  Returns the number of k-vectors."""
+        P = C.c_int32()
+        self._check(self._lib.qem_set_kset_exact(self._h, float(k_cutoff), C.byref(P)))
+        return P.value
+
+    def get_kset_weights(self):
+        """Per-row weights of a weighted k-set, or None for uniform sum_K / P weights."""
+        P = C.c_int32()
+        self._check(self._lib.qem_get_kset_weights(self._h, None, 0, C.byref(P)))
+        if P.value == 0:
+            return None
+        w = np.zeros(P.value)
+        self._check(self._lib.qem_get_kset_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_double)), P.value,
+                                                   C.byref(P)))
+        return w
+
     def get_kset(self):
         P = C.c_int32()
         s = C.c_double()
@@ -260,23 +287,26 @@ class QEM_short:
 
 class QEM_long:
     """QEM_long(L; k_cutoff, z_list, gamma_1, gamma_2, eps_0, accuracy, alpha, rbe_mode, rbe_p)
-    (QEM_long.jl:19-30).  A fresh random batch of rbe_p k-vectors is drawn on every forces call,
-    as Force_long.jl:235 does; pass `resample=False` to keep one batch."""
+    (QEM_long.jl:19-30).  rbe_mode=True: a fresh random batch of rbe_p k-vectors is drawn on every
+    forces call, as Force_long.jl:235 does (pass `resample=False` to keep one batch).
+    rbe_mode=False: the exact k-sum of Force_long.jl:220-233 (typos fixed) over every lattice k with
+    0 < |k| < k_cutoff, weighted by exp(-k^2 / 4 alpha)."""
 
     def __init__(self, L, *, k_cutoff=1.0, z_list=(), gamma_1=0, gamma_2=0, eps_0=1, accuracy=1e-6, alpha=1,
                  rbe_mode=True, rbe_p=30, precision="fp64", mode="julia", seed=0, resample=True, device=0):
-        if not rbe_mode:
-            raise NotImplementedError("rbe_mode=false: the exact k-sum branch of Force_long.jl:220-233 is not "
-                                      "provided (it is broken in the reference)")
         self.L, self.k_cutoff, self.z_list = tuple(L), k_cutoff, list(z_list)
         self.gamma_1, self.gamma_2, self.eps_0, self.accuracy = gamma_1, gamma_2, eps_0, accuracy
         self.alpha, self.rbe_mode, self.rbe_p = alpha, rbe_mode, rbe_p
-        flags = _mode_flags(mode) | (L.QEM_RESAMPLE_KSET if resample else 0)
+        flags = _mode_flags(mode) | (L.QEM_RESAMPLE_KSET if (resample and rbe_mode) else 0)
         # the short-range cutoff is irrelevant for the long range; any value < L/2 is valid
         self.engine = Engine(L_box=self.L, alpha=alpha, r_cutoff=0.25 * min(self.L[0], self.L[1]),
-                             gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0, accuracy=accuracy, rbe_p=rbe_p,
-                             mode_flags=flags, precision=_precision(precision), device=device)
-        self.engine.sample_kset(seed, rbe_p)
+                             gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0, accuracy=accuracy,
+                             rbe_p=rbe_p if rbe_mode else 0, mode_flags=flags, precision=_precision(precision),
+                             device=device)
+        if rbe_mode:
+            self.engine.sample_kset(seed, rbe_p)
+        else:
+            self.n_k = self.engine.set_kset_exact(k_cutoff)
 
 
 def QEM_inter(n_atoms, L, *, s=1.0, accuracy=1e-6, rbe_mode=True, rbe_p=30, eps_0=1.0, gamma_1=0.0, gamma_2=0.0,

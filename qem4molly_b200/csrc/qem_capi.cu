@@ -130,6 +130,7 @@ struct qem_handle {
     std::string err;
     // k-set (host master copy)
     std::vector<double> kset;
+    std::vector<double> kwt;  // per-k weights of a weighted (exact) k-set; empty: sum_K / P for every k
     double sum_K = 0;
     int P = 0;
     bool has_kset = false, kset_dirty = true;
@@ -149,8 +150,8 @@ struct qem_handle {
     // device scratch
     DevBuf xyz, q, F, pos, cell, cell_cnt, cell_start, cell_fill, cell_list, pos_of, pcount, poff, pairs, R, Upair,
         in_cnt, in_off, in_fill, in_list, scan_tmp;
-    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, tot, off, Utot, kf, Epart, status,
-        Eout, Fpart, pos_c;
+    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, kw, tot, off, Utot, kf, Epart,
+        status, Eout, Fpart, pos_c;
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
     // adjoint pass
@@ -230,7 +231,7 @@ static qem_status validate(const qem_params *p, std::string &why)
     if (!(p->accuracy > 0 && p->accuracy < 1)) { why = "accuracy must be in (0, 1)"; return QEM_ERR_ARG; }
     if (!finite_pos(p->eps_0)) { why = "eps_0 must be > 0"; return QEM_ERR_ARG; }
     if (p->N_t < 1 || p->N_t > QEM_MAX_NT) { why = "N_t must be in 1..64"; return QEM_ERR_ARG; }
-    if (p->rbe_p < 0) { why = "rbe_p must be >= 0"; return QEM_ERR_ARG; }
+    if (p->rbe_p < 0 || p->rbe_p > QEM_MAX_KSET) { why = "rbe_p must be in 0 .. QEM_MAX_KSET"; return QEM_ERR_ARG; }
     if (p->iter_period < 1) { why = "iter_period must be >= 1"; return QEM_ERR_ARG; }
     if (!std::isfinite(p->gamma_up) || !std::isfinite(p->gamma_down) || !(fabs(p->gamma_up * p->gamma_down) < 1.0)) {
         why = "|gamma_up * gamma_down| must be < 1 (the regularised gamma >= 1 path is not provided)";
@@ -325,6 +326,7 @@ static void sample_kset(qem_handle *h, int P)
 {
     const qem_params &p = h->p;
     h->kset.resize(3 * (size_t)P);
+    h->kwt.clear();
     double kmax = 0;
     for (int i = 0; i < P;) {
         const double ux = uniform01(h->rng) * h->cdfx.back(), uy = uniform01(h->rng) * h->cdfy.back();
@@ -354,6 +356,7 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
                                LongBuffers &b)
 {
     CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
+    CU(grow(h->kw, sizeof(double) * std::max(Pk, 1)));
     CU(grow(h->zperm, sizeof(int) * N));
     CU(grow(h->ztmp, sizeof(int) * N));
     CU(grow(h->zkey, sizeof(double) * N));
@@ -379,6 +382,7 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
     b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
     b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
     b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
+    b.kwt = h->kwt.empty() ? nullptr : ptr<double>(h->kw);
     b.tot = ptr<double>(h->tot); b.off = ptr<double>(h->off); b.Utot = ptr<double>(h->Utot);
     b.kf = h->kf.p;
     b.Epart = Ep + nbS;
@@ -550,6 +554,8 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         if ((h->kset_dirty || h->kin_lo != k_lo || h->kin_hi != k_hi) && Pk > 0) {
             CU(cudaMemcpyAsync(h->kin.p, h->kset.data() + 3 * (size_t)k_lo, sizeof(double) * 3 * Pk,
                                cudaMemcpyHostToDevice, sl));
+            if (!h->kwt.empty())
+                CU(cudaMemcpyAsync(h->kw.p, h->kwt.data() + k_lo, sizeof(double) * Pk, cudaMemcpyHostToDevice, sl));
             h->kset_dirty = false;
             h->kin_lo = k_lo;
             h->kin_hi = k_hi;
@@ -873,7 +879,7 @@ void qem_destroy(qem_handle *h)
     DevBuf *bufs[] = {&h->xyz, &h->q, &h->F, &h->pos, &h->cell, &h->cell_cnt, &h->cell_start, &h->cell_fill,
                       &h->cell_list, &h->pos_of, &h->pcount, &h->poff, &h->pairs, &h->R, &h->Upair, &h->in_cnt,
                       &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
-                      &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin,
+                      &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin, &h->kw,
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
@@ -898,18 +904,28 @@ void qem_destroy(qem_handle *h)
 const char *qem_last_error(const qem_handle *h) { return h ? h->err.c_str() : "NULL handle"; }
 const char *qem_status_string(qem_status s) { return status_str(s); }
 
-qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K)
+// rows (kx, ky, |k|) with |k| > 0; returns the largest |k| or -1
+static double check_krows(const double *k3, int P)
 {
-    if (!h) return QEM_ERR_ARG;
-    if (P < 0 || (P > 0 && !k3) || !std::isfinite(sum_K)) return fail(h, QEM_ERR_ARG, "bad k-set arguments");
     double kmax = 0;
     for (int i = 0; i < P; i++) {
         const double kx = k3[3 * i], ky = k3[3 * i + 1], k = k3[3 * i + 2];
         if (!std::isfinite(kx) || !std::isfinite(ky) || !(k > 0) || fabs(kx * kx + ky * ky - k * k) > 1e-9 * k * k)
-            return fail(h, QEM_ERR_ARG, "k-set rows must be (kx, ky, |k|) with |k| > 0 (Force_long.jl:7)");
+            return -1;
         kmax = std::max(kmax, k);
     }
+    return kmax;
+}
+
+qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (P < 0 || (P > 0 && !k3) || !std::isfinite(sum_K)) return fail(h, QEM_ERR_ARG, "bad k-set arguments");
+    if (P > QEM_MAX_KSET) return fail(h, QEM_ERR_RANGE, "more k-vectors than QEM_MAX_KSET");
+    const double kmax = check_krows(k3, P);
+    if (kmax < 0) return fail(h, QEM_ERR_ARG, "k-set rows must be (kx, ky, |k|) with |k| > 0 (Force_long.jl:7)");
     h->kset.assign(k3, k3 + 3 * (size_t)P);
+    h->kwt.clear();
     h->P = P;
     h->sum_K = sum_K;
     h->kmax = kmax;
@@ -919,10 +935,84 @@ qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K
     return QEM_OK;
 }
 
+qem_status qem_set_kset_weighted(qem_handle *h, const double *k3, const double *w, int32_t P)
+{
+    if (!h) return QEM_ERR_ARG;
+    if (P < 0 || (P > 0 && (!k3 || !w))) return fail(h, QEM_ERR_ARG, "bad k-set arguments");
+    if (P > QEM_MAX_KSET) return fail(h, QEM_ERR_RANGE, "more k-vectors than QEM_MAX_KSET");
+    const double kmax = check_krows(k3, P);
+    if (kmax < 0) return fail(h, QEM_ERR_ARG, "k-set rows must be (kx, ky, |k|) with |k| > 0 (Force_long.jl:7)");
+    double sw = 0;
+    for (int i = 0; i < P; i++) {
+        if (!std::isfinite(w[i])) return fail(h, QEM_ERR_ARG, "k weights must be finite");
+        sw += w[i];
+    }
+    h->kset.assign(k3, k3 + 3 * (size_t)P);
+    h->kwt.assign(w, w + P);
+    h->P = P;
+    h->sum_K = sw;
+    h->kmax = kmax;
+    h->has_kset = true;
+    h->kset_dirty = true;
+    h->cfg_version++;
+    return QEM_OK;
+}
+
+qem_status qem_exact_kset_rows(double Lx, double Ly, double alpha, double k_cutoff, double *k3, double *w,
+                               int64_t cap, int64_t *count)
+{
+    if (!count || !(Lx > 0) || !(Ly > 0) || !(alpha > 0) || !(k_cutoff > 0) || !std::isfinite(k_cutoff) ||
+        cap < 0 || (cap > 0 && (!k3 || !w)))
+        return QEM_ERR_ARG;
+    const double nxf = k_cutoff * Lx / (2.0 * QEM_PI), nyf = k_cutoff * Ly / (2.0 * QEM_PI);
+    if (nxf > 1e5 || nyf > 1e5) return QEM_ERR_RANGE;
+    const int64_t nx = (int64_t)nxf, ny = (int64_t)nyf;
+    int64_t n = 0;
+    for (int64_t a = -nx; a <= nx; a++)
+        for (int64_t b = -ny; b <= ny; b++) {
+            if (a == 0 && b == 0) continue;  // the k = 0 term is separate (Force_long.jl:214)
+            const double kx = 2.0 * QEM_PI * (double)a / Lx, ky = 2.0 * QEM_PI * (double)b / Ly;
+            const double k = sqrt(kx * kx + ky * ky);
+            if (!(k < k_cutoff)) continue;
+            if (n < cap) {
+                k3[3 * n] = kx;
+                k3[3 * n + 1] = ky;
+                k3[3 * n + 2] = k;
+                w[n] = exp(-k * k / (4.0 * alpha));
+            }
+            n++;
+        }
+    *count = n;
+    return QEM_OK;
+}
+
+qem_status qem_set_kset_exact(qem_handle *h, double k_cutoff, int32_t *P)
+{
+    if (!h) return QEM_ERR_ARG;
+    int64_t n = 0;
+    qem_status st = qem_exact_kset_rows(h->p.Lx, h->p.Ly, h->p.alpha, k_cutoff, nullptr, nullptr, 0, &n);
+    if (st != QEM_OK) return fail(h, st, "exact k-set: need k_cutoff > 0 and at most 1e5 lattice steps per axis");
+    if (n > QEM_MAX_KSET) return fail(h, QEM_ERR_RANGE, "exact k-set larger than QEM_MAX_KSET: lower k_cutoff");
+    std::vector<double> k3(3 * (size_t)std::max<int64_t>(n, 1)), w((size_t)std::max<int64_t>(n, 1));
+    st = qem_exact_kset_rows(h->p.Lx, h->p.Ly, h->p.alpha, k_cutoff, k3.data(), w.data(), n, &n);
+    if (st != QEM_OK) return fail(h, st, "exact k-set generation failed");
+    if (P) *P = (int32_t)n;
+    return qem_set_kset_weighted(h, k3.data(), w.data(), (int32_t)n);
+}
+
+qem_status qem_get_kset_weights(const qem_handle *h, double *w_out, int32_t cap, int32_t *P)
+{
+    if (!h || !P) return QEM_ERR_ARG;
+    *P = h->kwt.empty() ? 0 : h->P;
+    if (w_out && cap > 0 && !h->kwt.empty()) memcpy(w_out, h->kwt.data(), sizeof(double) * (size_t)std::min(cap, h->P));
+    return QEM_OK;
+}
+
 qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P)
 {
     if (!h) return QEM_ERR_ARG;
     if (P < 0) return fail(h, QEM_ERR_ARG, "P < 0");
+    if (P > QEM_MAX_KSET) return fail(h, QEM_ERR_RANGE, "more k-vectors than QEM_MAX_KSET");
     h->rng = seed;
     sample_kset(h, P);
     return QEM_OK;
@@ -1176,6 +1266,8 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         }
         if ((h->kset_dirty || h->kin_lo != 0 || h->kin_hi != Pk) && Pk > 0) {
             CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
+            if (!h->kwt.empty())
+                CU(cudaMemcpyAsync(h->kw.p, h->kwt.data(), sizeof(double) * Pk, cudaMemcpyHostToDevice, s));
             h->kset_dirty = false;
             h->kin_lo = 0;
             h->kin_hi = Pk;

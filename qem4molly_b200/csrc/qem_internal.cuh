@@ -126,6 +126,7 @@ struct LongBuffers {
     void *stmp;           // scan scratch
     size_t stmp_bytes;
     int skip_k0 = 0;      // 1: leave out the k = 0 term (sharded ranks other than 0)
+    const double *kwt = nullptr;  // P per-k weights (exact k-sum); nullptr: sum_K / P for every k
 };
 // number of k slices for nch chunks and P k-vectors (at most max_ks)
 int qem_long_ksplit(int nch, int P, int max_ks);

@@ -60,8 +60,11 @@ struct LM<double> {
     static __device__ __forceinline__ void sc(double turns, double &s, double &c) { sincospi(2.0 * turns, &s, &c); }
 };
 
+// wk, esc: the force and energy weights of every k (random batch, sum_K / P
+// folded in); with per-k weights kwt (exact k-sum) wk = kwt / wden and
+// esc = -kwt / eden instead
 __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
-                         double wk, double esc)
+                         double wk, double esc, const double *__restrict__ kwt, double wden, double eden)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= P) return;
@@ -74,8 +77,8 @@ __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restri
     K.g = 0.5 / (g12 * exp(-2.0 * k * Lz) - 1.0);
     K.fx = kx / k;
     K.fy = ky / k;
-    K.wk = wk;
-    K.ek = esc / k;
+    K.wk = kwt ? kwt[m] / wden : wk;
+    K.ek = (kwt ? -kwt[m] / eden : esc) / k;
     kc[m] = K;
 }
 
@@ -1083,7 +1086,8 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         if (P > 0) {
             const double wk = (sum_K / P) / (Lx * Ly * eps0);
             const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
-            k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc);
+            k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
+                                                  2.0 * eps0 * Lx * Ly);
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);

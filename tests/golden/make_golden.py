@@ -26,6 +26,10 @@ What is generated (each case states the reference file it exercises):
   accurate-Bessel shim, so the python-convention oracle mode is pinned to
   ~1e-12.
 * ``icm_energy.json``  -- ICM.U_cal / ICM.F_cal on a 3-particle slab.
+* ``long_exact.json``  -- the exact (non-random-batch) long range of
+  Force_long_range_njit_exact.Force_long_cal on a 24-particle slab, with every
+  lattice vector up to the cutoff (k-sorted rows, so its k <= k_f1 loop takes
+  exactly that set).
 
 The accurate-Bessel shim replaces the python_lib ``Bessel`` module (whose J1
 has ~1.5e-5 absolute error) by numba functions calling libm's j0/j1, exactly
@@ -254,6 +258,50 @@ def gen_system(rng):
         E_long_k=Es_k + Ens_k, E_long_k0=E_k0)
 
 
+def gen_exact(rng):
+    """Exact (non-random-batch) long range: Force_long_range_njit_exact.Force_long_cal on a
+    24-particle slab.  Its loop takes KCAR rows while k <= k_f1 (line 19); the rows given
+    here are every lattice vector sorted by k, with one row past the cutoff, so the sum runs
+    over exactly {0 < k <= k_f1}, each k weighted by e^{-k^2/4 alpha} (lines 29-34)."""
+    import numpy as np
+
+    import Force_long_range_njit_exact as FE
+
+    N, Lx, Ly, Lz = 24, 12.0, 10.0, 3.0
+    alpha, k_c = 0.8, 2.95
+    g1, g2 = 0.6, -0.45  # gamma_down, gamma_up
+    e1 = (1 - g1) / (1 + g1)
+    e3 = (1 - g2) / (1 + g2)
+    q = np.array([1.0 if i % 2 == 0 else -1.0 for i in range(N)])
+    x = rng.random(N) * Lx
+    y = rng.random(N) * Ly
+    z = 0.3 + rng.random(N) * (Lz - 0.6)
+    POSCAR = np.stack([q, x, y, z], axis=1)
+    M = int(k_c * max(Lx, Ly) / (2 * np.pi)) + 2
+    rows = []
+    for m1 in range(-M, M + 1):
+        for m2 in range(-M, M + 1):
+            if m1 == 0 and m2 == 0:
+                continue
+            kx, ky = 2 * np.pi * m1 / Lx, 2 * np.pi * m2 / Ly
+            K = kx * kx + ky * ky
+            rows.append([kx, ky, K, np.sqrt(K)])
+    rows.sort(key=lambda r: r[3])
+    KCAR = np.array(rows)
+    n_in = int(np.sum(KCAR[:, 3] <= k_c))
+    assert np.min(np.abs(KCAR[:, 3] - k_c)) > 1e-9 and n_in < len(rows)
+    KCAR = KCAR[: n_in + 1].copy()
+    zl = np.argsort(z, kind="stable")
+    eq_cell = zl.reshape(N, 1).copy()
+    eq_size = np.arange(1, N + 1)
+    Fx, Fy, Fz, Fzs = FE.Force_long_cal(POSCAR, KCAR, k_c, alpha, Lx, Ly, Lz, 1.0, e1, 1.0, e3, 0.0, zl, eq_cell,
+                                        eq_size, N)
+    return dict(source="Force_long_range_njit_exact.py:10-45 (Force_long_cal), z force plus its self part",
+                N=N, L=[Lx, Ly, Lz], alpha=alpha, k_cutoff=k_c, gamma_1=g1, gamma_2=g2, n_k=n_in,
+                q=q.tolist(), xyz=np.stack([x, y, z], 1).tolist(),
+                F_long=np.stack([Fx, Fy, Fz + Fzs], 1).tolist())
+
+
 def gen_icm(rng):
     import numpy as np
 
@@ -315,6 +363,7 @@ def run_variant(bessel):
               dict(source="test/Force_short_test.jl:55-93 with accurate J0/J1",
                    cases=gen_short_pair(np.random.default_rng(20261206), "accurate")))
         _dump("system_python.json", gen_system(np.random.default_rng(20261207)))
+        _dump("long_exact.json", gen_exact(np.random.default_rng(20261208)))
 
 
 if __name__ == "__main__":

@@ -66,3 +66,29 @@ def test_null_handle_calls_fail_cleanly(lib):
     assert lib.qem_set_kset(None, None, 0, 0.0) == 1
     assert lib.qem_last_error(None) == b"NULL handle"
     assert lib.qem_status_string(2).startswith(b"particle run out")
+
+
+def test_exact_kset_rows_match_oracle(lib):
+    """qem_exact_kset_rows (host only) gives the oracle's exact-sum k-set, Force_long.jl:220-233
+    with its typos fixed: same rows in the same order, weights exp(-k^2 / 4 alpha)."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle as O
+
+    for Lx, Ly, alpha, kc in [(12.0, 10.0, 0.8, 2.95), (100.0, 100.0, 0.1, 1.2), (37.0, 91.0, 0.3, 0.9)]:
+        n = C.c_int64()
+        dp = C.POINTER(C.c_double)
+        assert lib.qem_exact_kset_rows(Lx, Ly, alpha, kc, None, None, 0, C.byref(n)) == 0
+        k3 = np.zeros((n.value, 3))
+        w = np.zeros(n.value)
+        assert lib.qem_exact_kset_rows(Lx, Ly, alpha, kc, k3.ctypes.data_as(dp), w.ctypes.data_as(dp), n.value,
+                                       C.byref(n)) == 0
+        k3o, wo = O.exact_kset((Lx, Ly), alpha, kc)
+        np.testing.assert_array_equal(k3, k3o)
+        np.testing.assert_array_equal(w, wo)
+    n = C.c_int64()
+    assert lib.qem_exact_kset_rows(10.0, 10.0, 0.1, -1.0, None, None, 0, C.byref(n)) == 1
+    assert lib.qem_exact_kset_rows(10.0, 10.0, 0.1, 1e9, None, None, 0, C.byref(n)) == 8  # QEM_ERR_RANGE
+    assert lib.qem_set_kset_exact(None, 1.0, None) == 1

@@ -170,6 +170,29 @@ def test_system_python_convention():
     assert np.isclose(O.energy_long(p, xyz, q, k3, d["sum_K"]), d["E_long_k"] + d["E_long_k0"], rtol=1e-12)
 
 
+def test_exact_long_range_vs_python_exact():
+    """Exact k-sum (every lattice vector 0 < k < k_c, weights e^{-k^2/4 alpha}) against
+    Force_long_range_njit_exact.Force_long_cal (long_exact.json)."""
+    d = load("long_exact.json")
+    xyz, q = np.array(d["xyz"]), np.array(d["q"])
+    p = O.params(d["L"], d["alpha"], 1.0, d["gamma_1"], d["gamma_2"])
+    k3, w = O.exact_kset(d["L"], d["alpha"], d["k_cutoff"])
+    assert k3.shape[0] == d["n_k"]
+    assert np.all((k3[:, 2] > 0) & (k3[:, 2] < d["k_cutoff"]))
+    np.testing.assert_allclose(k3[:, 2], np.hypot(k3[:, 0], k3[:, 1]), rtol=1e-15)
+    np.testing.assert_allclose(w, np.exp(-k3[:, 2] ** 2 / (4 * d["alpha"])), rtol=1e-15)
+    F = O.F_long_weighted(p, xyz, q, k3, w)
+    Fr = np.array(d["F_long"])
+    assert np.abs(F - Fr).max() <= 1e-12 * np.abs(Fr).max()
+    # the weighted form with uniform weights is the random-batch F_long
+    rng = np.random.default_rng(3)
+    sel = rng.choice(k3.shape[0], 9, replace=False)
+    np.testing.assert_allclose(O.F_long_weighted(p, xyz, q, k3[sel], np.full(9, 2.5 / 9)),
+                               O.F_long(p, xyz, q, k3[sel], 2.5), rtol=0, atol=1e-15 * np.abs(Fr).max())
+    assert np.isclose(O.energy_long_weighted(p, xyz, q, k3[sel], np.full(9, 2.5 / 9)),
+                      O.energy_long(p, xyz, q, k3[sel], 2.5), rtol=1e-14)
+
+
 def test_sortperm_is_stable():
     """QEM_long.jl:39-40 sortperm: stable ascending, ties keep index order."""
     rng = np.random.default_rng(3)
