@@ -19,6 +19,11 @@ data-path collective; value = total evaluations/s over all ranks ("weak").
 velocity-Verlet steps (dt = 1e-3, unit masses) recorded once as a CUDA graph
 and replayed --steps times; value = MD steps/s of the whole batch.
 
+--workload exact measures the exact (non-random-batch) long range: every
+lattice k with 0 < |k| < 1.0 (7,9xx vectors) weighted by exp(-k^2 / 4 alpha) on a
+1e4-particle slab at the benchmark density; value = long-range evaluations/s
+(FP32+fix), the FP64 path and the oracle's CPU rate beside it.
+
 --impl reference times the FP64 CPU restatement of the reference algorithm
 (oracle/, OpenMP on all host cores) on a bounded sample of the same workload
 and extrapolates to evaluations/s of the full system.
@@ -52,9 +57,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=100_000)
-    ap.add_argument("--workload", choices=["slab", "batch"], default="slab",
+    ap.add_argument("--workload", choices=["slab", "batch", "exact"], default="slab",
                     help="slab: the N = 1e5 benchmark system (default); batch: 256 independent slabs, "
-                         "graph-replayed velocity-Verlet steps")
+                         "graph-replayed velocity-Verlet steps; exact: the exact k-sum long range")
     return ap.parse_args()
 
 
@@ -382,6 +387,107 @@ def run_batch(args):
                "particle_steps_per_s": args.steps * sum(N) * world * 1000.0 / ms, "clocks": clocks}
         print(json.dumps(out), flush=True)
 
+# ----------------------------------------------------------------------------- exact k-sum workload
+FLOPS_PER_K_TERM = 80   # op model per (k, particle) long-range term (FP32 flops)
+SFU_PER_K_TERM = 4      # MUFU ops per term in the same model
+
+
+def run_exact(args):
+    import numpy as np
+    import torch
+
+    from qem4molly_b200 import _lib as L
+    from qem4molly_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = L.load()
+    fp32_peak, mufu_peak = C.c_double(0), C.c_double(0)
+    lib.qem_measure_peaks(local, C.byref(fp32_peak), C.byref(mufu_peak))
+    N, k_c = 10_000, 1.0
+    cfg = W.config2(N=N, seed=None if rank == 0 else W.SEED0 + 2 + 1000 * rank)
+    cfg["L"] = (1000.0 * np.sqrt(N / 100_000), 1000.0 * np.sqrt(N / 100_000), 10.0)
+    rng = np.random.default_rng(W.SEED0 + 6 + 1000 * rank)
+    cfg["xyz"] = np.stack([rng.random(N) * cfg["L"][0], rng.random(N) * cfg["L"][1], 0.5 + 9 * rng.random(N)], 1)
+    engines = {}
+    for prec in ("fp32", "fp64"):
+        e = W.engine_for(cfg, prec, device=local)
+        P = e.set_kset_exact(k_c)
+        engines[prec] = e
+    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
+    q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
+    F = torch.empty_like(x)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    terms = L.QEM_TERM_LONG
+
+    def timed(e, K):
+        per = []
+        for _ in range(K):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e.forces_device(x, q, F, terms=terms)
+            b.record(stream)
+            b.synchronize()
+            per.append(a.elapsed_time(b))
+        return per
+
+    for e in engines.values():
+        for _ in range(max(args.warmup, 3)):
+            e.forces_device(x, q, F, terms=terms)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = Clocks(local)
+    K = max(3, min(args.steps, 100))
+    ms32 = max_over_ranks(float(np.mean(timed(engines["fp32"], K))), world, dev)
+    ms64 = max_over_ranks(float(np.mean(timed(engines["fp64"], max(3, K // 4)))), world, dev)
+    clocks = clk.stop()
+    F32 = engines["fp32"].forces(cfg["xyz"], cfg["q"], terms=terms)
+    F64 = engines["fp64"].forces(cfg["xyz"], cfg["q"], terms=terms)
+    err, err_max = W.rel_err(F32, F64)
+    launches = int(engines["fp32"].counts()["launches"])
+    terms_pn = P * N
+    out = None
+    if rank == 0:
+        out = {"metric": "QEM exact k-sum long-range evals/s (every lattice k with 0 < |k| < k_c, no random batch)",
+               "value": world * 1000.0 / ms32, "unit": "evals/s", "n_gpus": world, "steps": K,
+               "warmup": max(args.warmup, 3), "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32+f64fix", "data": "synthetic (seeded)",
+               "config": {"workload": f"QEM slab N={N} Lx=Ly={cfg['L'][0]:.1f} Lz=10 gamma=0.95/0.95 alpha=0.1, "
+                                      f"exact k-sum k_c={k_c} ({P} k-vectors), long range only",
+                          "N": N, "P": P, "k_cutoff": k_c,
+                          "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)"},
+               "gpu_launches": launches * K,
+               "roofline": {"bound": "mufu", "work_model": f"{FLOPS_PER_K_TERM} FP32 flops + {SFU_PER_K_TERM} MUFU "
+                                                          f"ops per (k, particle) term, {terms_pn} terms per evaluation",
+                            "achieved": terms_pn * SFU_PER_K_TERM / (ms32 * 1e-3) / 1e12, "peak": mufu_peak.value,
+                            "unit": "Tops/s",
+                            "frac": terms_pn * SFU_PER_K_TERM / (ms32 * 1e-3) / 1e12 / mufu_peak.value,
+                            "fp32": {"achieved": terms_pn * FLOPS_PER_K_TERM / (ms32 * 1e-3) / 1e12,
+                                     "peak": fp32_peak.value, "unit": "TFLOP/s"},
+                            "peak_source": "measured in this run (qem_measure_peaks)", "traffic": None},
+               "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64},
+               "force_rel_err_vs_fp64": err, "force_max_err_vs_fp64_rms": err_max, "clocks": clocks}
+    if rank == 0 and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
+        k3, w = O.exact_kset(cfg["L"], cfg["alpha"], k_c)
+        n_s = min(P, 1000)
+        t0 = time.perf_counter()
+        O.F_long_weighted(p, cfg["xyz"], cfg["q"], k3[:n_s], w[:n_s])
+        t_s = time.perf_counter() - t0
+        cores = int(O.lib().qo_max_threads())
+        out["cpu_baseline"] = {"value": 1.0 / (t_s * P / n_s), "unit": "evals/s", "cores": cores, "kind": "port",
+                               "sample": f"oracle FP64 on {cores} threads: {n_s} of {P} k-vectors over all {N} "
+                                         f"particles ({t_s:.1f} s), extrapolated to the full k-set"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args):
     rank, world, _ = dist_env()
@@ -422,6 +528,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "exact":
+        run_exact(args)
     else:
         run_ours(args)
 

@@ -109,7 +109,7 @@ extern "C" {
 
 qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t *N, qem_batch **out)
 {
-    if (!out || B <= 0 || !handles || !N) return QEM_ERR_ARG;
+    if (!out || B <= 0 || !handles || !N || !handles[0]) return QEM_ERR_ARG;
     *out = nullptr;
     qem_batch *b = new qem_batch();
     b->B = B;
@@ -130,6 +130,10 @@ qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t
         return QEM_ERR_ARG;
     }
     b->Ntot = (int)tot;
+    // the systems run concurrently on the stream pool and fill the GPU
+    // together, so each keeps few k-slices (fewer force partials to write
+    // and sum per system)
+    for (qem_handle *hh : b->h) qem_handle_set_long_max_ks(hh, 8);
     if (cudaSetDevice(b->device) != cudaSuccess) {
         delete b;
         return QEM_ERR_CUDA;

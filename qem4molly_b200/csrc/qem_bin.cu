@@ -706,7 +706,9 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 {
     if (N <= 0) return cudaSuccess;
     cudaError_t e;
-    if (g.ncx >= 3 && g.ncy >= 3) {
+    // one warp per owner cell pays off from about two particles per cell;
+    // sparser systems take one thread per owner.  Both give the same lists.
+    if (g.ncx >= 3 && g.ncy >= 3 && (int64_t)N >= 2 * (int64_t)ncell) {
         const int nb = nblk((int64_t)ncell * 32, 128);
         k_pairs_cell<false><<<nb, 128, 0, s>>>(ncell, pos_c, cell_start, cell_list, g, rc2, pcount, nullptr, nullptr,
                                                0, in_slot, nullptr, nullptr, nullptr);
@@ -717,8 +719,9 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
                                               in_slot, in_off, in_list, status);
         return cudaGetLastError();
     }
-    // fewer than 3 cells along x or y: one thread per owner over the full
-    // deduplicated stencil, incoming entries scattered with atomics and sorted
+    // one thread per owner (over the full deduplicated stencil when there are
+    // fewer than 3 cells along x or y), incoming entries scattered with
+    // atomics and sorted
     k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
                                                  nullptr, 0, nullptr, nullptr);
     if ((e = scan_impl<int, int64_t>(pcount, poff, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;

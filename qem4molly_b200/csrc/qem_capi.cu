@@ -138,6 +138,7 @@ struct qem_handle {
     // sharding of one system over ranks (qem_set_shard)
     int shard_rank = 0, shard_world = 1;
     uint64_t cfg_version = 0;  // bumped by k-set and shard changes
+    int long_max_ks = QEM_LONG_MAX_KS;  // cap on the k-slices of the long-range force pass
     uint64_t rng = 0x51ed5eedULL;
     std::vector<double> cdfx, cdfy;
     long mxmax = 0, mymax = 0;
@@ -507,8 +508,11 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     // energy partials: [short blocks | ks x long chunks | k0 blocks | P split terms]
     const int LCH = qem_long_chunk();
     const int nbS = (N + 255) / 256, nch = (N + LCH - 1) / LCH, nb0 = (N + 255) / 256;
-    const int ks = qem_long_ksplit(nch, 1 << 30, 8);
     const int P = do_long ? (h->has_kset ? h->P : 0) : 0;
+    // k-slices of the force pass, from the size of the whole k-set (or of the
+    // batch about to be drawn); small systems with many k-vectors get up to
+    // QEM_LONG_MAX_KS slices so that the pass still fills the GPU
+    const int ks = qem_long_ksplit(nch, std::max(h->has_kset ? h->P : h->p.rbe_p, 1), h->long_max_ks);
     const size_t nEpart = (size_t)nbS + (size_t)ks * nch + nb0 + std::max(P, h->p.rbe_p) + 8;
     CU(grow(h->Epart, sizeof(double) * nEpart));
     double *Ep = ptr<double>(h->Epart);
@@ -582,7 +586,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         if (rebuild) {
             const qem_status bs = build_pairs(h, N, st, s);
             if (bs != QEM_OK) return bs;
-            launches += h->geom.ncx >= 3 && h->geom.ncy >= 3 ? 15 : 16;
+            launches += h->geom.ncx >= 3 && h->geom.ncy >= 3 && N >= 2 * (int64_t)h->ncell ? 15 : 16;
         }
         h->short_calls++;
         mk_bin = h->prof.mark(s);
@@ -1257,7 +1261,7 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         const int Pk = h->has_kset ? h->P : 0;
         const int LCH = qem_long_chunk();
         const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;
-        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), 8);
+        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), h->long_max_ks);
         CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks * nch + nb0 + std::max(Pk, 1) + 8)));
         LongBuffers b;
         {
@@ -1359,6 +1363,13 @@ qem_status qem_forces_async(qem_handle *h, int N, const double *xyz, const doubl
 {
     bool retry = false;
     return run_once(h, N, xyz, q, F, nullptr, terms, QEM_MEM_DEVICE, s, retry, true);
+}
+
+void qem_handle_set_long_max_ks(qem_handle *h, int max_ks)
+{
+    if (!h || max_ks < 1) return;
+    h->long_max_ks = std::min(max_ks, QEM_LONG_MAX_KS);
+    h->cfg_version++;
 }
 
 qem_status qem_status_check(qem_handle *h, cudaStream_t s)

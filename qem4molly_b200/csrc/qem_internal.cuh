@@ -128,8 +128,11 @@ struct LongBuffers {
     int skip_k0 = 0;      // 1: leave out the k = 0 term (sharded ranks other than 0)
     const double *kwt = nullptr;  // P per-k weights (exact k-sum); nullptr: sum_K / P for every k
 };
-// number of k slices for nch chunks and P k-vectors (at most max_ks)
+// number of k slices for nch chunks and P k-vectors (at most max_ks); the
+// per-slice force partials take ks x N x 3 doubles, and ks x nch stays near
+// one wave of force-pass blocks, so they stay below ~15 MB at any N
 int qem_long_ksplit(int nch, int P, int max_ks);
+constexpr int QEM_LONG_MAX_KS = 64;
 // stage 0: z-ordered gather, k = 0 term, per-k constants, chunk totals and
 // their scan; stage 1: the k-sliced force pass, added into F3.
 cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const double4 *pos, const int *zperm,
@@ -146,6 +149,8 @@ qem_status qem_forces_async(qem_handle *h, int N, const double *xyz, const doubl
 // synchronises s, reads and clears the handle's device status word
 qem_status qem_status_check(qem_handle *h, cudaStream_t s);
 const qem_params *qem_handle_params(const qem_handle *h);
+// caps the k-slices of the handle's long-range force pass (1 .. QEM_LONG_MAX_KS)
+void qem_handle_set_long_max_ks(qem_handle *h, int max_ks);
 const char *qem_handle_error(const qem_handle *h);
 
 // ---- adjoint (FP64) --------------------------------------------------------

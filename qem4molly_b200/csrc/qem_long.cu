@@ -1059,10 +1059,10 @@ static int sm_count()
 int qem_long_ksplit(int nch, int P, int max_ks)
 {
     // as many whole k-slices of the nch chunks as fit in one wave of resident
-    // force-pass blocks
+    // force-pass blocks, each slice with at least two k groups of LKB vectors
     int ks = sm_count() * LF_MINB / (nch > 0 ? nch : 1);
     ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
-    const int pm = P > LKB ? (P + LKB - 1) / LKB : 1;  // at most one slice per k group
+    const int pm = P > 2 * LKB ? P / (2 * LKB) : 1;
     return ks < pm ? ks : pm;
 }
 

@@ -48,8 +48,11 @@ def kset_of(e):
 
 # ---------------------------------------------------------------- integer work
 @pytest.mark.parametrize("Lb,rc", [((100.0, 100.0, 10.0), 10.0), ((25.0, 25.0, 10.0), 10.0),
-                                   ((33.0, 47.0, 5.0), 10.0), ((200.0, 90.0, 10.0), 7.5)])
+                                   ((33.0, 47.0, 5.0), 10.0), ((200.0, 90.0, 10.0), 7.5),
+                                   ((1000.0, 1000.0, 10.0), 10.0)])
 def test_pair_list_bitexact(Lb, rc):
+    """Pair set equal to the brute-force oracle's: dense boxes (one warp per owner cell),
+    a box with 2 cells along an axis (full stencil) and a sparse box (one thread per owner)."""
     xyz, _ = slab(3000, Lb, 11)
     xyz[:7, :2] -= np.array([Lb[0], 0.0])  # some coordinates outside [0, L): wrapped by the binning
     e = Engine(L_box=Lb, alpha=0.1, r_cutoff=rc, rbe_p=0)
