@@ -372,6 +372,16 @@ def run_batch(args):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    # the same MD with the Andersen thermostat on (kT = 1, nu = 10: p = 0.01 per step)
+    K_a = max(3, min(args.steps, 200))
+    b.set_thermostat(1.0, 10.0, 7)
+    b.md(1, dt, x, v, q, F)  # records the thermostatted step
+    torch.cuda.synchronize()
+    e0.record()
+    b.md(K_a, dt, x, v, q, F)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_a = max_over_ranks(e0.elapsed_time(e1), world, dev)
     barrier(world)
     if rank == 0:
         n_sys = len(cfgs) * world
@@ -384,7 +394,10 @@ def run_batch(args):
                           "systems": n_sys, "particles_per_gpu": int(sum(N)), "pool_width": width,
                           "l2": "working set (< 100 MB) stays in L2 between steps; not flushed"},
                "batch_forces_graph_ms": ms_eval, "eager_per_system_forces_ms": eager_ms,
-               "particle_steps_per_s": args.steps * sum(N) * world * 1000.0 / ms, "clocks": clocks}
+               "particle_steps_per_s": args.steps * sum(N) * world * 1000.0 / ms,
+               "andersen": {"kT": 1.0, "nu": 10.0, "steps": K_a, "ms_per_step": ms_a / K_a,
+                            "value": K_a * 1000.0 / ms_a, "unit": "steps/s"},
+               "clocks": clocks}
         print(json.dumps(out), flush=True)
 
 # ----------------------------------------------------------------------------- exact k-sum workload

@@ -281,7 +281,17 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  *   step and each system keeps its current k-set for the whole run.
  * qem_batch_autotune: times the graph-replayed force evaluation for stream
  *   pool widths 1, 2, 4, ... up to min(B, 128) and keeps the fastest;
- *   returns the width and its time per batch evaluation (ms). */
+ *   returns the width and its time per batch evaluation (ms).
+ * qem_batch_set_thermostat: the Andersen thermostat of the MD steps (Molly's
+ *   AndersenThermostat(temp, coupling_const) in test/QEM_test.jl:53-56;
+ *   python_lib Andersen.py:8-22): after each step every particle, with
+ *   probability min(1, nu dt) (nu = 1 / coupling_const), takes a new velocity
+ *   with N(0, kT) components (unit masses).  nu = 0 or kT = 0 switches it
+ *   off.  The draws are a counter-based function of (seed, step, particle):
+ *   u_k = (SplitMix64-finalised seed, step, particle, k) >> 11, u in (0, 1];
+ *   collision if u_0 <= p; Box-Muller on (u_1, u_2) and (u_3, u_4) for x, y
+ *   and z.  The call resets the step counter (synchronising the device);
+ *   qem_batch_thermostat_step reads it (steps taken since). */
 typedef struct qem_batch qem_batch;
 qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t *N, qem_batch **out);
 void qem_batch_destroy(qem_batch *b);
@@ -293,6 +303,8 @@ qem_status qem_batch_md(qem_batch *b, int32_t nsteps, double dt, double *xyz, do
                         uint32_t terms, void *stream);
 qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
                               void *stream, int32_t *width, double *ms_per_eval);
+qem_status qem_batch_set_thermostat(qem_batch *b, double kT, double nu, uint64_t seed);
+qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step);
 
 /* Library identity (version string and the compiled CUDA architecture). */
 const char *qem_version(void);

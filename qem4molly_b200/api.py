@@ -397,6 +397,17 @@ class Batch:
         self._check(self._lib.qem_batch_md(self._b, int(nsteps), float(dt), self._ptr(xyz), self._ptr(v),
                                            self._ptr(q), self._ptr(F), int(terms), self._stream(xyz, stream)))
 
+    def set_thermostat(self, kT, nu, seed=0):
+        """Andersen thermostat of the MD steps (Molly AndersenThermostat(temp, coupling_const),
+        nu = 1 / coupling_const; unit masses); kT = 0 or nu = 0 switches it off."""
+        self._check(self._lib.qem_batch_set_thermostat(self._b, float(kT), float(nu), int(seed) & (2**64 - 1)))
+
+    def thermostat_step(self):
+        """Number of thermostatted steps since the last set_thermostat."""
+        n = C.c_uint64()
+        self._check(self._lib.qem_batch_thermostat_step(self._b, C.byref(n)))
+        return n.value
+
     def autotune(self, xyz, q, F, terms=L.QEM_TERM_ALL, stream=None):
         """Chooses the stream-pool width; returns (width, ms per batch evaluation)."""
         w = C.c_int32()

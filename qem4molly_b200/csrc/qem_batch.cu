@@ -10,6 +10,7 @@
 // pipelines concurrently and from replaying one recorded graph per MD step
 // instead of issuing some forty launches per system from the host.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -43,6 +44,50 @@ __global__ void k_vv_kick(int n3, double *__restrict__ v, double *__restrict__ F
     F[i] = fn;
 }
 
+// Andersen thermostat (Molly AndersenThermostat(temp, coupling_const), used by
+// test/QEM_test.jl:53-56; python_lib Andersen.py:8-22): after each step every
+// particle, with probability p = dt / coupling_const, takes a fresh velocity
+// with N(0, sigma^2) components, sigma^2 = kT / m (unit masses here).  Random
+// numbers come from a counter-based generator: the SplitMix64 finaliser
+// (Steele, Lea and Flood, OOPSLA 2014; Vigna's constants) of
+// seed + golden-ratio increments of (step, particle, draw), so every draw is
+// a pure function of (seed, step, i, draw) and a replayed graph draws new
+// numbers through the step counter in device memory.
+__host__ __device__ inline uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+__host__ __device__ inline uint64_t draw64(uint64_t seed, uint64_t step, uint64_t i, uint64_t k)
+{
+    const uint64_t G = 0x9e3779b97f4a7c15ULL;
+    return mix64(mix64(mix64(seed + G * (step + 1)) + G * (i + 1)) + G * (k + 1));
+}
+// uniform in (0, 1]: 53 random bits
+__device__ inline double unit53(uint64_t r) { return ((double)(r >> 11) + 1.0) * 0x1.0p-53; }
+
+__global__ void k_andersen(int n, double *__restrict__ v, double p, double sigma, uint64_t seed,
+                           const unsigned long long *__restrict__ step)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t st = *step;
+    if (unit53(draw64(seed, st, i, 0)) > p) return;  // no collision (P(u <= p) = p)
+    // Box-Muller: two uniforms -> two normals; three components from two pairs
+    const double u1 = unit53(draw64(seed, st, i, 1)), u2 = unit53(draw64(seed, st, i, 2));
+    const double u3 = unit53(draw64(seed, st, i, 3)), u4 = unit53(draw64(seed, st, i, 4));
+    const double r1 = sigma * sqrt(-2.0 * log(u1)), r2 = sigma * sqrt(-2.0 * log(u3));
+    double s1, c1, s2, c2;
+    sincospi(2.0 * u2, &s1, &c1);
+    sincospi(2.0 * u4, &s2, &c2);
+    v[3 * i] = r1 * c1;
+    v[3 * i + 1] = r1 * s1;
+    v[3 * i + 2] = r2 * c2;
+}
+
+__global__ void k_step_inc(unsigned long long *step) { *step += 1; }
+
 }  // namespace
 
 struct qem_batch {
@@ -64,6 +109,10 @@ struct qem_batch {
     double md_dt = 0;
     uint32_t md_terms = 0;
     int md_W = 0;
+    // Andersen thermostat of the MD steps (off while therm_nu == 0)
+    double therm_kT = 0, therm_nu = 0;
+    uint64_t therm_seed = 0;
+    unsigned long long *therm_step = nullptr;  // device step counter of the random draws
     std::string err;
 };
 
@@ -185,6 +234,7 @@ void qem_batch_destroy(qem_batch *b)
     if (b->sys) cudaFree(b->sys);
     if (b->box) cudaFree(b->box);
     if (b->Fn) cudaFree(b->Fn);
+    if (b->therm_step) cudaFree(b->therm_step);
     delete b;
 }
 
@@ -250,6 +300,11 @@ qem_status qem_batch_md(qem_batch *b, int32_t nsteps, double dt, double *xyz, do
         k_vv_drift<<<(n + T - 1) / T, T, 0, c>>>(n, xyz, v, F, dt, b->sys, b->box);
         st = enqueue_forces(b, xyz, q, b->Fn, terms, c);
         k_vv_kick<<<(3 * n + T - 1) / T, T, 0, c>>>(3 * n, v, F, b->Fn, dt);
+        if (b->therm_nu > 0) {
+            k_andersen<<<(n + T - 1) / T, T, 0, c>>>(n, v, std::min(1.0, b->therm_nu * dt), sqrt(b->therm_kT),
+                                                     b->therm_seed, b->therm_step);
+            k_step_inc<<<1, 1, 0, c>>>(b->therm_step);
+        }
         const cudaError_t ec = cudaStreamEndCapture(c, &g);
         if (st != QEM_OK) {
             if (g) cudaGraphDestroy(g);
@@ -269,6 +324,37 @@ qem_status qem_batch_md(qem_batch *b, int32_t nsteps, double dt, double *xyz, do
     }
     for (int k = 0; k < nsteps; k++) BCU(cudaGraphLaunch(b->md_exec, s));
     return qem_batch_check(b, stream);
+}
+
+qem_status qem_batch_set_thermostat(qem_batch *b, double kT, double nu, uint64_t seed)
+{
+    if (!b) return QEM_ERR_ARG;
+    if (!(kT >= 0) || !(nu >= 0) || !std::isfinite(kT) || !std::isfinite(nu))
+        return bfail(b, QEM_ERR_ARG, "thermostat: kT and nu must be finite and >= 0");
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaDeviceSynchronize());  // no recorded MD step may still be using the counter
+    if (!b->therm_step) BCU(cudaMalloc(&b->therm_step, sizeof(unsigned long long)));
+    BCU(cudaMemset(b->therm_step, 0, sizeof(unsigned long long)));
+    BCU(cudaDeviceSynchronize());
+    b->therm_kT = kT;
+    b->therm_nu = kT > 0 ? nu : 0;
+    b->therm_seed = seed;
+    drop_md_graph(b);
+    b->err.clear();
+    return QEM_OK;
+}
+
+qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step)
+{
+    if (!b || !step) return QEM_ERR_ARG;
+    *step = 0;
+    if (!b->therm_step) return QEM_OK;
+    unsigned long long v = 0;
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaMemcpy(&v, b->therm_step, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return QEM_ERR_CUDA;
+    *step = v;
+    return QEM_OK;
 }
 
 qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
