@@ -72,6 +72,11 @@ typedef int32_t qem_status;
                                     (QEM_short.jl:32-36); default rebuilds every call             */
 #define QEM_RESAMPLE_KSET 0x10u  /* draw a fresh random batch of k-vectors on every long-range
                                     call (Force_long.jl:235); default reuses the current batch    */
+#define QEM_EQUAL_Z_TIES 0x20u   /* particles of equal z are neither below nor above each other in
+                                    the z-ordered long-range sums (python_lib equal_cell,
+                                    Sigma_Gamma_func_njit.py:168-281); default: sortperm(z) order,
+                                    ties by index (QEM_long.jl:39-40).  Costs a second long-range
+                                    pass (the mean over both tie orders)                          */
 #define QEM_PYTHON_MODE (QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL)
 
 /* precision */

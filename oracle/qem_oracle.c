@@ -36,6 +36,10 @@
  *   dir_mode 1: minimum-image direction (neighbor_check.py:28-38)
  *   pair_mode 0: F[j] -= F_ij (QEM_short.jl:46-47)
  *   pair_mode 1: F[j] += F_short_ij(j, i)  (full-list python_lib semantics)
+ *   z_ties 0: the z-ordered sums follow sortperm(z) (stable; tied particles
+ *             are ordered by index, QEM_long.jl:39-40)
+ *   z_ties 1: tied particles are neither below nor above each other
+ *             (python_lib equal_cell, Sigma_Gamma_func_njit.py:168-281)
  */
 #include <math.h>
 #include <stdint.h>
@@ -56,6 +60,8 @@ typedef struct {
     int cutoff_mode;
     int dir_mode;
     int pair_mode;
+    int z_ties; /* 1: equal-z particles are neither below nor above each other in the z-ordered
+                   sums (python_lib equal_cell, Sigma_Gamma_func_njit.py:168-281) */
 } qo_params;
 
 typedef struct {
@@ -601,6 +607,77 @@ void qo_Flz_sort_k0(int N, const int *zlist, const double *q, double *out)
     free(Q1);
 }
 
+/* Equal-z groups of the z order: g0[i], g1[i] = first and one-past-last sorted
+ * position of the group of sorted position i (a new group starts where z
+ * strictly increases, as the equal_cell construction of
+ * Force_long_range_njit_exact.py:130-156). */
+static void z_groups(int N, const int *zlist, const double *xyz, int *g0, int *g1)
+{
+    int s = 0;
+    for (int i = 1; i <= N; i++)
+        if (i == N || xyz[3 * zlist[i] + 2] > xyz[3 * zlist[i - 1] + 2]) {
+            for (int t = s; t < i; t++) {
+                g0[t] = s;
+                g1[t] = i;
+            }
+            s = i;
+        }
+}
+
+/* Fl_sort with equal-z groups (Sigma_Gamma_func_njit.py:168-238): the x / y
+ * parts as Fl_sort (F_long_xy_sum_2 takes the plain order), the z part with
+ * sums over strictly lower (A, B) and strictly higher (C, D) groups. */
+void qo_Fl_sort_ties(const double *kset, int N, const int *zlist, const double *xyz, const double *q, double *out,
+                     int nthreads)
+{
+    qo_Fl_sort(kset, N, zlist, xyz, q, out, nthreads);
+    if (N == 0) return;
+    double kx = kset[0], ky = kset[1], k = kset[2];
+    double *PA = calloc(4 * (size_t)(N + 1), sizeof(double)), *PB = PA + N + 1, *SC = PB + N + 1, *SD = SC + N + 1;
+    int *g0 = malloc(sizeof(int) * 2 * (size_t)N), *g1 = g0 + N;
+    z_groups(N, zlist, xyz, g0, g1);
+    for (int i = 0; i < N; i++) { /* PA[i] = sum over sorted positions < i */
+        int l = zlist[i];
+        double x = xyz[3 * l], y = xyz[3 * l + 1], z = xyz[3 * l + 2];
+        PA[i + 1] = PA[i] + q[l] * exp(+k * z) * cos(kx * x + ky * y);
+        PB[i + 1] = PB[i] + q[l] * exp(+k * z) * sin(kx * x + ky * y);
+    }
+    for (int i = N - 1; i >= 0; i--) { /* SC[i] = sum over sorted positions >= i */
+        int l = zlist[i];
+        double x = xyz[3 * l], y = xyz[3 * l + 1], z = xyz[3 * l + 2];
+        SC[i] = SC[i + 1] + q[l] * exp(-k * z) * cos(kx * x + ky * y);
+        SD[i] = SD[i + 1] + q[l] * exp(-k * z) * sin(kx * x + ky * y);
+    }
+    for (int i = 0; i < N; i++) {
+        int l = zlist[i];
+        double qi = q[l], x = xyz[3 * l], y = xyz[3 * l + 1], z = xyz[3 * l + 2];
+        double c = cos(kx * x + ky * y), s = sin(kx * x + ky * y);
+        double A = PA[g0[i]], B = PB[g0[i]], Cs = SC[g1[i]], D = SD[g1[i]];
+        out[3 * l + 2] = (qi / 2) * (c * exp(-k * z) * A + s * exp(-k * z) * B - c * exp(k * z) * Cs -
+                                     s * exp(k * z) * D);
+    }
+    free(g0);
+    free(PA);
+}
+
+/* Flz_sort_k0 with equal-z groups (Sigma_Gamma_func_njit.py:240-281) */
+void qo_Flz_sort_k0_ties(int N, const int *zlist, const double *xyz, const double *q, double *out)
+{
+    memset(out, 0, sizeof(double) * 3 * (size_t)N);
+    if (N == 0) return;
+    double *P = calloc((size_t)N + 1, sizeof(double)), tot = 0;
+    int *g0 = malloc(sizeof(int) * 2 * (size_t)N), *g1 = g0 + N;
+    z_groups(N, zlist, xyz, g0, g1);
+    for (int i = 0; i < N; i++) P[i + 1] = P[i] + q[zlist[i]];
+    tot = P[N];
+    for (int i = 0; i < N; i++) {
+        int l = zlist[i];
+        out[3 * l + 2] = q[l] * (P[g0[i]] - (tot - P[g1[i]]));
+    }
+    free(g0);
+    free(P);
+}
+
 /* Force_long.jl:164-184 (z only) */
 void qo_Flz_self(const double *kset, int N, const double *xyz, const double *q, double g1, double g2, double Lz,
                  double *out)
@@ -621,7 +698,8 @@ void qo_F_l_total(const qo_params *p, const double *kset, int N, const double *x
 {
     double *a = malloc(sizeof(double) * 9 * (size_t)(N > 0 ? N : 1)), *b = a + 3 * N, *c = b + 3 * N;
     qo_Fl_non_sort(kset, N, xyz, q, p->gamma_1, p->gamma_2, p->Lz, a, nthreads);
-    qo_Fl_sort(kset, N, zlist, xyz, q, b, nthreads);
+    if (p->z_ties) qo_Fl_sort_ties(kset, N, zlist, xyz, q, b, nthreads);
+    else qo_Fl_sort(kset, N, zlist, xyz, q, b, nthreads);
     qo_Flz_self(kset, N, xyz, q, p->gamma_1, p->gamma_2, p->Lz, c);
     double den = p->Lx * p->Ly * p->eps_0;
     for (int t = 0; t < 3 * N; t++) out[t] = (a[t] + b[t] + c[t]) / den;
@@ -637,7 +715,8 @@ void qo_F_long(const qo_params *p, int N, const double *xyz, const double *q, co
     if (zlist_in) memcpy(zlist, zlist_in, sizeof(int) * N);
     else qo_sortperm_z(N, xyz, zlist);
     double *t = malloc(sizeof(double) * 3 * (size_t)(N > 0 ? N : 1));
-    qo_Flz_sort_k0(N, zlist, q, t);
+    if (p->z_ties) qo_Flz_sort_k0_ties(N, zlist, xyz, q, t);
+    else qo_Flz_sort_k0(N, zlist, q, t);
     double den0 = 2 * p->Lx * p->Ly * p->eps_0;
     for (int i = 0; i < 3 * N; i++) F[i] = 0 + t[i] / den0;
     double w = sum_K / P;
@@ -847,7 +926,8 @@ void qo_F_long_w(const qo_params *p, int N, const double *xyz, const double *q, 
     if (zlist_in) memcpy(zlist, zlist_in, sizeof(int) * N);
     else qo_sortperm_z(N, xyz, zlist);
     double *t = malloc(sizeof(double) * 3 * (size_t)(N > 0 ? N : 1));
-    qo_Flz_sort_k0(N, zlist, q, t);
+    if (p->z_ties) qo_Flz_sort_k0_ties(N, zlist, xyz, q, t);
+    else qo_Flz_sort_k0(N, zlist, q, t);
     double den0 = 2 * p->Lx * p->Ly * p->eps_0;
     for (int i = 0; i < 3 * N; i++) F[i] = 0 + t[i] / den0;
     for (int m = 0; m < P; m++) {

@@ -19,7 +19,7 @@ STATUS = {0: "QEM_OK", 1: "QEM_ERR_ARG", 2: "QEM_ERR_OUT_OF_SLAB", 3: "QEM_ERR_N
           4: "QEM_ERR_NB_OVERFLOW", 5: "QEM_ERR_TIMEOUT", 6: "QEM_ERR_CUDA", 7: "QEM_ERR_NO_KSET",
           8: "QEM_ERR_RANGE"}
 QEM_CUTOFF_PYTHON, QEM_DIR_MINIMAGE, QEM_PAIR_PHYSICAL = 0x1, 0x2, 0x4
-QEM_STALE_NEIGHBORS, QEM_RESAMPLE_KSET = 0x8, 0x10
+QEM_STALE_NEIGHBORS, QEM_RESAMPLE_KSET, QEM_EQUAL_Z_TIES = 0x8, 0x10, 0x20
 QEM_PYTHON_MODE = QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL
 QEM_FP64, QEM_FP32_FIX = 0, 1
 QEM_TERM_SHORT, QEM_TERM_LONG, QEM_TERM_LJ, QEM_TERM_ALL = 0x1, 0x2, 0x4, 0x7

@@ -554,15 +554,19 @@ __global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restric
 // ---------------------------------------------------------------------------
 // z order: bitonic sort of 1024-element tiles in shared memory, then merge
 // passes by co-ranking.  Keys are (z, index): a total order, so the result is
-// the stable ascending order of z.  Non-finite z was zeroed by k_pack.
+// the stable ascending order of z.  Non-finite z was zeroed by k_pack.  REV
+// orders equal z by descending index instead (the second order of the
+// equal-z tie mode).
 // ---------------------------------------------------------------------------
 constexpr int ZTILE = 1024;
 
+template <bool REV>
 __device__ __forceinline__ bool zless(double za, int ia, double zb, int ib)
 {
-    return (za < zb) || (za == zb && ia < ib);
+    return (za < zb) || (za == zb && (REV ? ia > ib : ia < ib));
 }
 
+template <bool REV>
 __global__ void k_ztile(int N, const double4 *__restrict__ pos, double *__restrict__ key, int *__restrict__ idx)
 {
     __shared__ double sk[ZTILE];
@@ -587,7 +591,7 @@ __global__ void k_ztile(int N, const double4 *__restrict__ pos, double *__restri
                 bool up = ((lo & size) == 0);
                 double ka = sk[lo], kb = sk[hi];
                 int ia = si[lo], ib = si[hi];
-                bool swap = up ? zless(kb, ib, ka, ia) : zless(ka, ia, kb, ib);
+                bool swap = up ? zless<REV>(kb, ib, ka, ia) : zless<REV>(ka, ia, kb, ib);
                 if (swap) {
                     sk[lo] = kb; sk[hi] = ka;
                     si[lo] = ib; si[hi] = ia;
@@ -605,6 +609,7 @@ __global__ void k_ztile(int N, const double4 *__restrict__ pos, double *__restri
     }
 }
 
+template <bool REV>
 __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
                          double *__restrict__ key_out, int *__restrict__ idx_out)
 {
@@ -622,7 +627,7 @@ __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const
         int lo = rstart, hi = rend;
         while (lo < hi) {
             int mid = (lo + hi) >> 1;
-            if (zless(key[mid], idx[mid], kz, ki)) lo = mid + 1;
+            if (zless<REV>(key[mid], idx[mid], kz, ki)) lo = mid + 1;
             else hi = mid;
         }
         pos_out = lstart + (p - lstart) + (lo - rstart);
@@ -630,7 +635,7 @@ __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const
         int lo = lstart, hi = lend;
         while (lo < hi) {
             int mid = (lo + hi) >> 1;
-            if (zless(key[mid], idx[mid], kz, ki)) lo = mid + 1;
+            if (zless<REV>(key[mid], idx[mid], kz, ki)) lo = mid + 1;
             else hi = mid;
         }
         pos_out = lstart + (p - rstart) + (lo - lstart);
@@ -736,15 +741,17 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 }
 
 cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
-                             cudaStream_t s)
+                             cudaStream_t s, bool rev_ties)
 {
     if (N <= 0) return cudaSuccess;
-    k_ztile<<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
+    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
+    else k_ztile<false><<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
     double *ka = zkey, *kb = zkey_tmp;
     int *ia = zperm, *ib = ztmp;
     int passes = 0;
     for (int w = ZTILE; w < N; w <<= 1) {
-        k_zmerge<<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
+        if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
+        else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
         double *tk = ka; ka = kb; kb = tk;
         int *ti = ia; ia = ib; ib = ti;
         passes++;

@@ -156,7 +156,7 @@ struct qem_handle {
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
     // adjoint pass
-    DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart;
+    DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh;
     cudaStream_t s2 = nullptr;  // side stream of the long range
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     unsigned *h_status = nullptr;
@@ -248,7 +248,7 @@ static qem_status validate(const qem_params *p, std::string &why)
         }
     }
     const uint32_t known = QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL | QEM_STALE_NEIGHBORS |
-                           QEM_RESAMPLE_KSET;
+                           QEM_RESAMPLE_KSET | QEM_EQUAL_Z_TIES;
     if (p->mode_flags & ~known) { why = "unknown mode flag"; return QEM_ERR_ARG; }
     if (p->precision != QEM_FP64 && p->precision != QEM_FP32_FIX) { why = "precision must be QEM_FP64 or QEM_FP32_FIX"; return QEM_ERR_ARG; }
     for (int i = 0; i < 5; i++)
@@ -573,8 +573,24 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         mk_lprep = h->prof.mark(sl);
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 1));
-        mk_lforce = h->prof.mark(sl);
         launches += 22;
+        if (h->p.mode_flags & QEM_EQUAL_Z_TIES) {
+            // Equal-z ties: a tied pair counts once as below and once as above
+            // in the two orders (z, index up) and (z, index down), and every
+            // other part of the long range is the same in both, so the mean of
+            // the two evaluations is the force with tied particles neither
+            // below nor above each other.  The energy does not depend on the
+            // order of ties and comes from the first pass.
+            CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
+                                ptr<double>(h->zkey), ptr<double>(h->zkey2), sl, true));
+            for (int stage = 0; stage < 2; stage++)
+                CU(qem_launch_long(prec, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
+                                   h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch,
+                                   st, sl, stage));
+            CU(qem_launch_scale(3 * N, 0.5, FL, FL, sl));
+            launches += 23;
+        }
+        mk_lforce = h->prof.mark(sl);
         h->counts[2] = Pk;
     }
 
@@ -887,7 +903,7 @@ void qem_destroy(qem_handle *h)
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
-                      &h->lam, &h->ggk, &h->Gpart};
+                      &h->lam, &h->ggk, &h->Gpart, &h->gFh};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -1197,6 +1213,7 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
                                 cudaStream_t s, bool &retry)
 {
     retry = false;
+    bool ties_adj = false;  // long-range gamma gradient of the second tie order in gout[4 .. 6)
     const bool do_short = terms & QEM_TERM_SHORT;
     const bool do_long = terms & QEM_TERM_LONG;
     const bool do_lj = (terms & QEM_TERM_LJ) && h->p.n_walls > 0;
@@ -1298,11 +1315,32 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         a.w1 = ptr<double>(h->w1); a.w2 = ptr<double>(h->w2); a.s1 = ptr<double>(h->ws1); a.s2 = ptr<double>(h->ws2);
         a.atot = ptr<double>(h->atot); a.aoff = ptr<double>(h->aoff); a.lam = ptr<double>(h->lam);
         a.ggk = ptr<double>(h->ggk); a.Gpart = ptr<double>(h->Gpart); a.gam = gout + 2;
-        CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
-                               h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch, ks, s));
+        if (!(h->p.mode_flags & QEM_EQUAL_Z_TIES)) {
+            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                   h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch, ks, s));
+        } else {
+            // the forward force is the mean over the two tie orders, so the
+            // adjoint is the sum of both orders' adjoints of (gF / 2, gE / 2);
+            // the second order's gamma gradient goes to gout[4 .. 6)
+            CU(grow(h->gFh, sizeof(double) * 3 * N));
+            double *gFh = ptr<double>(h->gFh);
+            if (gF_d) CU(qem_launch_scale(3 * N, 0.5, gF_d, gFh, s));
+            else CU(cudaMemsetAsync(gFh, 0, sizeof(double) * 3 * N, s));
+            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                   h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
+            CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
+                                ptr<double>(h->zkey), ptr<double>(h->zkey2), s, true));
+            CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
+                               h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch,
+                               st, s, 0));
+            a.gam = gout + 4;
+            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                   h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
+            ties_adj = true;
+        }
     }
-    double hg[4] = {0, 0, 0, 0};
-    CU(cudaMemcpyAsync(hg, gout, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    double hg[6] = {0, 0, 0, 0, 0, 0};
+    CU(cudaMemcpyAsync(hg, gout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
     if (mem == QEM_MEM_HOST) {
         CU(cudaMemcpyAsync(gxyz, gx_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
         if (gq) CU(cudaMemcpyAsync(gq, gq_d, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
@@ -1325,8 +1363,8 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
     if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
     if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
     if (ggamma) {
-        ggamma[0] = hg[0] + hg[2];
-        ggamma[1] = hg[1] + hg[3];
+        ggamma[0] = hg[0] + (ties_adj ? hg[2] + hg[4] : hg[2]);
+        ggamma[1] = hg[1] + (ties_adj ? hg[3] + hg[5] : hg[3]);
     }
     h->err.clear();
     return QEM_OK;

@@ -102,8 +102,11 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s);
 
+// stable z order (equal z by ascending index; by descending index with rev_ties)
 cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
-                             cudaStream_t s);
+                             cudaStream_t s, bool rev_ties = false);
+// y = a x (y may be x)
+cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s);
 struct LongBuffers {
     double *zx, *zy;      // z-ordered in-plane coordinates (FP64, phases)
     float *zhf;           // z - Lz/2 (FP32 path)

@@ -1125,6 +1125,19 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     return cudaGetLastError();
 }
 
+__global__ void k_scale_vec(int n, double a, const double *x, double *y)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = a * x[i];
+}
+
+cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_scale_vec<<<nblk(n, 256), 256, 0, s>>>(n, a, x, y);
+    return cudaGetLastError();
+}
+
 cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s)
 {
     if (n <= 0) return cudaSuccess;

@@ -149,18 +149,33 @@ def main(argv=None):
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--precision", default="fp32", choices=("fp32", "fp64"))
     ap.add_argument("--N", type=int, default=None, help="particle count (configs 2, 3, 5)")
+    ap.add_argument("--ties", type=float, default=0.0,
+                    help="round z to multiples of this spacing and evaluate with QEM_EQUAL_Z_TIES")
     a = ap.parse_args(argv)
+    from . import _lib as L
+
     make = {1: config1, 2: config2, 3: config3, 5: config5}[a.config]
     cfg = make(N=a.N) if (a.N and a.config != 1) else make()
-    e = engine_for(cfg, a.precision)
+    if a.ties > 0:
+        cfg["xyz"][:, 2] = np.round(cfg["xyz"][:, 2] / a.ties) * a.ties
+    e = engine_for(cfg, a.precision, mode_flags=L.QEM_EQUAL_Z_TIES if a.ties > 0 else 0)
     dev = torch.device("cuda", 0)
     x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
     q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
     F = torch.empty_like(x)
-    for _ in range(a.evals):
+    for _ in range(3):
         e.forces_device(x, q, F)
     torch.cuda.synchronize()
-    print(f"config {a.config}: N={len(cfg['q'])}, {a.evals} {a.precision} evaluations, |F|_max={F.abs().max().item():.6e}")
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(a.evals):
+        e.forces_device(x, q, F)
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / max(a.evals, 1)
+    print(f"config {a.config}: N={len(cfg['q'])}, {a.evals} {a.precision} evaluations "
+          f"{'with equal-z ties ' if a.ties > 0 else ''}(back to back, {ms:.3f} ms each), "
+          f"|F|_max={F.abs().max().item():.6e}")
 
 
 if __name__ == "__main__":

@@ -26,6 +26,8 @@ What is generated (each case states the reference file it exercises):
   accurate-Bessel shim, so the python-convention oracle mode is pinned to
   ~1e-12.
 * ``icm_energy.json``  -- ICM.U_cal / ICM.F_cal on a 3-particle slab.
+* ``long_ties.json``   -- equal-z ties: a 36-particle slab on 5 z levels
+  through the z-ordered sums with their equal_cell groups (fixed k-set).
 * ``long_exact.json``  -- the exact (non-random-batch) long range of
   Force_long_range_njit_exact.Force_long_cal on a 24-particle slab, with every
   lattice vector up to the cutoff (k-sorted rows, so its k <= k_f1 loop takes
@@ -302,6 +304,60 @@ def gen_exact(rng):
                 F_long=np.stack([Fx, Fy, Fz + Fzs], 1).tolist())
 
 
+def gen_ties(rng):
+    """Equal-z ties: a 36-particle slab on 5 z levels through the python_lib z-ordered sums
+    with their equal_cell groups (Sigma_Gamma_func_njit.F_long_z_sum_2), assembled for a fixed
+    k-set as Force_long_range_njit.Force_long_cal does; also the k = 0 energy."""
+    import numpy as np
+
+    import Energy_long_range_njit as El
+    import Sigma_Gamma_func_njit as S
+
+    N, Lx, Ly, Lz = 36, 18.0, 15.0, 4.0
+    g1, g2 = -0.5, 0.7  # gamma_down, gamma_up
+    e1 = (1 - g1) / (1 + g1)
+    e3 = (1 - g2) / (1 + g2)
+    q = rng.uniform(0.5, 1.5, N) * np.where(np.arange(N) % 2 == 0, 1.0, -1.0)
+    q[-1] -= q.sum()
+    x = rng.random(N) * Lx
+    y = rng.random(N) * Ly
+    z = rng.choice(np.array([0.5, 1.25, 2.0, 2.75, 3.5]), N)
+    POSCAR = np.stack([q, x, y, z], axis=1)
+    zl = np.argsort(z, kind="stable")
+    levels = [zl[z[zl] == v] for v in np.unique(z)]
+    G = len(levels)
+    eq_cell = np.full([G, max(len(m) for m in levels)], 9999)
+    for g, m in enumerate(levels):
+        eq_cell[g, :len(m)] = m
+    eq_size = np.cumsum([len(m) for m in levels])
+    P = 10
+    mx = rng.integers(-3, 4, P)
+    my = rng.integers(-3, 4, P)
+    for t in range(P):
+        if mx[t] == 0 and my[t] == 0:
+            my[t] = 2
+    kset = np.stack([2 * np.pi * mx / Lx, 2 * np.pi * my / Ly], axis=1)
+    S_tot = 2.3
+    FL = np.zeros((N, 3))
+    for t in range(P):
+        kx, ky = kset[t]
+        K = kx * kx + ky * ky
+        k4 = np.array([kx, ky, K, np.sqrt(K)])
+        a1 = S.F_long_sum_1(k4, e1, 1.0, e3, POSCAR, Lz)
+        a2 = S.F_long_xy_sum_2(k4, POSCAR, zl)
+        z0, z2 = S.F_long_z_sum_2(k4, POSCAR, zl, eq_cell, eq_size, G)
+        zs = S.F_long_z_self_sum(k4, POSCAR, e1, 1.0, e3, Lz)
+        w = (1 / (Lx * Ly)) * (S_tot / P)
+        FL[:, 0] += w * (a1[0] + a2[0])
+        FL[:, 1] += w * (a1[1] + a2[1])
+        FL[:, 2] += w * (a1[2] - z2 + zs)
+    FL[:, 2] += (1 / (2 * Lx * Ly)) * z0
+    E_k0 = El.Energy_long_kzero(POSCAR, P, P, kset, Lx, Ly, Lz, 1.0, e1, 1.0, e3, S_tot, zl, eq_cell, eq_size, G)
+    return dict(source="Sigma_Gamma_func_njit.py:8-304 with equal_cell groups, Energy_long_range_njit.py:25-44",
+                N=N, L=[Lx, Ly, Lz], gamma_1=g1, gamma_2=g2, q=q.tolist(), xyz=np.stack([x, y, z], 1).tolist(),
+                kset=kset.tolist(), sum_K=S_tot, F_long=FL.tolist(), E_long_k0=E_k0, n_levels=G)
+
+
 def gen_icm(rng):
     import numpy as np
 
@@ -364,6 +420,7 @@ def run_variant(bessel):
                    cases=gen_short_pair(np.random.default_rng(20261206), "accurate")))
         _dump("system_python.json", gen_system(np.random.default_rng(20261207)))
         _dump("long_exact.json", gen_exact(np.random.default_rng(20261208)))
+        _dump("long_ties.json", gen_ties(np.random.default_rng(20261209)))
 
 
 if __name__ == "__main__":

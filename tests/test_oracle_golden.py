@@ -193,6 +193,26 @@ def test_exact_long_range_vs_python_exact():
                       O.energy_long(p, xyz, q, k3[sel], 2.5), rtol=1e-14)
 
 
+def test_equal_z_ties_vs_python_equal_cell():
+    """Particles on 5 z levels (long_ties.json): with z_ties the oracle's z-ordered sums count
+    equal-z particles as neither below nor above (python_lib equal_cell); the plain sortperm
+    order differs in F_z only, and the k = 0 energy does not depend on it."""
+    d = load("long_ties.json")
+    xyz, q = np.array(d["xyz"]), np.array(d["q"])
+    ks = np.array(d["kset"])
+    k3 = np.concatenate([ks, np.hypot(ks[:, 0], ks[:, 1])[:, None]], 1)
+    Fr = np.array(d["F_long"])
+    zl = np.argsort(xyz[:, 2], kind="stable").astype(np.int32)
+    p = O.params(d["L"], 1.0, 1.0, d["gamma_1"], d["gamma_2"], z_ties=1)
+    F = O.F_long(p, xyz, q, k3, d["sum_K"])
+    assert np.abs(F - Fr).max() <= 1e-12 * np.abs(Fr).max()
+    assert np.isclose(O.energy_k0(p, xyz, q, zl), d["E_long_k0"], rtol=1e-13)
+    p0 = O.params(d["L"], 1.0, 1.0, d["gamma_1"], d["gamma_2"])
+    F0 = O.F_long(p0, xyz, q, k3, d["sum_K"])
+    assert np.abs(F0[:, :2] - Fr[:, :2]).max() <= 1e-12 * np.abs(Fr).max()
+    assert np.abs(F0[:, 2] - Fr[:, 2]).max() > 0.05 * np.abs(Fr).max()
+
+
 def test_sortperm_is_stable():
     """QEM_long.jl:39-40 sortperm: stable ascending, ties keep index order."""
     rng = np.random.default_rng(3)
