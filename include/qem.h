@@ -120,8 +120,28 @@ typedef struct {
     uint32_t mode_flags;/* QEM_CUTOFF_PYTHON | ...                                      */
     int32_t precision;  /* QEM_FP64 or QEM_FP32_FIX                                     */
     int32_t device;     /* CUDA device ordinal                                          */
-    int32_t reserved[5];/* must be zero                                                 */
+    int32_t reserved0;  /* must be zero                                                 */
+    double pv_eps;      /* gamma_up * gamma_down > 1 only: half-width of the window around
+                           the pole k_0 = ln(gamma_up gamma_down) / (2 Lz) of the
+                           regularised short-range quadrature (python_lib INCAR['eps']) */
+    int32_t reserved[2];/* must be zero                                                 */
 } qem_params;
+
+/* gamma_up * gamma_down > 1 (metamaterial substrates; python_lib
+ * Force_short_norm_njit.py, green_norm_njit.py, Force_short_range_njit.py:
+ * 258-286, 311-314): 1 / (g12 e^{-2 k Lz} - 1) has a pole at k_0, and each
+ * short-range integral runs over [0, k_0 - e], [k_0 - e, k_0 + e],
+ * [k_0 + e, 2 k_0], [2 k_0, k_f] with N_1, 10, N_1, N_t - 2 N_1 nodes
+ * (N_1 = int(N_t k_0 / k_f), k_f = max(python limit, 2.1 k_0)), the window
+ * through the pole-free part of the denominator and the two sides with the
+ * pole term subtracted (principal value).  Needs QEM_FP64, QEM_CUTOFF_PYTHON
+ * (the reference defines it for the python_lib only), 0 < pv_eps < k_0 and
+ * N_1 >= 1 for both integral families; energies and the adjoint are not
+ * defined there (QEM_ERR_ARG).  Two details of the reference are kept: the
+ * window of the Gauss rho integrand has no exp(-k^2 / 4 alpha) factor
+ * (Force_short_norm_njit.py:59) and the self force adds the point integral
+ * with the opposite sign (Force_short_norm_njit.py:330-331).  The long range
+ * is unchanged (as in the python_lib). */
 
 typedef struct qem_handle qem_handle;
 

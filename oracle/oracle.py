@@ -33,7 +33,7 @@ class Params(C.Structure):
         ("gamma_1", C.c_double), ("gamma_2", C.c_double),
         ("eps_0", C.c_double), ("accuracy", C.c_double),
         ("N_t", C.c_int), ("cutoff_mode", C.c_int),
-        ("dir_mode", C.c_int), ("pair_mode", C.c_int), ("z_ties", C.c_int),
+        ("dir_mode", C.c_int), ("pair_mode", C.c_int), ("z_ties", C.c_int), ("pv_eps", C.c_double),
     ]
 
 
@@ -117,13 +117,13 @@ def _i(a):
 
 
 def params(L, alpha, r_cutoff, gamma_1=0.0, gamma_2=0.0, eps_0=1.0, accuracy=1e-6, N_t=30,
-           cutoff_mode=CUTOFF_JULIA, dir_mode=DIR_RAW, pair_mode=PAIR_JULIA, z_ties=0) -> Params:
+           cutoff_mode=CUTOFF_JULIA, dir_mode=DIR_RAW, pair_mode=PAIR_JULIA, z_ties=0, pv_eps=0.0) -> Params:
     """z_ties=1: equal-z particles are neither below nor above each other in the z-ordered sums
     (python_lib equal_cell, Sigma_Gamma_func_njit.py:168-281); 0: the plain sortperm order."""
     Lx, Ly, Lz = L
     return Params(float(Lx), float(Ly), float(Lz), float(alpha), float(r_cutoff), float(gamma_1),
                   float(gamma_2), float(eps_0), float(accuracy), int(N_t), int(cutoff_mode),
-                  int(dir_mode), int(pair_mode), int(z_ties))
+                  int(dir_mode), int(pair_mode), int(z_ties), float(pv_eps))
 
 
 def gauss_legendre(n):

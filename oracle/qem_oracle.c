@@ -62,6 +62,9 @@ typedef struct {
     int pair_mode;
     int z_ties; /* 1: equal-z particles are neither below nor above each other in the z-ordered
                    sums (python_lib equal_cell, Sigma_Gamma_func_njit.py:168-281) */
+    double pv_eps; /* gamma_1 gamma_2 > 1 (python cutoffs only): half-width of the window around
+                      the pole k_0 = ln(gamma_1 gamma_2) / (2 L_z) of the regularised quadrature
+                      (Force_short_norm_njit.py; INCAR['eps'] of Force_short_range_njit.py:301) */
 } qo_params;
 
 typedef struct {
@@ -206,10 +209,96 @@ static double integrand(int which, const qo_params *p, double k, const qo_elem *
     return 0;
 }
 
-/* Gaussian_int.jl:9-23 with region (0, K) */
+/* ------------------------------------------------------------------ */
+/* gamma_1 gamma_2 > 1: regularised quadrature (python_lib                */
+/* Force_short_norm_njit.py:11-414, green_norm_njit.py:6-35,              */
+/* Force_short_range_njit.py:258-286).  1 / (g12 e^{-2 k L_z} - 1) has a   */
+/* pole at k_0 = ln(g12) / (2 L_z); every integral runs over [0, k_0 - e], */
+/* [k_0 - e, k_0 + e], [k_0 + e, 2 k_0] and [2 k_0, k_f] with N_1, 10, N_1 */
+/* and N_t - 2 N_1 Gauss-Legendre nodes, N_1 = int(N_t k_0 / k_f), k_f =   */
+/* max(python limit, 2.1 k_0).  With f = up(k) / (g12 e^{-2kLz} - 1):      */
+/* inside the window f is up(k) gamma_norm(k) - up'(k_0) / (2 L_z)         */
+/* (gamma_norm: the pole-free part, by its series), up to 2 k_0 the pole   */
+/* term up(k_0) / (2 L_z (k - k_0)) is added (its principal value over     */
+/* [0, 2 k_0] is zero), beyond 2 k_0 f itself.                            */
+/* ------------------------------------------------------------------ */
+static int norm_active(const qo_params *p) { return p->gamma_1 * p->gamma_2 > 1; }
+
+/* green_norm_njit.py:13-33: u / d with ten series terms in x = 2 L_z (k - k_0) */
+static double gamma_norm(const qo_params *p, double k)
+{
+    double g12 = p->gamma_1 * p->gamma_2, k0 = log(g12) / (2 * p->Lz);
+    double x = 2 * p->Lz * (k - k0), u = 0.5, d = -1 + x / 2, u0 = 0.5, d0 = x / 2;
+    for (int i = 0; i < 10; i++) {
+        u0 = u0 * (-x) / (i + 3);
+        d0 = d0 * (-x) / (i + 3);
+        u += u0;
+        d += d0;
+    }
+    return u / d;
+}
+
+/* the integrand without its 1 / (g12 e^{-2kLz} - 1) factor */
+static double integrand_up(int which, const qo_params *p, double k, const qo_elem *e, int l)
+{
+    double g12 = p->gamma_1 * p->gamma_2;
+    switch (which) {
+    case F_SR_GAUSS: return k * green_u(k, e, l) * exp(-k * k / (4 * p->alpha)) * j1(k * e->rho);
+    case F_SR_POINT: return k * g12 * green_u(k, e, l) * exp(-2 * k * p->Lz) * j1(k * e->rho);
+    case F_SZ_GAUSS: return dz_green_u(k, e, l) * exp(-k * k / (4 * p->alpha)) * j0(k * e->rho);
+    case F_SZ_POINT: return g12 * dz_green_u(k, e, l) * exp(-2 * k * p->Lz) * j0(k * e->rho);
+    }
+    return 0;
+}
+
+/* number of nodes of the two outer sub-intervals below 2 k_0 for a family limit */
+int qo_norm_n1(const qo_params *p, int point)
+{
+    double g12 = p->gamma_1 * p->gamma_2, k0 = log(g12) / (2 * p->Lz);
+    double kf = point ? fmax(-log(p->accuracy) / (2 * p->Lz), 2.1 * k0) : fmax(sqrt(-4 * p->alpha * log(p->accuracy)), 2.1 * k0);
+    return (int)(p->N_t * k0 / kf);
+}
+
+static double gl_int_norm(int which, const qo_params *p, const qo_elem *e, int l)
+{
+    const int point = (which == F_SR_POINT || which == F_SZ_POINT);
+    double g12 = p->gamma_1 * p->gamma_2, k0 = log(g12) / (2 * p->Lz), ep = p->pv_eps;
+    double kf = point ? fmax(-log(p->accuracy) / (2 * p->Lz), 2.1 * k0) : fmax(sqrt(-4 * p->alpha * log(p->accuracy)), 2.1 * k0);
+    int n1 = (int)(p->N_t * k0 / kf), n3 = p->N_t - 2 * n1;
+    double k1 = k0 - 0.01 * ep, k2 = k0 + 0.01 * ep;
+    double df = (integrand_up(which, p, k2, e, l) - integrand_up(which, p, k1, e, l)) / (k2 - k1);
+    double up0 = integrand_up(which, p, k0, e, l);
+    double lo[4] = {0, k0 - ep, k0 + ep, 2 * k0}, hi[4] = {k0 - ep, k0 + ep, 2 * k0, kf};
+    int nn[4] = {n1, 10, n1, n3};
+    double s = 0, xn[256], wn[256];
+    for (int t = 0; t < 4; t++) {
+        if (nn[t] < 1) continue;
+        qo_gauss_legendre(nn[t], xn, wn);
+        double a = lo[t], b = hi[t];
+        for (int i = 0; i < nn[t]; i++) {
+            double k = 0.5 * (b - a) * xn[i] + 0.5 * (b + a), f;
+            if (fabs(k - k0) <= ep) {
+                /* the Gauss rho integrand of the window drops its e^{-k^2/4alpha} factor
+                   (Force_short_norm_njit.py:59; its df keeps it), reproduced */
+                double upk = which == F_SR_GAUSS ? k * green_u(k, e, l) * j1(k * e->rho)
+                                                 : integrand_up(which, p, k, e, l);
+                f = upk * gamma_norm(p, k) - df / (2 * p->Lz);
+            }
+            else if (k <= 2 * k0)
+                f = integrand_up(which, p, k, e, l) / (g12 * exp(-2 * k * p->Lz) - 1) + up0 / (2 * p->Lz * (k - k0));
+            else
+                f = integrand_up(which, p, k, e, l) / (g12 * exp(-2 * k * p->Lz) - 1);
+            s += 0.5 * (b - a) * (wn[i] * f);
+        }
+    }
+    return s;
+}
+
+/* Gaussian_int.jl:9-23 with region (0, K); the regularised form for g12 > 1 */
 static double gl_int(int which, const qo_params *p, const qo_elem *e, int l, double K,
                      const double *xn, const double *wn)
 {
+    if (norm_active(p) && which != U_GAUSS && which != U_POINT) return gl_int_norm(which, p, e, l);
     double s = 0;
     for (int i = 0; i < p->N_t; i++) {
         double x = K / 2 + K * xn[i] / 2;
@@ -317,7 +406,9 @@ double qo_F_short_i(const qo_params *p, double q_i, const double *ci, int single
     Fp2 *= 0.5;
     if (!single)
         for (int l = 1; l <= 4; l++) Fg += gl_int(F_SZ_GAUSS, p, &e, l, gauss_limit(p, &e, l - 1), xn, wn);
-    double Fszi = -Fp1 + Fp2 + Fg;
+    /* for g12 > 1 the self force adds the point integral with the opposite sign
+       (Force_short_norm_njit.py:330-331 against Force_short_range_njit.py:224), reproduced */
+    double Fszi = (norm_active(p) ? Fp1 : -Fp1) + Fp2 + Fg;
     return -q_i * q_i / (2 * QO_PI * p->eps_0) * Fszi;
 }
 

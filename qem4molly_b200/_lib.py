@@ -45,7 +45,7 @@ class Params(C.Structure):
                 ("eps_0", C.c_double), ("accuracy", C.c_double), ("N_t", C.c_int32), ("rbe_p", C.c_int32),
                 ("iter_period", C.c_int32), ("n_walls", C.c_int32), ("walls", LJWall * 2),
                 ("mode_flags", C.c_uint32), ("precision", C.c_int32), ("device", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("reserved0", C.c_int32), ("pv_eps", C.c_double), ("reserved", C.c_int32 * 2)]
 
 
 _lib = None

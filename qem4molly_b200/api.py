@@ -48,7 +48,9 @@ class Engine:
     """One libqem handle: a configured QEM short + long + wall evaluator."""
 
     def __init__(self, *, L_box, alpha, r_cutoff, gamma_1=0.0, gamma_2=0.0, eps_0=1.0, accuracy=1e-6,
-                 N_t=30, rbe_p=30, iter_period=100, walls=(), mode_flags=0, precision=L.QEM_FP64, device=0):
+                 N_t=30, rbe_p=30, iter_period=100, walls=(), mode_flags=0, precision=L.QEM_FP64, device=0,
+                 pv_eps=0.0):
+        """pv_eps: window half-width of the regularised quadrature for gamma_1 * gamma_2 > 1."""
         lib = L.load()
         p = L.default_params()
         p.Lx, p.Ly, p.Lz = (float(v) for v in L_box)
@@ -63,6 +65,7 @@ class Engine:
         p.mode_flags = int(mode_flags)
         p.precision = int(precision)
         p.device = int(device)
+        p.pv_eps = float(pv_eps)
         self.params = p
         h = C.c_void_p()
         st = lib.qem_create(C.byref(p), C.byref(h))

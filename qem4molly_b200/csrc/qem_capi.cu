@@ -2,6 +2,7 @@
 // validation, device scratch, k-set sampling and the per-call orchestration of
 // the binning, short-range and long-range kernels.
 #include <algorithm>
+#include <cstddef>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -131,6 +132,7 @@ struct qem_handle {
     // k-set (host master copy)
     std::vector<double> kset;
     std::vector<double> kwt;  // per-k weights of a weighted (exact) k-set; empty: sum_K / P for every k
+    std::vector<double> norm_host;  // node sets of the regularised quadrature (gamma_1 gamma_2 > 1)
     double sum_K = 0;
     int P = 0;
     bool has_kset = false, kset_dirty = true;
@@ -156,7 +158,7 @@ struct qem_handle {
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
     // adjoint pass
-    DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh;
+    DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh, normxw;
     cudaStream_t s2 = nullptr;  // side stream of the long range
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     unsigned *h_status = nullptr;
@@ -234,9 +236,27 @@ static qem_status validate(const qem_params *p, std::string &why)
     if (p->N_t < 1 || p->N_t > QEM_MAX_NT) { why = "N_t must be in 1..64"; return QEM_ERR_ARG; }
     if (p->rbe_p < 0 || p->rbe_p > QEM_MAX_KSET) { why = "rbe_p must be in 0 .. QEM_MAX_KSET"; return QEM_ERR_ARG; }
     if (p->iter_period < 1) { why = "iter_period must be >= 1"; return QEM_ERR_ARG; }
-    if (!std::isfinite(p->gamma_up) || !std::isfinite(p->gamma_down) || !(fabs(p->gamma_up * p->gamma_down) < 1.0)) {
-        why = "|gamma_up * gamma_down| must be < 1 (the regularised gamma >= 1 path is not provided)";
+    if (!std::isfinite(p->gamma_up) || !std::isfinite(p->gamma_down) || !(p->gamma_up * p->gamma_down > -1.0) ||
+        p->gamma_up * p->gamma_down == 1.0) {
+        why = "gamma_up * gamma_down must be in (-1, 1) or > 1";
         return QEM_ERR_ARG;
+    }
+    if (p->gamma_up * p->gamma_down > 1.0) {  // the regularised quadrature (python_lib)
+        const double g12 = p->gamma_up * p->gamma_down, k0 = log(g12) / (2.0 * p->Lz);
+        if (p->precision != QEM_FP64 || !(p->mode_flags & QEM_CUTOFF_PYTHON)) {
+            why = "gamma_up * gamma_down > 1 needs QEM_FP64 and QEM_CUTOFF_PYTHON (python_lib regularised quadrature)";
+            return QEM_ERR_ARG;
+        }
+        if (!(p->pv_eps > 0 && p->pv_eps < k0)) { why = "pv_eps must be in (0, k_0)"; return QEM_ERR_ARG; }
+        const double kf[2] = {std::max(sqrt(-4.0 * p->alpha * log(p->accuracy)), 2.1 * k0),
+                              std::max(-log(p->accuracy) / (2.0 * p->Lz), 2.1 * k0)};
+        for (double f : kf) {
+            const int n1 = (int)(p->N_t * k0 / f);
+            if (n1 < 1 || p->N_t - 2 * n1 < 1) {
+                why = "gamma_up * gamma_down > 1: N_t k_0 / k_f gives an empty sub-interval (raise N_t)";
+                return QEM_ERR_ARG;
+            }
+        }
     }
     if (p->n_walls < 0 || p->n_walls > 2) { why = "n_walls must be 0..2"; return QEM_ERR_ARG; }
     for (int w = 0; w < p->n_walls; w++) {
@@ -251,7 +271,8 @@ static qem_status validate(const qem_params *p, std::string &why)
                            QEM_RESAMPLE_KSET | QEM_EQUAL_Z_TIES;
     if (p->mode_flags & ~known) { why = "unknown mode flag"; return QEM_ERR_ARG; }
     if (p->precision != QEM_FP64 && p->precision != QEM_FP32_FIX) { why = "precision must be QEM_FP64 or QEM_FP32_FIX"; return QEM_ERR_ARG; }
-    for (int i = 0; i < 5; i++)
+    if (p->reserved0 != 0) { why = "reserved fields must be zero"; return QEM_ERR_ARG; }
+    for (int i = 0; i < 2; i++)
         if (p->reserved[i] != 0) { why = "reserved fields must be zero"; return QEM_ERR_ARG; }
     return QEM_OK;
 }
@@ -287,6 +308,26 @@ static void build_consts(qem_handle *h)
     gauss_legendre(p.N_t, x, w);
     for (int i = 0; i < p.N_t; i++) {
         c.xd[i] = x[i]; c.wd[i] = w[i];
+    }
+    if (c.g12 > 1.0) {  // regularised quadrature: node sets of the 4 sub-intervals per family
+        c.norm = 1;
+        c.k0 = log(c.g12) / (2.0 * p.Lz);
+        c.pv_eps = p.pv_eps;
+        c.kf_norm[0] = std::max(c.kf_gauss_py, 2.1 * c.k0);
+        c.kf_norm[1] = std::max(c.kf_point_py, 2.1 * c.k0);
+        h->norm_host.clear();
+        for (int f = 0; f < 2; f++) {
+            const int n1 = (int)(p.N_t * c.k0 / c.kf_norm[f]);
+            const int n[4] = {n1, 10, n1, p.N_t - 2 * n1};
+            for (int t = 0; t < 4; t++) {
+                double xs[QEM_MAX_NT + 16], ws[QEM_MAX_NT + 16];
+                gauss_legendre(n[t], xs, ws);
+                c.norm_n[f][t] = n[t];
+                c.norm_off[f][t] = (int)h->norm_host.size();
+                h->norm_host.insert(h->norm_host.end(), xs, xs + n[t]);
+                h->norm_host.insert(h->norm_host.end(), ws, ws + n[t]);
+            }
+        }
     }
     c.Nt2 = (p.N_t + 1) / 2;
     for (int m = 0; m < c.Nt2; m++) {
@@ -464,6 +505,8 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     }
     if (!xyz || !q || !F) return fail(h, QEM_ERR_ARG, "NULL coordinate, charge or force pointer");
     if (async && (mem != QEM_MEM_DEVICE || energy)) return fail(h, QEM_ERR_ARG, "async evaluation: device memory, no energy");
+    if (want_E && h->sc.norm && (do_short || do_lj))
+        return fail(h, QEM_ERR_ARG, "no short-range energy is defined for gamma_up * gamma_down > 1");
     CU(cudaSetDevice(h->p.device));
     const int prec = h->p.precision;
     const bool prof_on = h->prof.on;
@@ -838,6 +881,8 @@ static qem_status run(qem_handle *h, int N, const double *xyz, const double *q, 
 // ---------------------------------------------------------------------------
 extern "C" {
 
+static_assert(sizeof(qem_params) == 200 && offsetof(qem_params, pv_eps) == 184, "qem_params layout (ABI)");
+
 void qem_default_params(qem_params *p)
 {
     if (!p) return;
@@ -888,6 +933,15 @@ qem_status qem_create(const qem_params *p, qem_handle **out)
         qem_destroy(h);
         return QEM_ERR_CUDA;
     }
+    if (h->sc.norm) {
+        const size_t bytes = sizeof(double) * h->norm_host.size();
+        if (grow(h->normxw, bytes) != cudaSuccess ||
+            cudaMemcpy(h->normxw.p, h->norm_host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            qem_destroy(h);
+            return QEM_ERR_CUDA;
+        }
+        h->sc.norm_xw = ptr<double>(h->normxw);
+    }
     *out = h;
     return QEM_OK;
 }
@@ -903,7 +957,7 @@ void qem_destroy(qem_handle *h)
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
-                      &h->lam, &h->ggk, &h->Gpart, &h->gFh};
+                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -1215,6 +1269,8 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
     retry = false;
     bool ties_adj = false;  // long-range gamma gradient of the second tie order in gout[4 .. 6)
     const bool do_short = terms & QEM_TERM_SHORT;
+    if (h->sc.norm && do_short)
+        return fail(h, QEM_ERR_ARG, "the short-range adjoint is not defined for gamma_up * gamma_down > 1");
     const bool do_long = terms & QEM_TERM_LONG;
     const bool do_lj = (terms & QEM_TERM_LJ) && h->p.n_walls > 0;
     CU(grow(h->pos, sizeof(double4) * N));

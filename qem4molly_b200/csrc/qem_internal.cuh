@@ -39,6 +39,13 @@ struct ShortConsts {
     int shard_world;      // W >= 1; the self terms and walls belong to rank 0
     float2 xf2[QEM_MAX_NT / 2], wf2[QEM_MAX_NT / 2];
     double xd[QEM_MAX_NT], wd[QEM_MAX_NT];
+    // gamma_1 gamma_2 > 1: regularised quadrature (FP64), family 0 Gauss, 1 point;
+    // sub-interval t of family f has norm_n[f][t] nodes at norm_xw[norm_off[f][t]]
+    // and weights right after them
+    int norm;
+    double k0, pv_eps, kf_norm[2];
+    int norm_n[2][4], norm_off[2][4];
+    const double *norm_xw;
 };
 
 // 2-D cell grid of the in-plane binning

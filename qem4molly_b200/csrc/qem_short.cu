@@ -163,11 +163,84 @@ __device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v
     Ir = r.x + r.y; Iz = z.x + z.y; Iu = u.x + u.y;
 }
 
+// gamma_1 gamma_2 > 1 (python_lib Force_short_norm_njit.py:11-414,
+// green_norm_njit.py:13-33): the pole of 1 / (g12 e^{-2 k Lz} - 1) at k_0 is
+// handled on four sub-intervals [0, k0 - e], [k0 - e, k0 + e], [k0 + e, 2 k0],
+// [2 k0, k_f] with their own Gauss-Legendre node sets.  With
+// f(k) = F(k) / (g12 e^{-2kLz} - 1), F the integrand without that factor:
+// in the window F(k) gamma_norm(k) - F'(k0) / (2 Lz) (gamma_norm: the pole-free
+// part, ten series terms; F' by the reference's central difference with step
+// 0.01 e), up to 2 k0 f + F(k0) / (2 Lz (k - k0)), beyond 2 k0 f.  The Gauss
+// rho integrand of the window carries no exp(-k^2 / 4 alpha) (as in the
+// reference, Force_short_norm_njit.py:59).  Same image decomposition as the
+// plain path: F = k up(k) J(k rho) with up = -pf exp(-k (a' + c2 k)).
+__device__ __forceinline__ double gamma_norm_f64(double x)
+{
+    double u = 0.5, d = -1.0 + x / 2.0, u0 = 0.5, d0 = x / 2.0;
+#pragma unroll
+    for (int i = 0; i < 10; i++) {
+        u0 = u0 * (-x) / (i + 3);
+        d0 = d0 * (-x) / (i + 3);
+        u += u0;
+        d += d0;
+    }
+    return u / d;
+}
+
+template <bool WITH_J1>
+__device__ void quad_norm_f64(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz)
+{
+    const int f = v.c2 > 0.0 ? 0 : 1;  // 0: Gauss family, 1: point family
+    const double k0 = c.k0, ep = c.pv_eps, twoLz = c.twoLz;
+    auto up = [&](double k) { return -v.pf * exp(-k * fma(k, v.c2, v.ae)); };
+    auto Fr = [&](double k) { return WITH_J1 ? k * up(k) * j1(k * rho) : 0.0; };
+    auto Fz = [&](double k) { return k * up(k) * (WITH_J1 ? j0(k * rho) : 1.0); };
+    const double k1 = k0 - 0.01 * ep, k2 = k0 + 0.01 * ep;
+    const double dfr = (Fr(k2) - Fr(k1)) / (k2 - k1), dfz = (Fz(k2) - Fz(k1)) / (k2 - k1);
+    const double r0 = Fr(k0), z0 = Fz(k0);
+    const double lo[4] = {0.0, k0 - ep, k0 + ep, 2.0 * k0}, hi[4] = {k0 - ep, k0 + ep, 2.0 * k0, c.kf_norm[f]};
+    double r = 0, z = 0;
+#pragma unroll 1
+    for (int t = 0; t < 4; t++) {
+        const int n = c.norm_n[f][t];
+        const double *xs = c.norm_xw + c.norm_off[f][t], *ws = xs + n;
+        const double a = lo[t], b = hi[t];
+#pragma unroll 1
+        for (int i = 0; i < n; i++) {
+            const double k = 0.5 * (b - a) * xs[i] + 0.5 * (b + a), w = 0.5 * (b - a) * ws[i];
+            const double J0 = WITH_J1 ? j0(k * rho) : 1.0, J1 = WITH_J1 ? j1(k * rho) : 0.0;
+            const double u = up(k);
+            double fr, fz;
+            if (fabs(k - k0) <= ep) {
+                const double gn = gamma_norm_f64(twoLz * (k - k0));
+                const double ur = f == 0 ? -v.pf * exp(-k * v.ae) : u;  // no exp(-k^2/4 alpha) here
+                fr = k * ur * J1 * gn - dfr / twoLz;
+                fz = k * u * J0 * gn - dfz / twoLz;
+            } else {
+                const double g = 1.0 / (c.g12 * exp(-k * twoLz) - 1.0);
+                fr = k * u * J1 * g;
+                fz = k * u * J0 * g;
+                if (k <= 2.0 * k0) {
+                    fr += r0 / (twoLz * (k - k0));
+                    fz += z0 / (twoLz * (k - k0));
+                }
+            }
+            r += w * fr;
+            z += w * fz;
+        }
+    }
+    Ir = r;
+    Iz = z;
+}
+
 template <int PREC, bool ENERGY, bool WITH_J1>
 __device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
                                      double &Iu)
 {
-    if (PREC == QEM_FP64) {
+    if (PREC == QEM_FP64 && c.norm) {
+        quad_norm_f64<WITH_J1>(c, v, rho, Ir, Iz);
+        Iu = 0;
+    } else if (PREC == QEM_FP64) {
         quad_f64<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
     } else {
         float r, z, u;
@@ -312,8 +385,10 @@ __device__ void self_terms(const ShortConsts &c, double z, double q, double &Fz,
         const double sa = (l == 1) ? -1.0 : (l == 2) ? 1.0 : 0.0;
         double Ir, Iz, Iu;
         quad<PREC, ENERGY, false>(c, interval(c, a, b, gauss), 0.0, Ir, Iz, Iu);
-        const double sf = gauss ? 1.0 : -1.0;
-        if (zterm) Fs += sf * sa * Iz;  // -Fp1 + Fg
+        // -Fp1 + Fg; with g12 > 1 the reference adds the point part with the
+        // opposite sign (Force_short_norm_njit.py:330-331), reproduced
+        const double sf = (gauss || (PREC == QEM_FP64 && c.norm)) ? 1.0 : -1.0;
+        if (zterm) Fs += sf * sa * Iz;
         if (ENERGY) {
             U += sf * Iu;
             if (!gauss && l > 0) Ub += 0.5 * b / a;

@@ -151,6 +151,8 @@ def main(argv=None):
     ap.add_argument("--N", type=int, default=None, help="particle count (configs 2, 3, 5)")
     ap.add_argument("--ties", type=float, default=0.0,
                     help="round z to multiples of this spacing and evaluate with QEM_EQUAL_Z_TIES")
+    ap.add_argument("--norm", action="store_true",
+                    help="gamma_1 = gamma_2 = e with Lz = 2 (regularised quadrature, python mode, FP64)")
     a = ap.parse_args(argv)
     from . import _lib as L
 
@@ -158,7 +160,18 @@ def main(argv=None):
     cfg = make(N=a.N) if (a.N and a.config != 1) else make()
     if a.ties > 0:
         cfg["xyz"][:, 2] = np.round(cfg["xyz"][:, 2] / a.ties) * a.ties
-    e = engine_for(cfg, a.precision, mode_flags=L.QEM_EQUAL_Z_TIES if a.ties > 0 else 0)
+    if a.norm:
+        from .api import Engine
+
+        cfg["L"] = (cfg["L"][0], cfg["L"][1], 2.0)
+        cfg["xyz"][:, 2] = 0.2 + 1.6 * (cfg["xyz"][:, 2] - cfg["xyz"][:, 2].min()) / np.ptp(cfg["xyz"][:, 2])
+        e = Engine(L_box=cfg["L"], alpha=cfg["alpha"], r_cutoff=cfg["r_cutoff"], gamma_1=np.e, gamma_2=np.e,
+                   accuracy=cfg["accuracy"], N_t=cfg["N_t"], rbe_p=cfg["P"], mode_flags=L.QEM_PYTHON_MODE,
+                   precision=L.QEM_FP64, pv_eps=0.05)
+        e.sample_kset(7, cfg["P"])
+        a.precision = "fp64 (gamma_1 gamma_2 = e^2, Lz = 2, regularised)"
+    else:
+        e = engine_for(cfg, a.precision, mode_flags=L.QEM_EQUAL_Z_TIES if a.ties > 0 else 0)
     dev = torch.device("cuda", 0)
     x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
     q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)

@@ -26,6 +26,8 @@ What is generated (each case states the reference file it exercises):
   accurate-Bessel shim, so the python-convention oracle mode is pinned to
   ~1e-12.
 * ``icm_energy.json``  -- ICM.U_cal / ICM.F_cal on a 3-particle slab.
+* ``short_norm.json``  -- gamma_1 gamma_2 > 1: the regularised pair and self
+  forces of Force_short_norm_njit.py for 12 seeded pairs (accurate Bessel).
 * ``long_ties.json``   -- equal-z ties: a 36-particle slab on 5 z levels
   through the z-ordered sums with their equal_cell groups (fixed k-set).
 * ``long_exact.json``  -- the exact (non-random-batch) long range of
@@ -358,6 +360,38 @@ def gen_ties(rng):
                 kset=kset.tolist(), sum_K=S_tot, F_long=FL.tolist(), E_long_k0=E_k0, n_levels=G)
 
 
+def gen_norm(rng):
+    """gamma_1 gamma_2 > 1 (metamaterial substrates): the regularised short-range quadrature of
+    Force_short_norm_njit.py (Force_rhos_norm, Force_zs_norm, Force_zs_self_norm) with the node
+    sets of Force_short_range_njit.Gauss_para_gen, for seeded pairs and particles."""
+    import numpy as np
+
+    import Force_short_norm_njit as FN
+    import Force_short_range_njit as Fs
+
+    Lz, alpha, acc, N_t, eps = 2.0, 0.1, 1e-6, 30, 0.05
+    g1 = g2 = float(np.e)  # gamma_down = gamma_up: g12 = e^2, k_0 = 0.5
+    e1 = (1 - g1) / (1 + g1)
+    e3 = (1 - g2) / (1 + g2)
+    G = Fs.Gauss_para_gen(e1, 1.0, e3, Lz, N_t, acc, alpha)
+    INCAR = (1, 1, 1, 1, Lz, e1, 1.0, e3, alpha, acc)
+    cases = []
+    for t in range(12):
+        zi, zj = 0.2 + 1.6 * rng.random(2)
+        rho = 0.3 + 2.7 * rng.random()
+        ang = 2 * np.pi * rng.random()
+        xi, yi = 5.0, 5.0
+        xj, yj = xi + rho * np.cos(ang), yi + rho * np.sin(ang)
+        qi, qj = (1.0, -1.0) if t % 2 == 0 else (0.7, 1.3)
+        pos = (qj, qi, xj, xi, yj, yi, zj, zi)
+        cases.append(dict(q_i=qi, q_j=qj, c_i=[xi, yi, zi], c_j=[xj, yj, zj],
+                          F_rho=FN.Force_rhos_norm(pos, INCAR, eps, N_t, *G),
+                          F_z=FN.Force_zs_norm(pos, INCAR, eps, N_t, *G),
+                          F_z_self_j=FN.Force_zs_self_norm((qj, xj, yj, zj), INCAR, eps, N_t, *G)))
+    return dict(source="Force_short_norm_njit.py:68-414 with Force_short_range_njit.Gauss_para_gen (258-286)",
+                L_z=Lz, alpha=alpha, accuracy=acc, N_t=N_t, pv_eps=eps, gamma_1=g1, gamma_2=g2, cases=cases)
+
+
 def gen_icm(rng):
     import numpy as np
 
@@ -421,6 +455,7 @@ def run_variant(bessel):
         _dump("system_python.json", gen_system(np.random.default_rng(20261207)))
         _dump("long_exact.json", gen_exact(np.random.default_rng(20261208)))
         _dump("long_ties.json", gen_ties(np.random.default_rng(20261209)))
+        _dump("short_norm.json", gen_norm(np.random.default_rng(20261210)))
 
 
 if __name__ == "__main__":

@@ -92,3 +92,17 @@ def test_exact_kset_rows_match_oracle(lib):
     assert lib.qem_exact_kset_rows(10.0, 10.0, 0.1, -1.0, None, None, 0, C.byref(n)) == 1
     assert lib.qem_exact_kset_rows(10.0, 10.0, 0.1, 1e9, None, None, 0, C.byref(n)) == 8  # QEM_ERR_RANGE
     assert lib.qem_set_kset_exact(None, 1.0, None) == 1
+
+
+def test_params_layout_and_gamma_above_one_rules(lib):
+    """qem_params is 200 bytes with pv_eps at offset 184; gamma_up * gamma_down > 1 needs FP64,
+    python cutoffs, 0 < pv_eps < k_0 and non-empty sub-intervals (checked before any CUDA call)."""
+    assert C.sizeof(L.Params) == 200 and L.Params.pv_eps.offset == 184
+    e = float(np.exp(1.0))  # gamma_1 = gamma_2 = e: k_0 = ln(e^2) / (2 Lz) = 0.5 at Lz = 2
+    base = dict(Lz=2.0, alpha=0.1, gamma_up=e, gamma_down=e)
+    assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.0) == 1            # pv_eps missing
+    assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.6) == 1            # pv_eps >= k_0
+    assert _create(lib, **base, mode_flags=0, pv_eps=0.05) == 1                           # Julia cutoffs
+    assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.05, precision=L.QEM_FP32_FIX) == 1
+    assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.05, N_t=4) == 1     # N_1 = 0
+    assert _create(lib, Lz=2.0, gamma_up=1.0, gamma_down=1.0) == 1                         # the pole at k = 0

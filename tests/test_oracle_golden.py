@@ -213,6 +213,27 @@ def test_equal_z_ties_vs_python_equal_cell():
     assert np.abs(F0[:, 2] - Fr[:, 2]).max() > 0.05 * np.abs(Fr).max()
 
 
+def test_regularised_quadrature_vs_python_norm():
+    """gamma_1 gamma_2 > 1 (short_norm.json): the oracle's pair and self forces in python
+    mode against Force_rhos_norm / Force_zs_norm / Force_zs_self_norm."""
+    import ctypes as C
+
+    d = load("short_norm.json")
+    p = O.params((50.0, 50.0, d["L_z"]), d["alpha"], 10.0, d["gamma_1"], d["gamma_2"], accuracy=d["accuracy"],
+                 N_t=d["N_t"], cutoff_mode=O.CUTOFF_PYTHON, dir_mode=O.DIR_MINIMAGE, pair_mode=O.PAIR_PHYSICAL,
+                 pv_eps=d["pv_eps"])
+    L = O.lib()
+    for c in d["cases"]:
+        cj, ci = np.array(c["c_j"]), np.array(c["c_i"])
+        out = np.zeros(4)
+        L.qo_F_short_ij(C.byref(p), c["q_j"], c["q_i"], O._d(cj)[1], O._d(ci)[1], 0, O._d(out)[1])
+        rho = np.hypot(cj[0] - ci[0], cj[1] - ci[1])
+        assert np.isclose(out[0], c["F_rho"] * (cj[0] - ci[0]) / rho, rtol=1e-12, atol=0)
+        assert np.isclose(out[1], c["F_rho"] * (cj[1] - ci[1]) / rho, rtol=1e-12, atol=0)
+        assert np.isclose(out[2], c["F_z"], rtol=1e-11, atol=0)
+        assert np.isclose(L.qo_F_short_i(C.byref(p), c["q_j"], O._d(cj)[1], 0), c["F_z_self_j"], rtol=1e-12)
+
+
 def test_sortperm_is_stable():
     """QEM_long.jl:39-40 sortperm: stable ascending, ties keep index order."""
     rng = np.random.default_rng(3)
