@@ -187,6 +187,8 @@ struct qem_handle {
     };
     GraphKey gkey, gwarm;
     bool gwarm_valid = false;
+    int64_t enq_launches = 0;  // kernels enqueued by the last asynchronous (recorded) evaluation
+    int64_t glaunches = 0;     // kernels in the recorded evaluation graph
     cudaStream_t gcap = nullptr;
     cudaGraphExec_t gexec = nullptr;
 };
@@ -676,7 +678,10 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         launches++;
         CU(cudaMemcpyAsync(h->h_E, h->Eout.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
-    if (async) return QEM_OK;
+    if (async) {
+        h->enq_launches = launches;
+        return QEM_OK;
+    }
     if (mem == QEM_MEM_HOST) CU(cudaMemcpyAsync(F, F_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(h->h_status, st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     if (do_short)
@@ -817,6 +822,7 @@ static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const 
         }
         h->gexec = ex;
         h->gkey = k;
+        h->glaunches = h->enq_launches;
     }
     const bool do_short = terms & QEM_TERM_SHORT;
     unsigned *st = ptr<unsigned>(h->status);
@@ -844,7 +850,7 @@ static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const 
     }
     h->counts[0] = do_short ? h->Np : 0;
     h->counts[1] = N;
-    h->counts[3] = 1;
+    h->counts[3] = h->glaunches;  // the recorded kernels, replayed by one graph launch
     if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
     if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
     h->err.clear();

@@ -26,10 +26,13 @@ def test_replays_equal_the_ordinary_call(prec):
     ref = e.forces(cfg["xyz"], cfg["q"])           # pageable host memory: never replayed
     x, q = _dev(cfg["xyz"]), _dev(cfg["q"])
     F = _dev(np.zeros_like(cfg["xyz"]))
+    launches = []
     for _ in range(4):                              # ordinary, record + replay, replay, replay
         F.fill_(float("nan"))
         e.forces_device(x, q, F)
         assert np.array_equal(F.cpu().numpy(), ref)
+        launches.append(e.counts()["launches"])
+    assert len(set(launches)) == 1 and launches[0] > 20  # a replay runs the recorded kernels
 
 
 def test_replay_follows_coordinates_kset_and_buffers():
