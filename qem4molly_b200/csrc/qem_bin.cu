@@ -157,6 +157,63 @@ __global__ void k_scan_add(T *__restrict__ out, int n, const T *__restrict__ bsu
     if (i == 0) out[n] = bsum[(n + SCAN_BLOCK - 1) / SCAN_BLOCK];
 }
 
+// One-block exclusive scan for n <= SCAN_SMALL_MAX (one launch instead of
+// three; the many-small-systems batch is launch-bound): thread t owns
+// elements [t pt, (t + 1) pt), pt = ceil(n / SCAN_BLOCK) <= SCAN_SMALL_PT,
+// summed in order; the thread totals are scanned exclusively without an
+// "inclusive minus own" step; out[n] = total.
+constexpr int SCAN_SMALL_PT = 8;
+constexpr int SCAN_SMALL_MAX = SCAN_BLOCK * SCAN_SMALL_PT;
+
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const TI *__restrict__ in, TO *__restrict__ out, int n)
+{
+    __shared__ TO warp_tot[SCAN_BLOCK / 32];
+    const int pt = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    const int b = threadIdx.x * pt;
+    TO v[SCAN_SMALL_PT];
+    TO tot = (TO)0;
+#pragma unroll
+    for (int j = 0; j < SCAN_SMALL_PT; j++) {
+        const int i = b + j;
+        v[j] = (j < pt && i < n) ? (TO)in[i] : (TO)0;
+        const TO x = v[j];
+        v[j] = tot;  // exclusive within the thread
+        tot += x;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    TO x = tot;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const TO t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    TO ex = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) ex = (TO)0;
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        const TO y0 = warp_tot[lane];
+        TO y = y0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const TO t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        TO e = __shfl_up_sync(0xffffffffu, y, 1);
+        if (lane == 0) e = (TO)0;
+        warp_tot[lane] = e;  // exclusive over warps
+        if (lane == 31) out[n] = y;
+    }
+    __syncthreads();
+    const TO base = warp_tot[w] + ex;
+#pragma unroll
+    for (int j = 0; j < SCAN_SMALL_PT; j++) {
+        const int i = b + j;
+        if (j < pt && i < n) out[i] = base + v[j];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // cell counting sort
 // ---------------------------------------------------------------------------
@@ -649,6 +706,10 @@ inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 template <typename TI, typename TO>
 cudaError_t scan_impl(const TI *in, TO *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
+    if (n <= SCAN_SMALL_MAX) {
+        k_scan_small<TI, TO><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
+        return cudaGetLastError();
+    }
     int nb = nblk(n, SCAN_BLOCK);
     if (nb < 1) nb = 1;
     if (tmp_bytes < sizeof(TO) * (size_t)(nb + 1)) return cudaErrorInvalidValue;
@@ -663,6 +724,16 @@ cudaError_t scan_impl(const TI *in, TO *out, int n, void *tmp, size_t tmp_bytes,
 
 size_t qem_scan_tmp_bytes(int n) { return sizeof(double) * (size_t)(nblk(n, SCAN_BLOCK) + 2); }
 
+int qem_scan_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
+
+int qem_zsort_launches(int N)
+{
+    if (N <= 0) return 0;
+    int passes = 0;
+    for (int w = ZTILE; w < N; w <<= 1) passes++;
+    return 1 + passes;
+}
+
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
     return scan_impl<int, int64_t>(in, out, n, tmp, tmp_bytes, s);
@@ -670,6 +741,10 @@ cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, s
 
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
+    if (n <= SCAN_SMALL_MAX) {
+        k_scan_small<double, double><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
+        return cudaGetLastError();
+    }
     int nb = nblk(n, SCAN_BLOCK);
     if (nb < 1) nb = 1;
     if (tmp_bytes < sizeof(double) * (size_t)(nb + 1)) return cudaErrorInvalidValue;

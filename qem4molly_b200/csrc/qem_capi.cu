@@ -618,7 +618,9 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         mk_lprep = h->prof.mark(sl);
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 1));
-        launches += 22;
+        // z sort, zgather + q scan + k = 0 term, per-k constants + totals + scan, force pass + final
+        const int long_launches = qem_zsort_launches(N) + 2 + qem_scan_launches(N) + (Pk > 0 ? 3 : 0) + 2;
+        launches += long_launches;
         if (h->p.mode_flags & QEM_EQUAL_Z_TIES) {
             // Equal-z ties: a tied pair counts once as below and once as above
             // in the two orders (z, index up) and (z, index down), and every
@@ -633,7 +635,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
                                    h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch,
                                    st, sl, stage));
             CU(qem_launch_scale(3 * N, 0.5, FL, FL, sl));
-            launches += 23;
+            launches += long_launches + 1;
         }
         mk_lforce = h->prof.mark(sl);
         h->counts[2] = Pk;
@@ -647,7 +649,10 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         if (rebuild) {
             const qem_status bs = build_pairs(h, N, st, s);
             if (bs != QEM_OK) return bs;
-            launches += h->geom.ncx >= 3 && h->geom.ncy >= 3 && N >= 2 * (int64_t)h->ncell ? 15 : 16;
+            // cells: count, scan, scatter, sort; pairs: count, scan, (in_base | fill), scan, fill
+            // (+ incoming fill and sort on the thread-per-owner path)
+            const bool warp_path = h->geom.ncx >= 3 && h->geom.ncy >= 3 && N >= 2 * (int64_t)h->ncell;
+            launches += 3 + qem_scan_launches(h->ncell) + 3 + 2 * qem_scan_launches(N) + (warp_path ? 0 : 1);
         }
         h->short_calls++;
         mk_bin = h->prof.mark(s);

@@ -98,6 +98,9 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
+// kernel launches of one scan of n elements and of one z sort of N particles
+int qem_scan_launches(int n);
+int qem_zsort_launches(int N);
 
 // np: device pointer to the pair count; cap: capacity of pairs / R / Upair
 cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np, int64_t cap, const int2 *pairs,
