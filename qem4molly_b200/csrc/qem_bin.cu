@@ -292,6 +292,72 @@ __global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__res
     }
 }
 
+// The whole cell build of a small system (N and ncell at most CELLS_SMALL) in
+// one block: counts in shared memory, their scan, the atomic scatter, the
+// ascending order inside every cell (one warp per cell, as k_cell_sort) and
+// the cell-order positions.  The result is the same as the multi-kernel
+// build (the order inside a cell does not depend on the scatter).
+constexpr int CELLS_SMALL = 8192;
+
+__global__ void __launch_bounds__(1024) k_cells_small(int N, int ncell, const int *__restrict__ cell,
+                                                      const double4 *__restrict__ pos, int *__restrict__ cstart,
+                                                      int *__restrict__ clist, int *__restrict__ pos_of,
+                                                      double4 *__restrict__ pos_c)
+{
+    __shared__ int cnt[CELLS_SMALL];
+    __shared__ int warp_tot[32];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int c = tid; c < ncell; c += 1024) cnt[c] = 0;
+    __syncthreads();
+    for (int i = tid; i < N; i += 1024) atomicAdd(&cnt[cell[i]], 1);
+    __syncthreads();
+    // exclusive scan of cnt into cstart (thread t owns cells [t pt, (t + 1) pt)); cnt becomes the fill pointer
+    const int pt = (ncell + 1023) / 1024, b = tid * pt;
+    int tot = 0;
+    for (int j = 0; j < pt; j++)
+        if (b + j < ncell) tot += cnt[b + j];
+    int x = tot;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        warp_tot[lane] = y;  // inclusive over warps
+    }
+    __syncthreads();
+    int run = x - tot + (w > 0 ? warp_tot[w - 1] : 0);  // exclusive start of this thread's cells
+    for (int j = 0; j < pt; j++)
+        if (b + j < ncell) {
+            const int c = cnt[b + j];
+            cstart[b + j] = run;
+            cnt[b + j] = run;
+            run += c;
+        }
+    if (tid == 1023) cstart[ncell] = warp_tot[31];
+    __syncthreads();
+    for (int i = tid; i < N; i += 1024) clist[atomicAdd(&cnt[cell[i]], 1)] = i;
+    __syncthreads();
+    for (int c = w; c < ncell; c += 32) {
+        const int cb = cstart[c], ce = cstart[c + 1];
+        warp_sort_segment<int>(clist, cb, ce, lane, 0x7fffffff);
+    }
+    __syncthreads();
+    for (int s = tid; s < N; s += 1024) {
+        const int i = clist[s];
+        pos_of[i] = s;
+        pos_c[s] = pos[i];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // pair list (j > i, minimum-image rho^2 <= r_c^2)
 // ---------------------------------------------------------------------------
@@ -763,10 +829,16 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
     return cudaGetLastError();
 }
 
+bool qem_cells_small(int N, int ncell) { return N <= CELLS_SMALL && ncell <= CELLS_SMALL; }
+
 cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *pos, int *cell_cnt, int *cell_start,
                              int *cell_fill, int *cell_list, int *pos_of, double4 *pos_c, void *scan_tmp,
                              size_t scan_tmp_bytes, cudaStream_t s)
 {
+    if (qem_cells_small(N, ncell)) {
+        k_cells_small<<<1, 1024, 0, s>>>(N, ncell, cell, pos, cell_start, cell_list, pos_of, pos_c);
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(cell_cnt, 0, sizeof(int) * ncell, s);
     if (e != cudaSuccess) return e;
     k_cell_count<<<nblk(N, 256), 256, 0, s>>>(N, cell, cell_cnt);

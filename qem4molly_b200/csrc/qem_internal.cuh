@@ -100,6 +100,8 @@ cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, s
 size_t qem_scan_tmp_bytes(int n);
 // kernel launches of one scan of n elements and of one z sort of N particles
 int qem_scan_launches(int n);
+// whether the cell build of N particles in ncell cells runs as one one-block kernel
+bool qem_cells_small(int N, int ncell);
 int qem_zsort_launches(int N);
 
 // np: device pointer to the pair count; cap: capacity of pairs / R / Upair
