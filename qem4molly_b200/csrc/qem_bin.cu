@@ -386,13 +386,12 @@ __device__ __forceinline__ void stencil_range(int n, int &lo, int &hi)
 // most cap pairs (QEM_ST_OVERFLOW beyond) and counts each pair's incoming
 // entry for its second particle.
 template <bool FILL>
-__global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__restrict__ cell,
-                        const int *__restrict__ cstart, const int *__restrict__ clist, CellGeom g, double rc2,
-                        int *__restrict__ pcount, const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
-                        int64_t cap, int *__restrict__ in_cnt, unsigned *status)
+__device__ __forceinline__ void pairs_of_owner(int t, const double4 *__restrict__ pos_c, const int *__restrict__ cell,
+                                               const int *__restrict__ cstart, const int *__restrict__ clist,
+                                               const CellGeom &g, double rc2, int *__restrict__ pcount,
+                                               const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
+                                               int64_t cap, int *__restrict__ in_cnt, unsigned *status)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N) return;
     int i = clist[t];
     double4 pi = pos_c[t];
     int c = cell[i];
@@ -436,6 +435,16 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__r
         }
     }
     if (!FILL) pcount[t] = cnt;
+}
+
+template <bool FILL>
+__global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__restrict__ cell,
+                        const int *__restrict__ cstart, const int *__restrict__ clist, CellGeom g, double rc2,
+                        int *__restrict__ pcount, const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
+                        int64_t cap, int *__restrict__ in_cnt, unsigned *status)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < N) pairs_of_owner<FILL>(t, pos_c, cell, cstart, clist, g, rc2, pcount, poff, pairs, cap, in_cnt, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -648,10 +657,8 @@ __device__ __forceinline__ void sort_small_segment(int *list, int64_t b, int n)
 // segment sorted in registers (segments of more than 64 entries, which a
 // cutoff disc at these densities practically never holds, by insertion in
 // place)
-__global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restrict__ list)
+__device__ __forceinline__ void sort_incoming(int i, const int64_t *__restrict__ off, int *__restrict__ list)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
     const int64_t b = off[i], e = off[i + 1];
     const int64_t n = e - b;
     if (n <= 1) return;
@@ -672,6 +679,86 @@ __global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restric
             list[t + 1] = v;
         }
     }
+}
+
+__global__ void k_in_sort(int N, const int64_t *__restrict__ off, int *__restrict__ list)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) sort_incoming(i, off, list);
+}
+
+// The whole thread-per-owner pair-list build of a small system (N at most
+// PAIRS_SMALL) in one block: counts, their scan, the fill with the incoming
+// counts, their scan, the incoming scatter and the per-particle sort -- the
+// same steps and results as the multi-kernel build.
+constexpr int PAIRS_SMALL = 8192;
+
+// exclusive scan of n <= 8192 values by the calling block of 1024 threads; out[n] = total
+template <typename TI, typename TO>
+__device__ void block_scan_small(const TI *in, TO *out, int n, TO *warp_tot)
+{
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int pt = (n + 1023) / 1024, b = tid * pt;
+    TO tot = 0;
+    for (int j = 0; j < pt; j++)
+        if (b + j < n) tot += (TO)in[b + j];
+    TO x = tot;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const TO t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        TO y = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const TO t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        warp_tot[lane] = y;  // inclusive over warps
+    }
+    __syncthreads();
+    TO run = x - tot + (w > 0 ? warp_tot[w - 1] : (TO)0);
+    for (int j = 0; j < pt; j++)
+        if (b + j < n) {
+            const TO v = (TO)in[b + j];
+            out[b + j] = run;
+            run += v;
+        }
+    if (tid == 1023) out[n] = warp_tot[31];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__restrict__ pos_c,
+                                                      const int *__restrict__ cell, const int *__restrict__ cstart,
+                                                      const int *__restrict__ clist, CellGeom g, double rc2,
+                                                      int *__restrict__ pcount, int64_t *__restrict__ poff,
+                                                      int2 *__restrict__ pairs, int64_t cap, int *__restrict__ in_cnt,
+                                                      int *__restrict__ in_fill, int64_t *__restrict__ in_off,
+                                                      int *__restrict__ in_list, unsigned *status)
+{
+    __shared__ int64_t warp_tot[32];
+    const int tid = threadIdx.x;
+    for (int t = tid; t < N; t += 1024) {
+        pairs_of_owner<false>(t, pos_c, cell, cstart, clist, g, rc2, pcount, nullptr, nullptr, 0, nullptr, nullptr);
+        in_cnt[t] = 0;
+        in_fill[t] = 0;
+    }
+    __syncthreads();
+    block_scan_small<int, int64_t>(pcount, poff, N, warp_tot);
+    for (int t = tid; t < N; t += 1024)
+        pairs_of_owner<true>(t, pos_c, cell, cstart, clist, g, rc2, nullptr, poff, pairs, cap, in_cnt, status);
+    __syncthreads();
+    block_scan_small<int, int64_t>(in_cnt, in_off, N, warp_tot);
+    const int64_t np = min(poff[N], cap);
+    for (int64_t p = tid; p < np; p += 1024) {
+        const int j = pairs[p].y;
+        in_list[in_off[j] + atomicAdd(&in_fill[j], 1)] = (int)p;
+    }
+    __syncthreads();
+    for (int i = tid; i < N; i += 1024) sort_incoming(i, in_off, in_list);
 }
 
 // ---------------------------------------------------------------------------
@@ -873,7 +960,12 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
     }
     // one thread per owner (over the full deduplicated stencil when there are
     // fewer than 3 cells along x or y), incoming entries scattered with
-    // atomics and sorted
+    // atomics and sorted; a small system in one block
+    if (N <= PAIRS_SMALL) {
+        k_pairs_small<<<1, 1024, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, pcount, poff, pairs, cap,
+                                         in_cnt, in_slot, in_off, in_list, status);
+        return cudaGetLastError();
+    }
     k_pairs<false><<<nblk(N, 128), 128, 0, s>>>(N, pos_c, cell, cell_start, cell_list, g, rc2, pcount, nullptr,
                                                  nullptr, 0, nullptr, nullptr);
     if ((e = scan_impl<int, int64_t>(pcount, poff, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;

@@ -652,8 +652,8 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
             // cells: count, scan, scatter, sort; pairs: count, scan, (in_base | fill), scan, fill
             // (+ incoming fill and sort on the thread-per-owner path)
             const bool warp_path = h->geom.ncx >= 3 && h->geom.ncy >= 3 && N >= 2 * (int64_t)h->ncell;
-            launches += (qem_cells_small(N, h->ncell) ? 1 : 3 + qem_scan_launches(h->ncell)) + 3 +
-                        2 * qem_scan_launches(N) + (warp_path ? 0 : 1);
+            launches += (qem_cells_small(N, h->ncell) ? 1 : 3 + qem_scan_launches(h->ncell)) +
+                        (warp_path ? 3 + 2 * qem_scan_launches(N) : (N <= 8192 ? 1 : 4 + 2 * qem_scan_launches(N)));
         }
         h->short_calls++;
         mk_bin = h->prof.mark(s);
