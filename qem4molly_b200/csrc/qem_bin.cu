@@ -169,49 +169,7 @@ template <typename TI, typename TO>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const TI *__restrict__ in, TO *__restrict__ out, int n)
 {
     __shared__ TO warp_tot[SCAN_BLOCK / 32];
-    const int pt = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
-    const int b = threadIdx.x * pt;
-    TO v[SCAN_SMALL_PT];
-    TO tot = (TO)0;
-#pragma unroll
-    for (int j = 0; j < SCAN_SMALL_PT; j++) {
-        const int i = b + j;
-        v[j] = (j < pt && i < n) ? (TO)in[i] : (TO)0;
-        const TO x = v[j];
-        v[j] = tot;  // exclusive within the thread
-        tot += x;
-    }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    TO x = tot;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const TO t = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= d) x += t;
-    }
-    TO ex = __shfl_up_sync(0xffffffffu, x, 1);
-    if (lane == 0) ex = (TO)0;
-    if (lane == 31) warp_tot[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        const TO y0 = warp_tot[lane];
-        TO y = y0;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const TO t = __shfl_up_sync(0xffffffffu, y, d);
-            if (lane >= d) y += t;
-        }
-        TO e = __shfl_up_sync(0xffffffffu, y, 1);
-        if (lane == 0) e = (TO)0;
-        warp_tot[lane] = e;  // exclusive over warps
-        if (lane == 31) out[n] = y;
-    }
-    __syncthreads();
-    const TO base = warp_tot[w] + ex;
-#pragma unroll
-    for (int j = 0; j < SCAN_SMALL_PT; j++) {
-        const int i = b + j;
-        if (j < pt && i < n) out[i] = base + v[j];
-    }
+    qem_block_scan_excl_small<TI, TO>(in, out, n, warp_tot);
 }
 
 // ---------------------------------------------------------------------------

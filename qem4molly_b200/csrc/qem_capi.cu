@@ -619,8 +619,12 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 1));
         // z sort, zgather + q scan + k = 0 term, per-k constants + totals + scan, force pass + final
-        const int long_launches = qem_zsort_launches(N) + 2 + qem_scan_launches(N) + (Pk > 0 ? 3 : 0) + 2;
-        launches += long_launches;
+        auto long_launches = [&](bool energy_pass) {
+            return qem_zsort_launches(N) +
+                   (!energy_pass && N <= 8192 ? 1 + (Pk > 0 ? 2 : 0) : 2 + qem_scan_launches(N) + (Pk > 0 ? 3 : 0)) +
+                   2;
+        };
+        launches += long_launches(want_E);
         if (h->p.mode_flags & QEM_EQUAL_Z_TIES) {
             // Equal-z ties: a tied pair counts once as below and once as above
             // in the two orders (z, index up) and (z, index down), and every
@@ -635,7 +639,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
                                    h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch,
                                    st, sl, stage));
             CU(qem_launch_scale(3 * N, 0.5, FL, FL, sl));
-            launches += long_launches + 1;
+            launches += long_launches(false) + 1;
         }
         mk_lforce = h->prof.mark(sl);
         h->counts[2] = Pk;

@@ -98,6 +98,59 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
+// One-block exclusive scan of n <= 8192 values by the calling block of 1024
+// threads (thread t owns elements [t pt, (t + 1) pt), pt = ceil(n / 1024),
+// summed in order; the thread totals are scanned exclusively without an
+// "inclusive minus own" step); out[n] = total.  warp_tot: 32 entries of
+// shared memory.  Every block-wide caller gets the same arithmetic.
+template <typename TI, typename TO>
+__device__ void qem_block_scan_excl_small(const TI *__restrict__ in, TO *__restrict__ out, int n, TO *warp_tot)
+{
+    constexpr int PT = 8;
+    const int pt = (n + 1023) / 1024;
+    const int b = threadIdx.x * pt;
+    TO v[PT];
+    TO tot = (TO)0;
+#pragma unroll
+    for (int j = 0; j < PT; j++) {
+        const int i = b + j;
+        v[j] = (j < pt && i < n) ? (TO)in[i] : (TO)0;
+        const TO x = v[j];
+        v[j] = tot;  // exclusive within the thread
+        tot += x;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    TO x = tot;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const TO t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += t;
+    }
+    TO ex = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) ex = (TO)0;
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        TO y = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const TO t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= d) y += t;
+        }
+        TO e = __shfl_up_sync(0xffffffffu, y, 1);
+        if (lane == 0) e = (TO)0;
+        warp_tot[lane] = e;  // exclusive over warps
+        if (lane == 31) out[n] = y;
+    }
+    __syncthreads();
+    const TO base = warp_tot[w] + ex;
+#pragma unroll
+    for (int j = 0; j < PT; j++) {
+        const int i = b + j;
+        if (j < pt && i < n) out[i] = base + v[j];
+    }
+}
+
 // kernel launches of one scan of n elements and of one z sort of N particles
 int qem_scan_launches(int n);
 // whether the cell build of N particles in ncell cells runs as one one-block kernel

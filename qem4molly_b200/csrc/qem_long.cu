@@ -63,11 +63,10 @@ struct LM<double> {
 // wk, esc: the force and energy weights of every k (random batch, sum_K / P
 // folded in); with per-k weights kwt (exact k-sum) wk = kwt / wden and
 // esc = -kwt / eden instead
-__global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
-                         double wk, double esc, const double *__restrict__ kwt, double wden, double eden)
+__device__ __forceinline__ void kconst_one(int m, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz,
+                                           double g12, double wk, double esc, const double *__restrict__ kwt,
+                                           double wden, double eden)
 {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= P) return;
     const double kx = kin[3 * m], ky = kin[3 * m + 1], k = kin[3 * m + 2];
     KConst K;
     K.kx_2pi = kx / (2.0 * QEM_PI);
@@ -80,6 +79,13 @@ __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restri
     K.wk = kwt ? kwt[m] / wden : wk;
     K.ek = (kwt ? -kwt[m] / eden : esc) / k;
     kc[m] = K;
+}
+
+__global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
+                         double wk, double esc, const double *__restrict__ kwt, double wden, double eden)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < P) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden);
 }
 
 // z-ordered SoA copy of the particles
@@ -96,6 +102,45 @@ __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__r
     zhf[m] = (float)(p.z - h);
     qd[m] = p.w;
     qf[m] = (float)p.w;
+}
+
+// Stage 0 before the totals for a small system without energy, in one
+// block: the z-ordered gather, the scan of q, the k = 0 force and the per-k
+// constants -- the same arithmetic as k_zgather, the one-block scan, k_k0
+// and k_kconst.
+constexpr int LONG_PREP_SMALL = 8192;
+
+__global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *__restrict__ pos,
+                                                          const int *__restrict__ zperm, double h,
+                                                          double *__restrict__ zx, double *__restrict__ zy,
+                                                          float *__restrict__ zhf, double *__restrict__ zhd,
+                                                          float *__restrict__ qf, double *__restrict__ qd,
+                                                          double *__restrict__ qscan, double fscale,
+                                                          double *__restrict__ k0, int P,
+                                                          const double *__restrict__ kin, KConst *__restrict__ kc,
+                                                          double Lz, double g12, double wk, double esc,
+                                                          const double *__restrict__ kwt, double wden, double eden)
+{
+    __shared__ double warp_tot[32];
+    for (int m = threadIdx.x; m < P; m += 1024) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden);
+    for (int m = threadIdx.x; m < N; m += 1024) {
+        const double4 p = pos[zperm[m]];
+        zx[m] = p.x;
+        zy[m] = p.y;
+        zhd[m] = p.z - h;
+        zhf[m] = (float)(p.z - h);
+        qd[m] = p.w;
+        qf[m] = (float)p.w;
+    }
+    __syncthreads();
+    qem_block_scan_excl_small<double, double>(qd, qscan, N, warp_tot);
+    __syncthreads();
+    const double tot = qscan[N];
+    for (int m = threadIdx.x; m < N; m += 1024) {
+        const double q = qd[m], below = qscan[m];
+        const double above = (tot - below) - q;
+        k0[m] = q * (below - above) * fscale;
+    }
 }
 
 // k = 0 term (Force_long.jl:130-161, Energy_long_range_njit.py:25-44)
@@ -1074,6 +1119,29 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
 {
     (void)status;
     if (N <= 0) return cudaSuccess;
+    if (stage == 0 && !energy && N <= LONG_PREP_SMALL) {
+        const double h = 0.5 * Lz;
+        const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
+        const double wk = P > 0 ? (sum_K / P) / (Lx * Ly * eps0) : 0.0;
+        const double esc = P > 0 ? -(sum_K / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
+        k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, b.qscan, fscale,
+                                             b.k0, P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
+                                             2.0 * eps0 * Lx * Ly);
+        if (P > 0) {
+            dim3 gt(nch, nblk(P, KPB));
+            if (precision == QEM_FP64)
+                k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
+            else
+                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
+            if (precision == QEM_FP64)
+                k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
+                                                           (KForce<double> *)b.kf);
+            else
+                k_lscan<float><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, (float *)b.off, b.Utot, b.kc, g1, g2,
+                                                          b.Eks, (KForce<float> *)b.kf);
+        }
+        return cudaGetLastError();
+    }
     if (stage == 0) {
         const double h = 0.5 * Lz;
         k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd);

@@ -32,7 +32,7 @@ def test_replays_equal_the_ordinary_call(prec):
         e.forces_device(x, q, F)
         assert np.array_equal(F.cpu().numpy(), ref)
         launches.append(e.counts()["launches"])
-    assert len(set(launches)) == 1 and launches[0] > 20  # a replay runs the recorded kernels
+    assert len(set(launches)) == 1 and launches[0] > 10  # a replay runs the recorded kernels
 
 
 def test_replay_follows_coordinates_kset_and_buffers():
