@@ -253,22 +253,20 @@ qem_status qem_get_timings(const qem_handle *h, double *ms, int32_t cap, int32_t
 qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
 
 /* Long-range forces with no device allocation.  No counterpart in the
- * reference: it serves callers that must not call cudaMalloc (code running
- * during CUDA-graph stream capture, hosts that own all device memory in their
- * own pool, real-time loops).  Same result as qem_long_forces for the same
- * k-set: F (3N, overwritten) = Molly.forces(::QEM_long) with the rows k3
- * (P x (kx, ky, k), host memory) and normaliser sum_K.  xyz, q and F are
- * device memory of device p->device; work is ordered on `stream`.  Outside a
- * stream capture the call synchronises the stream before returning and
- * reports non-finite inputs; while `stream` is being captured it only
- * enqueues its work (no read-back), so the call can be recorded in a graph;
- * k3 must then be page-locked host memory (pageable copies cannot be
- * captured).  Scratch lives in one fixed
- * QEM_NOALLOC_SCRATCH_BYTES device array inside libqem.so that every GPU
+ * reference: it serves callers that must not call cudaMalloc (a host framework
+ * that owns all device memory in its own pool, a real-time loop that must not
+ * enter the CUDA allocator, whose cost and implicit synchronisation are
+ * unbounded).  Same result as qem_long_forces for the same k-set: F (3N,
+ * overwritten) = Molly.forces(::QEM_long) with the rows k3 (P x (kx, ky, k),
+ * host memory) and normaliser sum_K.  xyz, q and F are device memory of device
+ * p->device; work is ordered on `stream`, which the call synchronises before
+ * returning (non-finite inputs give QEM_ERR_NONFINITE).  Scratch lives in one
+ * fixed QEM_NOALLOC_SCRATCH_BYTES device array inside libqem.so that every GPU
  * loading the library holds until exit; larger N or P are rejected with
- * QEM_ERR_ARG.  The first call on a device looks up that array's address and
- * should precede any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * QEM_ERR_ARG.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current.  All calls share the
+ * array, which keeps the last call's contents: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 #define QEM_NOALLOC_MAX_N 32768
 #define QEM_NOALLOC_MAX_P 512
 #define QEM_NOALLOC_SCRATCH_BYTES (8u << 20)

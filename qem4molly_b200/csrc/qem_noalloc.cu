@@ -1,9 +1,10 @@
 // qem_noalloc.cu -- long-range (random-batch k-space) forces that allocate
 // no device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a stream is being
-// captured into a CUDA graph, host code that hands all device memory to its
-// own pool, or real-time loops that must not touch the allocator.  For them
+// Some callers cannot call cudaMalloc: a host framework that hands all device
+// memory to its own pool (a foreign allocation would fragment it or exceed
+// its budget), or a real-time loop that must not enter the CUDA allocator,
+// whose cost and implicit synchronisation are unbounded.  For them
 // qem_long_forces_noalloc runs the same kernels as qem_long_forces, with all
 // of their scratch (packed particles, z order, z-ordered copies, per-k
 // constants, chunk totals and offsets, status word) carved out of one
@@ -12,11 +13,8 @@
 //
 // Host code never dereferences the array's name: on the first call on a
 // device (that device current) cudaGetSymbolAddress gives its device address,
-// which is cached per device and passed to the kernels.  That first call
-// should therefore come before any stream capture.  Outside a capture the
-// call synchronises its stream and reports non-finite inputs; while the
-// stream is being captured it only enqueues its work, and the k-set copy
-// then needs page-locked host memory.  All calls share the
+// which is cached per device and passed to the kernels.  The call
+// synchronises its stream and reports non-finite inputs.  All calls share the
 // array, so calls that overlap on the GPU (different streams, host threads)
 // race: serialise them.  Nothing in the array needs to start at zero except
 // the status word, which is cleared on every call.
@@ -151,10 +149,6 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
         e = qem_launch_long(p->precision, false, N, P, pos, zperm, b, p->Lx, p->Ly, p->Lz, p->gamma_down, p->gamma_up,
                             p->eps_0, sum_K, F, nch, status, s, stage);
     if (e != cudaSuccess) return QEM_ERR_CUDA;
-    // under stream capture the call only enqueues its work: no host read-back
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return QEM_ERR_CUDA;
-    if (cap != cudaStreamCaptureStatusNone) return QEM_OK;
     unsigned host_status = 0;
     if (cudaMemcpyAsync(&host_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)

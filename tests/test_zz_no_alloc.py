@@ -1,9 +1,10 @@
 """qem_long_forces_noalloc: the long-range forces for callers that cannot call
-cudaMalloc (e.g. during CUDA-graph stream capture, or when a host framework
-owns all device memory).  Its scratch is a fixed array inside libqem.so, so it
-is checked here against the allocating entry point (qem_long_forces through a
-handle) on the same system and k-set, twice in a row, since every call
-reuses the same scratch.  This file is collected last on purpose."""
+cudaMalloc (a host framework that owns all device memory in its own pool, or
+a real-time loop that must not enter the CUDA allocator).  Its scratch is a
+fixed array inside libqem.so, so it is checked here against the allocating
+entry point (qem_long_forces through a handle) on the same system and k-set,
+twice in a row, since every call reuses the same scratch.  This file is
+collected last on purpose."""
 import ctypes as C
 
 import numpy as np
@@ -57,36 +58,3 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                        kbig.ctypes.data_as(C.POINTER(C.c_double)), 1.0, C.c_void_p(F.data_ptr()),
                                        None) == 1
 
-
-def test_noalloc_records_into_a_cuda_graph():
-    """Under stream capture the call only enqueues work (no read-back), so it
-    can be recorded once and replayed; k3 is page-locked host memory, as
-    copies from pageable memory cannot be captured."""
-    import torch
-
-    cfg = W.config2(N=20_000, seed=99)
-    e = W.engine_for(cfg, "fp64", seed=11)
-    k3, sK = e.get_kset()
-    F_ref = e.forces(cfg["xyz"], cfg["q"], terms=L.QEM_TERM_LONG)
-    lib = L.load()
-    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device="cuda")
-    q = torch.tensor(cfg["q"], dtype=torch.float64, device="cuda")
-    k3p = torch.tensor(np.ascontiguousarray(k3), dtype=torch.float64).pin_memory()
-    F = torch.full_like(x, float("nan"))
-
-    def call():
-        s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-        return lib.qem_long_forces_noalloc(C.byref(e.params), cfg["N"], C.c_void_p(x.data_ptr()),
-                                           C.c_void_p(q.data_ptr()), k3p.shape[0],
-                                           C.cast(C.c_void_p(k3p.data_ptr()), C.POINTER(C.c_double)), sK,
-                                           C.c_void_p(F.data_ptr()), s)
-
-    assert call() == 0  # outside capture first (looks up the scratch address)
-    torch.cuda.synchronize()
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        assert call() == 0
-    F.fill_(float("nan"))
-    g.replay()
-    torch.cuda.synchronize()
-    assert W.rel_err(F.cpu().numpy(), F_ref)[0] <= 1e-12
