@@ -787,6 +787,30 @@ static qem_handle::GraphKey graph_key(const qem_handle *h, int N, const double *
 }
 
 // replays (recording first if needed); fallback = true asks for an ordinary call
+// The long-range chain (z sort, scans, per-k totals, force pass) is a row of
+// short, latency-bound kernels on the side stream, while the pair kernel on
+// the caller's stream fills every SM with long-running blocks.  At equal
+// priority the long chain's blocks queue behind pair blocks and it ends last;
+// on a high-priority stream each of its blocks takes the next SM slot that a
+// pair block frees, so both chains finish together.  A recorded graph keeps
+// those priorities (kernel nodes copy the capturing stream's priority) when it
+// is instantiated with cudaGraphInstantiateFlagUseNodePriority.
+#ifndef QEM_LONG_PRIORITY
+#define QEM_LONG_PRIORITY 1
+#endif
+static cudaError_t create_side_stream(cudaStream_t *s)
+{
+    int least = 0, greatest = 0;
+    if (QEM_LONG_PRIORITY && cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess)
+        return cudaStreamCreateWithPriority(s, cudaStreamNonBlocking, greatest);
+    cudaGetLastError();
+    return cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+}
+static unsigned long long graph_instantiate_flags()
+{
+    return QEM_LONG_PRIORITY ? (unsigned long long)cudaGraphInstantiateFlagUseNodePriority : 0ull;
+}
+
 static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const double *xyz, const double *q,
                             double *F, uint32_t terms, cudaStream_t s, bool &fallback)
 {
@@ -821,7 +845,7 @@ static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const 
         const cudaError_t ec = cudaStreamEndCapture(h->gcap, &g);
         cudaGraphExec_t ex = nullptr;
         const bool ok = st == QEM_OK && ce == cudaSuccess && ec == cudaSuccess && g &&
-                        cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+                        cudaGraphInstantiateWithFlags(&ex, g, graph_instantiate_flags()) == cudaSuccess;
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
         if (!ok || !(graph_key(h, N, xyz, q, F, terms, k.mem) == k)) {
@@ -943,7 +967,7 @@ qem_status qem_create(const qem_params *p, qem_handle **out)
     if (cudaMallocHost(&h->h_status, sizeof(unsigned)) != cudaSuccess ||
         cudaMallocHost(&h->h_E, sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&h->h_np, sizeof(int64_t)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
+        create_side_stream(&h->s2) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         qem_destroy(h);
