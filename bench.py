@@ -288,7 +288,7 @@ def run_ours(args):
     roofline = {"bound": "fp32", "kernel": "k_short_pair<FP32>", "achieved": achieved, "peak": fp32_peak.value,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak.value if fp32_peak.value else None,
                 "traffic": traffic,
-                "peak_source": "measured in this run (qem_measure_peaks FMA chain); MEASURED_PEAKS.json has no FP32 figure",
+                "peak_source": "measured in this run (qem_measure_peaks: the larger of scalar and packed FP32x2 FMA chains); MEASURED_PEAKS.json has no FP32 figure",
                 "work_model": f"{FLOPS_PER_PAIR_NODE} FP32 flops + {SFU_PER_PAIR_NODE} MUFU ops per pair-node; "
                               f"{Np} pairs x 8 x {cfg['N_t']} nodes per launch",
                 "mufu": {"achieved": nodes * SFU_PER_PAIR_NODE / t_pair / 1e12, "peak": mufu_peak.value,

@@ -332,8 +332,9 @@ qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step);
 /* Library identity (version string and the compiled CUDA architecture). */
 const char *qem_version(void);
 
-/* Measured FP32 FMA throughput (TFLOP/s, 2 flops per FMA) and MUFU ex2
- * throughput (Tops/s) of `device`: the roofline denominators of the QEM
+/* Measured FP32 FMA throughput (TFLOP/s, 2 flops per FMA; the larger of
+ * scalar and packed FP32x2 FMA chains) and MUFU ex2 throughput (Tops/s) of
+ * `device`: the roofline denominators of the QEM
  * kernels, which are bound by those two pipes.  Diagnostic; no reference
  * counterpart. */
 qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, double *mufu_tops);

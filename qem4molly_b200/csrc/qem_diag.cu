@@ -4,7 +4,7 @@
 // by HBM or tensor cores, so their roofline needs the device's own FP32 FMA
 // and MUFU rates: these kernels measure them with CUDA events (dependent-free
 // chains of 8 independent accumulators per thread, enough warps to fill every
-// SM).
+// SM); the FP32 rate is the larger of scalar and packed FP32x2 FMA chains.
 #include <algorithm>
 
 #include "qem_internal.cuh"
@@ -25,6 +25,27 @@ __global__ void k_fma_peak(int iters, float seed, float *out)
     }
     const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
     if (s == 1234.5f) out[0] = s;  // keeps the chain alive
+}
+
+// the same chains as packed FP32x2 instructions (sm_100: one instruction
+// issues two FMAs), so that the FP32 denominator also covers kernels that use them
+__global__ void k_fma2_peak(int iters, float seed, float *out)
+{
+    float2 a[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = make_float2(seed + threadIdx.x + j, seed + threadIdx.x + j + 0.5f);
+    const float2 m = make_float2(0.9999999f, 0.9999999f), c = make_float2(1e-7f, 1e-7f);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) a[j] = __ffma2_rn(a[j], m, c);
+        }
+    }
+    float s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) s += a[j].x + a[j].y;
+    if (s == 1234.5f) out[0] = s;
 }
 
 __global__ void k_mufu_peak(int iters, float seed, float *out)
@@ -57,7 +78,7 @@ extern "C" qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, dou
     cudaEventCreate(&b);
     const int blocks = prop.multiProcessorCount * 8, threads = 256;
     const int it_fma = 4096, it_mufu = 1024;
-    float best_f = 1e30f, best_m = 1e30f;
+    float best_f = 1e30f, best_f2 = 1e30f, best_m = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
         float t = 0;
         cudaEventRecord(a);
@@ -66,6 +87,12 @@ extern "C" qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, dou
         cudaEventSynchronize(b);
         cudaEventElapsedTime(&t, a, b);
         if (rep > 0) best_f = std::min(best_f, t);
+        cudaEventRecord(a);
+        k_fma2_peak<<<blocks, threads>>>(it_fma, 1.0f, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t, a, b);
+        if (rep > 0) best_f2 = std::min(best_f2, t);
         cudaEventRecord(a);
         k_mufu_peak<<<blocks, threads>>>(it_mufu, 1.0f, d);
         cudaEventRecord(b);
@@ -79,7 +106,10 @@ extern "C" qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, dou
     cudaFree(d);
     if (e != cudaSuccess) return QEM_ERR_CUDA;
     const double nthr = (double)blocks * threads;
-    if (fp32_tflops) *fp32_tflops = 2.0 * nthr * it_fma * 16 * 8 / (best_f * 1e-3) * 1e-12;
+    // scalar: 16 x 8 FMAs per iteration; packed: 8 x 8 instructions of two FMAs
+    const double f1 = 2.0 * nthr * it_fma * 16 * 8 / (best_f * 1e-3) * 1e-12;
+    const double f2 = 2.0 * nthr * it_fma * 8 * 8 * 2 / (best_f2 * 1e-3) * 1e-12;
+    if (fp32_tflops) *fp32_tflops = std::max(f1, f2);
     if (mufu_tops) *mufu_tops = nthr * it_mufu * 16 * 4 / (best_m * 1e-3) * 1e-12;
     return QEM_OK;
 }
