@@ -50,7 +50,7 @@ constexpr int PAIR_BLOCK = QEM_PAIR_BLOCK;  // pairs per block, ordered by rho i
 #define QEM_PAIR_MINB 4
 #endif
 #ifndef QEM_NODE_UNROLL
-#define QEM_NODE_UNROLL 2
+#define QEM_NODE_UNROLL 3
 #endif
 constexpr int NODE_UNROLL = QEM_NODE_UNROLL;
 
