@@ -39,6 +39,9 @@ constexpr int LCH = LT * PPT;   // particles per chunk
 constexpr int NW = LT / 32;     // warps per block
 constexpr int KPB = 16;         // k-vectors per block in the totals pass
 constexpr int LKB = 8;          // k-vectors per FP32 accumulation batch of the force pass
+#ifndef QEM_LF_WAVES_PCT
+#define QEM_LF_WAVES_PCT 100
+#endif
 #ifndef QEM_LF_MINB
 #define QEM_LF_MINB 8
 #endif
@@ -1103,9 +1106,10 @@ static int sm_count()
 
 int qem_long_ksplit(int nch, int P, int max_ks)
 {
-    // as many whole k-slices of the nch chunks as fit in one wave of resident
-    // force-pass blocks, each slice with at least two k groups of LKB vectors
-    int ks = sm_count() * LF_MINB / (nch > 0 ? nch : 1);
+    // as many whole k-slices of the nch chunks as fit in QEM_LF_WAVES_PCT / 100
+    // waves of resident force-pass blocks, each slice with at least two k
+    // groups of LKB vectors
+    int ks = (int)((int64_t)sm_count() * LF_MINB * QEM_LF_WAVES_PCT / (100 * (int64_t)(nch > 0 ? nch : 1)));
     ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
     const int pm = P > 2 * LKB ? P / (2 * LKB) : 1;
     return ks < pm ? ks : pm;
