@@ -667,21 +667,19 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         mk_pair = h->prof.mark(s);
     }
     if (do_short || do_lj) {
+        if (concurrent) {  // join: the long range ran on the side stream into Flong, which the gather adds
+            CU(cudaEventRecord(h->ev_join, h->s2));
+            CU(cudaStreamWaitEvent(s, h->ev_join, 0));
+        }
         CU(qem_launch_short_gather(prec, want_E, do_short, do_lj, N, ptr<double4>(h->pos), ptr<int>(h->pos_of),
                                    ptr<int64_t>(h->poff), ptr<double4>(h->R), ptr<double>(h->Upair),
                                    ptr<int64_t>(h->in_off), ptr<int>(h->in_list), h->pair_cap, h->sc, F_d, Ep,
-                                   st, s));
+                                   st, s, concurrent ? ptr<double>(h->Flong) : nullptr));
         launches++;
     } else if (!do_long) {  // (a long-only call has already zeroed F_d in front of its kernels)
         CU(cudaMemsetAsync(F_d, 0, sizeof(double) * 3 * N, s));
     }
     mk_gather = h->prof.mark(s);
-    if (concurrent) {  // join: the long range ran on the side stream into Flong
-        CU(cudaEventRecord(h->ev_join, h->s2));
-        CU(cudaStreamWaitEvent(s, h->ev_join, 0));
-        CU(qem_launch_add3(3 * N, ptr<double>(h->Flong), F_d, s));
-        launches++;
-    }
     if (want_E) {
         const int nE = nbS + ks * nch + nb0 + (do_long ? (h->has_kset ? h->P : 0) : 0);
         CU(qem_launch_reduce_sum(Ep, nE, ptr<double>(h->Eout), s));

@@ -165,7 +165,7 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
                                     const double *Upair, const int64_t *in_off, const int *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
-                                    cudaStream_t s);
+                                    cudaStream_t s, const double *Fadd = nullptr);
 
 // stable z order (equal z by ascending index; by descending index with rev_ties)
 cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
@@ -247,8 +247,6 @@ struct LongAdjBuffers {
 cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffers &b, const LongAdjBuffers &a,
                                 double Lx, double Ly, double Lz, double g1, double g2, double eps0, const double *gF,
                                 double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s);
-// out[i] += a[i] for n doubles
-cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // device helpers

@@ -676,12 +676,6 @@ __global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, cons
     F3[3 * i + 2] += fz + k0[m];
 }
 
-__global__ void k_add(int n, const double *__restrict__ a, double *__restrict__ out)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] += a[i];
-}
-
 __global__ void k_reduce_sum(const double *__restrict__ in, int n, double *__restrict__ out)
 {
     // single block, fixed order: deterministic
@@ -1207,13 +1201,6 @@ cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaSt
 {
     if (n <= 0) return cudaSuccess;
     k_scale_vec<<<nblk(n, 256), 256, 0, s>>>(n, a, x, y);
-    return cudaGetLastError();
-}
-
-cudaError_t qem_launch_add3(int n, const double *a, double *out, cudaStream_t s)
-{
-    if (n <= 0) return cudaSuccess;
-    k_add<<<nblk(n, 256), 256, 0, s>>>(n, a, out);
     return cudaGetLastError();
 }
 

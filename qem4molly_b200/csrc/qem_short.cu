@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
                                                        const int *__restrict__ in_list, int64_t cap,
                                                        const ShortConsts c, double *__restrict__ F3,
                                                        double *__restrict__ Epart, unsigned *status, int do_short,
-                                                       int do_lj)
+                                                       int do_lj, const double *__restrict__ Fadd)
 {
     __shared__ double red[256 / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -450,6 +450,11 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
                     Fz += c.wall_dir[w] * ((24.0 * c.wall_eps[w] * invr2) * (2.0 * s6 * s6 - s6));
                 }
             }
+        }
+        if (Fadd) {  // the long-range forces of a concurrent long-range pass, added last
+            Fx += Fadd[3 * i];
+            Fy += Fadd[3 * i + 1];
+            Fz += Fadd[3 * i + 2];
         }
         F3[3 * i] = Fx;
         F3[3 * i + 1] = Fy;
@@ -492,7 +497,7 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
                                     const double4 *pos, const int *pos_of, const int64_t *poff, const double4 *R,
                                     const double *Upair, const int64_t *in_off, const int *in_list, int64_t cap,
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
-                                    cudaStream_t s)
+                                    cudaStream_t s, const double *Fadd)
 {
     if (N <= 0) return cudaSuccess;
     const int B = 256;
@@ -501,17 +506,17 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
     if (precision == QEM_FP64) {
         if (energy)
             k_short_gather<QEM_FP64, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap, c,
-                                                            F3, Epart, status, ds, dl);
+                                                            F3, Epart, status, ds, dl, Fadd);
         else
             k_short_gather<QEM_FP64, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap, c,
-                                                             F3, Epart, status, ds, dl);
+                                                             F3, Epart, status, ds, dl, Fadd);
     } else {
         if (energy)
             k_short_gather<QEM_FP32_FIX, true><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list, cap,
-                                                                c, F3, Epart, status, ds, dl);
+                                                                c, F3, Epart, status, ds, dl, Fadd);
         else
             k_short_gather<QEM_FP32_FIX, false><<<G, B, 0, s>>>(N, pos, pos_of, poff, R, Upair, in_off, in_list,
-                                                                 cap, c, F3, Epart, status, ds, dl);
+                                                                 cap, c, F3, Epart, status, ds, dl, Fadd);
     }
     return cudaGetLastError();
 }
