@@ -157,19 +157,24 @@ __global__ void k_scan_add(T *__restrict__ out, int n, const T *__restrict__ bsu
     if (i == 0) out[n] = bsum[(n + SCAN_BLOCK - 1) / SCAN_BLOCK];
 }
 
-// One-block exclusive scan for n <= SCAN_SMALL_MAX (one launch instead of
-// three; the many-small-systems batch is launch-bound): thread t owns
-// elements [t pt, (t + 1) pt), pt = ceil(n / SCAN_BLOCK) <= SCAN_SMALL_PT,
-// summed in order; the thread totals are scanned exclusively without an
-// "inclusive minus own" step; out[n] = total.
+// One-block exclusive scan for small n (one launch instead of three; the
+// many-small-systems batch and the binning chain in front of the pair kernel
+// are launch-bound): thread t owns elements [t pt, (t + 1) pt),
+// pt = ceil(n / SCAN_BLOCK) <= PT, summed in order; the thread totals are
+// scanned exclusively without an "inclusive minus own" step; out[n] = total.
+// Integer scans (exact in any order) take it up to 16 elements per thread,
+// e.g. the 10^4 cells of a 1000 x 1000 slab with r_c = 10; FP64 scans keep
+// 8, so their summation order at a given n is unchanged.
 constexpr int SCAN_SMALL_PT = 8;
 constexpr int SCAN_SMALL_MAX = SCAN_BLOCK * SCAN_SMALL_PT;
+constexpr int SCAN_SMALL_PT_INT = 16;
+constexpr int SCAN_SMALL_MAX_INT = SCAN_BLOCK * SCAN_SMALL_PT_INT;
 
-template <typename TI, typename TO>
+template <typename TI, typename TO, int PT>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const TI *__restrict__ in, TO *__restrict__ out, int n)
 {
     __shared__ TO warp_tot[SCAN_BLOCK / 32];
-    qem_block_scan_excl_small<TI, TO>(in, out, n, warp_tot);
+    qem_block_scan_excl_small<TI, TO, PT>(in, out, n, warp_tot);
 }
 
 // ---------------------------------------------------------------------------
@@ -817,8 +822,8 @@ inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 template <typename TI, typename TO>
 cudaError_t scan_impl(const TI *in, TO *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
-    if (n <= SCAN_SMALL_MAX) {
-        k_scan_small<TI, TO><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
+    if (n <= SCAN_SMALL_MAX_INT) {
+        k_scan_small<TI, TO, SCAN_SMALL_PT_INT><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
         return cudaGetLastError();
     }
     int nb = nblk(n, SCAN_BLOCK);
@@ -835,7 +840,8 @@ cudaError_t scan_impl(const TI *in, TO *out, int n, void *tmp, size_t tmp_bytes,
 
 size_t qem_scan_tmp_bytes(int n) { return sizeof(double) * (size_t)(nblk(n, SCAN_BLOCK) + 2); }
 
-int qem_scan_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
+int qem_scan_launches(int n) { return n <= SCAN_SMALL_MAX_INT ? 1 : 3; }
+int qem_scan_f64_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
 
 int qem_zsort_launches(int N)
 {
@@ -853,7 +859,7 @@ cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, s
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
     if (n <= SCAN_SMALL_MAX) {
-        k_scan_small<double, double><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
+        k_scan_small<double, double, SCAN_SMALL_PT><<<1, SCAN_BLOCK, 0, s>>>(in, out, n < 0 ? 0 : n);
         return cudaGetLastError();
     }
     int nb = nblk(n, SCAN_BLOCK);

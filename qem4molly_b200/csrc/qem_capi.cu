@@ -621,7 +621,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         // z sort, zgather + q scan + k = 0 term, per-k constants + totals + scan, force pass + final
         auto long_launches = [&](bool energy_pass) {
             return qem_zsort_launches(N) +
-                   (!energy_pass && N <= 8192 ? 1 + (Pk > 0 ? 2 : 0) : 2 + qem_scan_launches(N) + (Pk > 0 ? 3 : 0)) +
+                   (!energy_pass && N <= 8192 ? 1 + (Pk > 0 ? 2 : 0) : 2 + qem_scan_f64_launches(N) + (Pk > 0 ? 3 : 0)) +
                    2;
         };
         launches += long_launches(want_E);

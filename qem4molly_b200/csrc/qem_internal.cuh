@@ -98,15 +98,15 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
-// One-block exclusive scan of n <= 8192 values by the calling block of 1024
-// threads (thread t owns elements [t pt, (t + 1) pt), pt = ceil(n / 1024),
+// One-block exclusive scan of n <= PT * 1024 values by the calling block of
+// 1024 threads (thread t owns elements [t pt, (t + 1) pt), pt = ceil(n / 1024),
 // summed in order; the thread totals are scanned exclusively without an
 // "inclusive minus own" step); out[n] = total.  warp_tot: 32 entries of
-// shared memory.  Every block-wide caller gets the same arithmetic.
-template <typename TI, typename TO>
+// shared memory.  Every block-wide caller gets the same arithmetic (PT only
+// bounds the registers).
+template <typename TI, typename TO, int PT = 8>
 __device__ void qem_block_scan_excl_small(const TI *__restrict__ in, TO *__restrict__ out, int n, TO *warp_tot)
 {
-    constexpr int PT = 8;
     const int pt = (n + 1023) / 1024;
     const int b = threadIdx.x * pt;
     TO v[PT];
@@ -151,8 +151,10 @@ __device__ void qem_block_scan_excl_small(const TI *__restrict__ in, TO *__restr
     }
 }
 
-// kernel launches of one scan of n elements and of one z sort of N particles
+// kernel launches of one integer scan of n elements, of one FP64 scan
+// (qem_scan_f64_excl) and of one z sort of N particles
 int qem_scan_launches(int n);
+int qem_scan_f64_launches(int n);
 // whether the cell build of N particles in ncell cells runs as one one-block kernel
 bool qem_cells_small(int N, int ncell);
 int qem_zsort_launches(int N);
