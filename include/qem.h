@@ -81,9 +81,11 @@ typedef int32_t qem_status;
 
 /* precision */
 #define QEM_FP64 0      /* plain FP64 everywhere                                           */
-#define QEM_FP32_FIX 1  /* FP32 quadrature and structure sums (compensated), FP64 k-space
+#define QEM_FP32_FIX 1  /* FP32 quadrature nodes and structure sums, FP64 k-space
                            denominators and phases, cancellation-free short-range
-                           denominators, FP64 final force/energy reductions              */
+                           denominators; FP32 partial sums are short (one quadrature
+                           interval, one chunk, a batch of 8 k-vectors) and are added
+                           into FP64, as are all final force/energy reductions        */
 
 /* terms (bit mask) */
 #define QEM_TERM_SHORT 0x1u
@@ -256,17 +258,19 @@ qem_status qem_get_counts(const qem_handle *h, int64_t *counts, int32_t cap);
  * reference: it serves callers that must not call cudaMalloc (a host framework
  * that owns all device memory in its own pool, a real-time loop that must not
  * enter the CUDA allocator, whose cost and implicit synchronisation are
- * unbounded).  Same result as qem_long_forces for the same k-set: F (3N,
- * overwritten) = Molly.forces(::QEM_long) with the rows k3 (P x (kx, ky, k),
- * host memory) and normaliser sum_K.  xyz, q and F are device memory of device
- * p->device; work is ordered on `stream`, which the call synchronises before
- * returning (non-finite inputs give QEM_ERR_NONFINITE).  Scratch lives in one
- * fixed QEM_NOALLOC_SCRATCH_BYTES device array inside libqem.so that every GPU
+ * unbounded).  F (3N, overwritten) is the same as qem_long_forces gives on a
+ * handle with the same parameters, fed the rows k3 (P x (kx, ky, k), host
+ * memory) and normaliser sum_K by qem_set_kset.  xyz, q and F are device
+ * memory of device p->device; work is ordered on `stream`, which the call
+ * synchronises before returning (non-finite inputs give QEM_ERR_NONFINITE; in
+ * QEM_FP32_FIX a particle with max(k) |z - L_z / 2| > 60, far outside the
+ * slab, gives QEM_ERR_RANGE).  Scratch lives in one fixed
+ * QEM_NOALLOC_SCRATCH_BYTES device array inside libqem.so that every GPU
  * loading the library holds until exit; larger N or P are rejected with
- * QEM_ERR_ARG.  The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current.  All calls share the
- * array, which keeps the last call's contents: calls that overlap on the GPU
- * race and must be serialised by the caller. */
+ * QEM_ERR_ARG.  Every call looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current.  All calls share the array,
+ * which keeps the last call's contents: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 #define QEM_NOALLOC_MAX_N 32768
 #define QEM_NOALLOC_MAX_P 512
 #define QEM_NOALLOC_SCRATCH_BYTES (8u << 20)

@@ -209,6 +209,10 @@ static const char *status_str(qem_status s)
     return "unknown status";
 }
 
+// the FP32 k-space path's device check (k_zgather): e^{+-k (z - Lz/2)} would
+// leave FP32 range for a particle far outside the slab
+static const char *range_msg = "FP32 k-space path: max(k) * |z - L_z / 2| > 60 for some particle (use QEM_FP64)";
+
 static qem_status fail(qem_handle *h, qem_status s, const std::string &msg)
 {
     if (h) h->err = std::string(status_str(s)) + ": " + msg;
@@ -595,6 +599,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
             if (ls != QEM_OK) return ls;
         }
         b.skip_k0 = h->shard_rank != 0;
+        b.zlim = prec == QEM_FP32_FIX && Pk > 0 ? qem_fp32_zlim(h->kmax) : 0.0;
         if (concurrent) {  // fork after pack (positions) and the energy-partial clear
             CU(cudaEventRecord(h->ev_fork, s));
             CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
@@ -722,6 +727,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     const unsigned stv = *h->h_status;
     if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
     if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    if (stv & QEM_ST_RANGE) return fail(h, QEM_ERR_RANGE, range_msg);
     if (want_E) *energy = *h->h_E;
     h->err.clear();
     return QEM_OK;
@@ -885,6 +891,7 @@ static qem_status run_graph(qem_handle *h, const qem_handle::GraphKey &k, const 
     h->counts[3] = h->glaunches;  // the recorded kernels, replayed by one graph launch
     if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
     if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    if (stv & QEM_ST_RANGE) return fail(h, QEM_ERR_RANGE, range_msg);
     h->err.clear();
     return QEM_OK;
 }
@@ -1515,6 +1522,7 @@ qem_status qem_status_check(qem_handle *h, cudaStream_t s)
     if (stv & QEM_ST_OVERFLOW) return fail(h, QEM_ERR_NB_OVERFLOW, "pair list outgrew its capacity in an asynchronous call");
     if (stv & QEM_ST_NONFINITE) return fail(h, QEM_ERR_NONFINITE, "NaN or Inf in coordinates or charges");
     if (stv & QEM_ST_OUT_OF_SLAB) return fail(h, QEM_ERR_OUT_OF_SLAB, "direction * (z - sub_pos) <= 0 for some particle");
+    if (stv & QEM_ST_RANGE) return fail(h, QEM_ERR_RANGE, range_msg);
     return QEM_OK;
 }
 

@@ -197,7 +197,12 @@ struct LongBuffers {
     size_t stmp_bytes;
     int skip_k0 = 0;      // 1: leave out the k = 0 term (sharded ranks other than 0)
     const double *kwt = nullptr;  // P per-k weights (exact k-sum); nullptr: sum_K / P for every k
+    double zlim = 0.0;    // FP32 path: largest |z - Lz/2| whose e^{+-k (z - Lz/2)} stays in FP32
+                          // range for every k (QEM_ST_RANGE beyond); 0: no check
 };
+// zlim of the FP32 k-space path for a k-set whose largest |k| is kmax:
+// e^{+-k (z - Lz/2)} <= e^{60}, so that sums over many particles stay finite
+inline double qem_fp32_zlim(double kmax) { return kmax > 0 ? 60.0 / kmax : 0.0; }
 // number of k slices for nch chunks and P k-vectors (at most max_ks); the
 // per-slice force partials take ks x N x 3 doubles, and ks x nch stays near
 // one wave of force-pass blocks, so they stay below ~15 MB at any N
@@ -383,16 +388,4 @@ __device__ __forceinline__ float fast_rcp(float x)
     return r;
 }
 
-// Kahan-compensated FP32 accumulation
-struct KahanF {
-    float s, c;
-    __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
-    __device__ __forceinline__ void add(float v)
-    {
-        float y = v - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-};
 #endif

@@ -92,13 +92,22 @@ __global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restri
 }
 
 // z-ordered SoA copy of the particles
+// zlim > 0 (FP32 path): |z - h| must stay within zlim, so that e^{+-k (z - h)}
+// stays inside FP32 range for every k of the set; QEM_ST_RANGE otherwise
+__device__ __forceinline__ void zrange_check(double zh, double zlim, unsigned *status)
+{
+    if (zlim > 0.0 && !(fabs(zh) <= zlim)) atomicOr(status, QEM_ST_RANGE);
+}
+
 __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__restrict__ zperm, double h,
                           double *__restrict__ zx, double *__restrict__ zy, float *__restrict__ zhf,
-                          double *__restrict__ zhd, float *__restrict__ qf, double *__restrict__ qd)
+                          double *__restrict__ zhd, float *__restrict__ qf, double *__restrict__ qd, double zlim,
+                          unsigned *status)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= N) return;
     const double4 p = pos[zperm[m]];
+    zrange_check(p.z - h, zlim, status);
     zx[m] = p.x;
     zy[m] = p.y;
     zhd[m] = p.z - h;
@@ -122,12 +131,14 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
                                                           double *__restrict__ k0, int P,
                                                           const double *__restrict__ kin, KConst *__restrict__ kc,
                                                           double Lz, double g12, double wk, double esc,
-                                                          const double *__restrict__ kwt, double wden, double eden)
+                                                          const double *__restrict__ kwt, double wden, double eden,
+                                                          double zlim, unsigned *status)
 {
     __shared__ double warp_tot[32];
     for (int m = threadIdx.x; m < P; m += 1024) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden);
     for (int m = threadIdx.x; m < N; m += 1024) {
         const double4 p = pos[zperm[m]];
+        zrange_check(p.z - h, zlim, status);
         zx[m] = p.x;
         zy[m] = p.y;
         zhd[m] = p.z - h;
@@ -1115,8 +1126,8 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
                             const LongBuffers &b, double Lx, double Ly, double Lz, double g1, double g2, double eps0,
                             double sum_K, double *F3, int nch, unsigned *status, cudaStream_t s, int stage)
 {
-    (void)status;
     if (N <= 0) return cudaSuccess;
+    const double zlim = precision == QEM_FP64 ? 0.0 : b.zlim;
     if (stage == 0 && !energy && N <= LONG_PREP_SMALL) {
         const double h = 0.5 * Lz;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
@@ -1124,7 +1135,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const double esc = P > 0 ? -(sum_K / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
         k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, b.qscan, fscale,
                                              b.k0, P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                             2.0 * eps0 * Lx * Ly);
+                                             2.0 * eps0 * Lx * Ly, zlim, status);
         if (P > 0) {
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
@@ -1142,7 +1153,8 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     }
     if (stage == 0) {
         const double h = 0.5 * Lz;
-        k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd);
+        k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, zlim,
+                                               status);
         cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
         if (e != cudaSuccess) return e;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);

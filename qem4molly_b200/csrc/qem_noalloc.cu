@@ -11,15 +11,19 @@
 // file-scope __device__ array of QEM_NOALLOC_SCRATCH_BYTES.  Every GPU that
 // loads libqem.so holds that array until the process exits.
 //
-// Host code never dereferences the array's name: on the first call on a
-// device (that device current) cudaGetSymbolAddress gives its device address,
-// which is cached per device and passed to the kernels.  The call
-// synchronises its stream and reports non-finite inputs.  All calls share the
+// Host code never dereferences the array's name: on every call, with the
+// call's device current, cudaGetSymbolAddress gives its device address, which
+// is passed to the kernels.  The address is not cached: a host framework that
+// tears the primary context down and creates it again (or a
+// cudaDeviceReset) loads the module anew, and the array may then live
+// elsewhere.  The lookup costs little next to the call's own synchronisation.
+// The call synchronises its stream and reports non-finite inputs (and, in
+// FP32, particles so far outside the slab that e^{+-k (z - L_z/2)} would leave
+// FP32 range).  All calls share the
 // array, so calls that overlap on the GPU (different streams, host threads)
 // race: serialise them.  Nothing in the array needs to start at zero except
 // the status word, which is cleared on every call.
 #include <cstdio>
-#include <mutex>
 
 #include "qem_internal.cuh"
 
@@ -63,24 +67,18 @@ static_assert(NA_BYTES <= QEM_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[QEM_NOALLOC_SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
-unsigned char *g_scratch_addr[MAX_DEVICES] = {nullptr};
-std::mutex g_scratch_mu;
-
-// device address of g_noalloc_scratch on `dev` (which must be current)
-qem_status scratch_address(int dev, unsigned char **out)
+// device address of g_noalloc_scratch on the current device, looked up afresh
+// on every call (the module, and with it the array, is loaded again after a
+// context is destroyed and re-created)
+qem_status scratch_address(unsigned char **out)
 {
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) {
-            fprintf(stderr, "qem_long_forces_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
-            return QEM_ERR_CUDA;
-        }
-        g_scratch_addr[dev] = (unsigned char *)ptr;
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+        fprintf(stderr, "qem_long_forces_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+        return QEM_ERR_CUDA;
     }
-    *out = g_scratch_addr[dev];
+    *out = (unsigned char *)ptr;
     return QEM_OK;
 }
 
@@ -102,7 +100,7 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     if (!xyz || !q || !F || (P > 0 && !k3)) return reject("NULL pointer");
     if (!(p->Lx > 0 && p->Ly > 0 && p->Lz > 0 && p->eps_0 > 0) || !std::isfinite(sum_K) ||
         !(fabs(p->gamma_up * p->gamma_down) < 1.0) ||
-        (p->precision != QEM_FP64 && p->precision != QEM_FP32_FIX) || p->device < 0 || p->device >= MAX_DEVICES)
+        (p->precision != QEM_FP64 && p->precision != QEM_FP32_FIX) || p->device < 0)
         return reject("invalid parameters");
     double kmax = 0;
     for (int i = 0; i < P; i++) {
@@ -115,7 +113,7 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     if (qem_long_chunk() != NA_CH) return reject("scratch layout does not match the long-range chunk size");
     if (cudaSetDevice(p->device) != cudaSuccess) return QEM_ERR_CUDA;
     unsigned char *S = nullptr;
-    qem_status st = scratch_address(p->device, &S);
+    qem_status st = scratch_address(&S);
     if (st != QEM_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     unsigned *status = (unsigned *)(S + O_STATUS);
@@ -145,6 +143,7 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     b.Fpart = (double *)(S + O_FPART);
     b.Eks = b.Epart + (size_t)b.ks * nch + (NA_MAX_N + 255) / 256;
     b.stmp = S + O_STMP; b.stmp_bytes = STMP_BYTES;
+    b.zlim = p->precision == QEM_FP32_FIX && P > 0 ? qem_fp32_zlim(kmax) : 0.0;
     for (int stage = 0; stage < 2 && e == cudaSuccess; stage++)
         e = qem_launch_long(p->precision, false, N, P, pos, zperm, b, p->Lx, p->Ly, p->Lz, p->gamma_down, p->gamma_up,
                             p->eps_0, sum_K, F, nch, status, s, stage);
@@ -154,5 +153,6 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
         cudaStreamSynchronize(s) != cudaSuccess)
         return QEM_ERR_CUDA;
     if (host_status & QEM_ST_NONFINITE) return QEM_ERR_NONFINITE;
+    if (host_status & QEM_ST_RANGE) return QEM_ERR_RANGE;
     return QEM_OK;
 }

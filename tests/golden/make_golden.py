@@ -1,10 +1,12 @@
 """Generate golden vectors for the QEM oracle from the reference's own code.
 
-Run in a container that has the reference checkout (read-only) at
-``/root/reference``; the fixtures it writes (``tests/golden/*.json``) are
-committed, so the test-suite and the GPU box never need the reference tree.
+Run where a checkout of the reference (ArrogantGao/QEM4Molly) exists; its
+root is taken from ``--reference DIR`` or the ``QEM_REFERENCE_DIR``
+environment variable, and defaults to ``/root/reference``.  The fixtures it
+writes (``tests/golden/*.json``) are committed, so the test-suite and the GPU
+box never need the reference tree.
 
-    python tests/golden/make_golden.py            # writes all fixtures
+    python tests/golden/make_golden.py [--reference DIR]   # writes all fixtures
 
 What is generated (each case states the reference file it exercises):
 
@@ -50,7 +52,19 @@ import tempfile
 import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_LIB = "/root/reference/src/python_lib"
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def _reference_root(argv):
+    for i, a in enumerate(argv):
+        if a.startswith("--reference="):
+            return a.split("=", 1)[1]
+        if a == "--reference" and i + 1 < len(argv):
+            return argv[i + 1]
+    return os.environ.get("QEM_REFERENCE_DIR", DEFAULT_REFERENCE)
+
+
+REF_LIB = os.path.join(_reference_root(sys.argv[1:]), "src", "python_lib")
 
 
 def _setup(bessel: str):
@@ -459,8 +473,11 @@ def run_variant(bessel):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1].startswith("--bessel="):
-        run_variant(sys.argv[1].split("=", 1)[1])
+    variant = [a for a in sys.argv[1:] if a.startswith("--bessel=")]
+    if variant:
+        run_variant(variant[0].split("=", 1)[1])
     else:
+        ref = os.path.dirname(os.path.dirname(REF_LIB))
         for v in ("ref", "accurate"):
-            subprocess.run([sys.executable, os.path.abspath(__file__), f"--bessel={v}"], check=True)
+            subprocess.run([sys.executable, os.path.abspath(__file__), f"--bessel={v}", f"--reference={ref}"],
+                           check=True)
