@@ -6,10 +6,11 @@
 Workload (one "step" = one force evaluation of the whole system): the N = 1e5
 slab of the benchmark configuration -- +-1 charges, Lx = Ly = 1000, Lz = 10,
 gamma_up = gamma_down = 0.95, alpha = 0.1, r_c = 10, 30-node Gauss-Legendre
-quadrature, P = 500 random-batch k-vectors (seeded), Julia-reference
+quadrature, P = 500 random-batch k-vectors, a fresh seeded batch drawn on
+every evaluation as the reference does (Force_long.jl:235), Julia-reference
 semantics -- evaluated by the FP32+FP64-fix path (short + self + long range).
 The plain FP64 GPU path is timed in the same run and reported beside it, with
-the FP32 path's force error against it.
+the FP32 path's force error against it (both on the same batch).
 
 Multi-GPU (torchrun): one independent system per rank (seeded per rank), no
 data-path collective; value = total evaluations/s over all ranks ("weak").
@@ -25,8 +26,10 @@ lattice k with 0 < |k| < 1.0 (7,9xx vectors) weighted by exp(-k^2 / 4 alpha) on 
 (FP32+fix), the FP64 path and the oracle's CPU rate beside it.
 
 --impl reference times the FP64 CPU restatement of the reference algorithm
-(oracle/, OpenMP on all host cores) on a bounded sample of the same workload
-and extrapolates to evaluations/s of the full system.
+(oracle/, OpenMP on all host cores) on complete evaluations of the same
+system, each with a fresh batch drawn the reference's way (K_set_generator
+probabilities, weighted sampling with replacement); it times as many of the
+requested steps as fit in about two minutes and reports that count.
 """
 from __future__ import annotations
 
@@ -48,6 +51,18 @@ UNIT = "evals/s"
 FLOPS_PER_PAIR_NODE = 100   # op model per short-range quadrature node (FP32 flops)
 SFU_PER_PAIR_NODE = 6       # MUFU ops per node in the same model
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+REF_BUDGET_S = 120.0        # wall time of the reference arm's timed evaluations
+
+
+def slab_config(cfg, Np):
+    """The `config` of the N = 1e5 slab line: the same dict on both arms."""
+    return {"workload": f"QEM slab N={cfg['N']} Lx=Ly={cfg['L'][0]:g} Lz=10 gamma=0.95/0.95 alpha=0.1 r_c=10 "
+                        f"N_t=30 P={cfg['P']} (short+self+long), Julia-reference semantics",
+            "N": cfg["N"], "pairs": int(Np), "P": cfg["P"],
+            "kset": "a fresh seeded random batch of P k-vectors on every evaluation (Force_long.jl:235)",
+            "l2": "GPU arm: L2 flushed between steps (256 MiB write outside the per-step timing)"}
 
 
 def parse():
@@ -80,6 +95,9 @@ class Clocks:
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.02)  # the first sample precedes the timed region
         except Exception:
             self.proc = None
 
@@ -128,50 +146,41 @@ def barrier(world: int):
 
 
 # ----------------------------------------------------------------------------- CPU baseline
-def cpu_sample(cfg, pairs, seconds_target=15.0, n_pairs=None, n_self=None, P_s=None):
-    """FP64 oracle (OpenMP, all host cores) on a bounded sample of one evaluation; returns
-    (evals/s extrapolated to the full system, cores, description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
+class RefEvaluator:
+    """Complete FP64 evaluations of a slab by the CPU restatement of the
+    reference (oracle/, OpenMP on all host cores): the neighbour list, every
+    pair and self term, and the long range with a fresh batch per evaluation
+    drawn as the reference draws it (K_set_generator table, weighted sampling
+    with replacement, Force_long.jl:235)."""
 
-    import oracle as O
+    def __init__(self, cfg, seed=7):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
 
-    p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"],
-                 accuracy=cfg["accuracy"], N_t=cfg["N_t"])
-    cores = O.max_threads()
-    xyz, q, N = cfg["xyz"], cfg["q"], cfg["N"]
-    Np = len(pairs)
-    # size the sample from a short calibration so the whole sample takes ~seconds_target
-    t0 = time.perf_counter()
-    O.pairs_eval(p, xyz, q, pairs[:2000])
-    t_pair = (time.perf_counter() - t0) / 2000
-    if n_pairs is None:
-        n_pairs = int(min(Np, max(2000, 0.6 * seconds_target / max(t_pair, 1e-9))))
-    if n_self is None:
-        n_self = min(N, max(1000, n_pairs // 10))
-    if P_s is None:
-        P_s = 4
-    t0 = time.perf_counter()
-    O.pairs_eval(p, xyz, q, pairs[:n_pairs])
-    t_pairs = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.self_eval(p, xyz, q, n_self)
-    t_self = time.perf_counter() - t0
-    rng = np.random.default_rng(1)
-    k3 = np.zeros((P_s, 3))
-    for i in range(P_s):
-        mx, my = rng.integers(-40, 41, 2)
-        mx = mx if (mx or my) else 1
-        k3[i] = [2 * np.pi * mx / cfg["L"][0], 2 * np.pi * my / cfg["L"][1], 0]
-        k3[i, 2] = np.hypot(k3[i, 0], k3[i, 1])
-    t0 = time.perf_counter()
-    O.F_long(p, xyz, q, k3, 1.0)
-    t_long = time.perf_counter() - t0
-    t_full = t_pairs * (Np / n_pairs) + t_self * (N / n_self) + t_long * (cfg["P"] / P_s)
-    desc = (f"oracle FP64 on {cores} threads: {n_pairs} of {Np} pairs, {n_self} of {N} self terms, "
-            f"{P_s} of {cfg['P']} k-vectors over all N; extrapolated to one full evaluation "
-            f"({t_pairs + t_self + t_long:.1f} s measured, {t_full:.1f} s per evaluation)")
-    return 1.0 / t_full, cores, desc
+        import oracle as O
+
+        self.O, self.cfg = O, cfg
+        self.p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"],
+                          accuracy=cfg["accuracy"], N_t=cfg["N_t"])
+        self.K, Prob, self.sum_K = O.kset_generator(cfg["L"][0], cfg["L"][1], cfg["alpha"], cfg["accuracy"])
+        self.Prob = Prob.astype(np.float64) / Prob.astype(np.float64).sum()
+        self.rng = np.random.default_rng(seed)
+        self.cores = int(O.max_threads())
+        self.npairs = 0
+
+    def __call__(self):
+        O, cfg = self.O, self.cfg
+        k3 = self.K[self.rng.choice(len(self.K), size=cfg["P"], replace=True, p=self.Prob)]
+        pl = O.pairs(self.p, cfg["xyz"], method="cells")
+        self.npairs = len(pl)
+        return O.short_forces(self.p, cfg["xyz"], cfg["q"], pl) + O.F_long(self.p, cfg["xyz"], cfg["q"], k3,
+                                                                          self.sum_K)
+
+    def describe(self, n, seconds):
+        c = self.cfg
+        return (f"oracle FP64 on {self.cores} threads: {n} complete evaluation(s) of the N={c['N']} slab "
+                f"({self.npairs} pairs, {c['N']} self terms, P={c['P']} k-vectors over all N, a fresh batch "
+                f"each), {seconds:.1f} s each")
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -196,8 +205,10 @@ def run_ours(args):
     lib.qem_measure_peaks(local, C.byref(fp32_peak), C.byref(mufu_peak))
 
     cfg = W.config2(N=args.N, seed=None if rank == 0 else W.SEED0 + 2 + 1000 * rank)
-    e32 = W.engine_for(cfg, "fp32", device=local)
-    e64 = W.engine_for(cfg, "fp64", device=local)  # same seeded k-set
+    # a fresh random batch on every evaluation, drawn on the device (batch n of the seed at call n)
+    kseed = 7 + 1000 * rank
+    e32 = W.engine_for(cfg, "fp32", mode_flags=L.QEM_RESAMPLE_KSET, seed=kseed, device=local)
+    e64 = W.engine_for(cfg, "fp64", mode_flags=L.QEM_RESAMPLE_KSET, seed=kseed, device=local)
     x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
     q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
     F = torch.empty_like(x)
@@ -217,11 +228,15 @@ def run_ours(args):
             per.append(a.elapsed_time(b))
         return per
 
-    def kernel_times(e, K, terms=terms):
-        """Per-phase CUDA-event times (on the streams each phase is launched on) over K profiled steps."""
+    def kernel_times(e, K, terms=terms, min_s=0.0):
+        """Per-phase CUDA-event times (on the streams each phase is launched on) over K profiled steps
+        (more while under min_s seconds of wall time, so the clock sampler sees the load)."""
         e.set_profiling(True)
         kt = {}
-        for _ in range(K):
+        t0 = time.perf_counter()
+        it = 0
+        while it < K or time.perf_counter() - t0 < min_s:
+            it += 1
             flush.zero_()
             e.forces_device(x, q, F, terms=terms)
             for k, v in e.timings().items():
@@ -240,7 +255,7 @@ def run_ours(args):
     per32 = timed(e32, args.steps)
     torch.cuda.synchronize()
     barrier(world)
-    kt32 = kernel_times(e32, args.steps)
+    kt32 = kernel_times(e32, args.steps, min_s=1.0)
     counts = e32.counts()  # kernels of one full evaluation (before the short-range-only pass)
     # the pair kernel alone on the GPU (short range only): in the full step the
     # high-priority long-range chain shares its SMs and stretches its span
@@ -254,7 +269,10 @@ def run_ours(args):
     ms64 = max_over_ranks(float(np.sum(per64)) / K64, world, dev)
     kt64 = kernel_times(e64, K64)
 
-    # accuracy of the FP32+fix path against the plain FP64 path (parity-tested against the oracle)
+    # accuracy of the FP32+fix path against the plain FP64 path (parity-tested against the
+    # oracle) on the same batch: both engines restart at batch 0 of the seed
+    e32.sample_kset(kseed, cfg["P"])
+    e64.sample_kset(kseed, cfg["P"])
     e32.forces_device(x, q, F, terms=terms)
     F32 = F.cpu().numpy().copy()
     e64.forces_device(x, q, F, terms=terms)
@@ -297,29 +315,26 @@ def run_ours(args):
     out = {"metric": METRIC, "value": world * 1000.0 / ms32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64fix", "data": "synthetic (seeded, per-rank system)",
-           "config": {"workload": f"QEM slab N={cfg['N']} Lx=Ly={cfg['L'][0]:g} Lz=10 gamma=0.95/0.95 alpha=0.1 "
-                                  f"r_c=10 N_t=30 P={cfg['P']} (short+self+long), Julia-reference semantics",
-                      "N": cfg["N"], "pairs": Np, "P": cfg["P"], "precision": "FP32+FP64-fix",
-                      "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
-                      "kernel_times": "kernel_ms comes from a profiled pass of the same steps right after the "
-                                      "timed loop (per-phase CUDA events on their own streams; the long range "
-                                      "overlaps the pair kernel there); roofline.achieved uses the pair kernel's "
-                                      "span in a profiled short-range-only pass (the kernel alone on the GPU); "
-                                      "the timed loop itself runs the unprofiled production path",
-                      "parallelism": f"{world} independent systems (one per GPU); per GPU the long range "
-                                     "runs on a second stream concurrently with the short range"},
+           "config": slab_config(cfg, Np),
+           "notes": {"precision": "FP32+FP64-fix; the fp64 key is the plain FP64 GPU path on the same workload",
+                     "kernel_times": "kernel_ms comes from a profiled pass of the same steps right after the "
+                                     "timed loop (per-phase CUDA events on their own streams; the long range "
+                                     "overlaps the pair kernel there); roofline.achieved uses the pair kernel's "
+                                     "span in a profiled short-range-only pass (the kernel alone on the GPU); "
+                                     "the timed loop itself runs the unprofiled production path",
+                     "parallelism": f"{world} independent systems (one per GPU); per GPU the long range "
+                                    "runs on a second stream concurrently with the short range"},
            "e2e": e2e, "gpu_launches": int(counts["launches"]) * args.steps, "roofline": roofline,
            "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64, "steps": K64},
            "speedup_vs_fp64": ms64 / ms32, "force_rel_err_vs_fp64": err, "force_max_err_vs_fp64_rms": err_max,
            "kernel_ms": {"fp32": kt32, "fp64": kt64, "fp32_short_only": kt32_short}, "clocks": clk}
     if rank == 0 and world == 1:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-
-        p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
-        pairs = O.pairs(p, cfg["xyz"], method="cells")
-        v, cores, desc = cpu_sample(cfg, pairs)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+        ref = RefEvaluator(cfg)
+        t0 = time.perf_counter()
+        ref()
+        t_ref = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / t_ref, "unit": UNIT, "cores": ref.cores, "kind": "port",
+                               "sample": ref.describe(1, t_ref)}
     if rank == 0:
         print(json.dumps(out), flush=True)
     e32.close()
@@ -508,35 +523,37 @@ def run_exact(args):
 
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args):
+    """Complete evaluations by RefEvaluator.  One untimed warm-up evaluation
+    sizes the run: as many of the requested steps as fit in REF_BUDGET_S are
+    timed, and the line reports that count."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    import numpy as np
 
     from qem4molly_b200 import workloads as W
 
     cfg = W.config2(N=args.N)
-    p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
-    pairs = O.pairs(p, cfg["xyz"], method="cells")
-    per_step = max(2.0, min(10.0, 150.0 / (args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_sample(cfg, pairs, seconds_target=per_step / 4)
-    vals, desc, cores = [], "", 1
+    ref = RefEvaluator(cfg)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, cores, desc = cpu_sample(cfg, pairs, seconds_target=per_step)
-        vals.append(v)
-    wall = time.perf_counter() - t0
-    value = len(vals) / sum(1.0 / v for v in vals)
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": f"QEM slab N={cfg['N']} (same system as the GPU arm), FP64 CPU restatement of "
-                                  "the reference algorithm, bounded samples extrapolated per evaluation"},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+    ref()
+    t_warm = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(REF_BUDGET_S / max(t_warm, 1e-3))))
+    per = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref()
+        per.append(time.perf_counter() - t0)
+    ms = 1000.0 * float(np.mean(per))
+    value = 1000.0 / ms
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": 1,
+           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded)", "impl": "reference", "config": slab_config(cfg, ref.npairs),
+           "requested_steps": args.steps,
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": "port",
+                            "sample": ref.describe(steps, ms / 1000.0)},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-           "sample_wall_s": wall}
+           "timed_wall_s": float(np.sum(per)), "warmup_s": t_warm}
     print(json.dumps(out), flush=True)
 
 

@@ -71,7 +71,10 @@ typedef int32_t qem_status;
 #define QEM_STALE_NEIGHBORS 0x8u /* rebuild the pair list only on calls 1, 1+iter_period, ...
                                     (QEM_short.jl:32-36); default rebuilds every call             */
 #define QEM_RESAMPLE_KSET 0x10u  /* draw a fresh random batch of k-vectors on every long-range
-                                    call (Force_long.jl:235); default reuses the current batch    */
+                                    call (Force_long.jl:235), on the device: call n after
+                                    qem_sample_kset(seed, P) uses batch n of that seed
+                                    (qem_draw_kset); recorded graphs and qem_batch_md draw new
+                                    batches too.  Default reuses the current batch               */
 #define QEM_EQUAL_Z_TIES 0x20u   /* particles of equal z are neither below nor above each other in
                                     the z-ordered long-range sums (python_lib equal_cell,
                                     Sigma_Gamma_func_njit.py:168-281); default: sortperm(z) order,
@@ -164,13 +167,29 @@ const char *qem_status_string(qem_status s);
 
 /* Random-batch k-set.  qem_set_kset feeds P rows of (kx, ky, k) and the
  * normaliser sum_K (K_set_generator.jl:28) -- the way parity runs feed the
- * same batch to the library and to the oracle.  qem_sample_kset draws P
- * vectors from exp(-k^2 / 4 alpha) on the 2 pi (m / Lx, n / Ly) lattice
- * (k != 0, |m| <= ceil(k_c Lx / 2 pi) + 1, K_set_generator.jl:7-9) with the
- * library's own seeded separable sampler. */
+ * same batch to the library and to the oracle.  qem_sample_kset makes batch 0
+ * of the library's own sampler the current k-set: P vectors from
+ * exp(-k^2 / 4 alpha) on the 2 pi (m / Lx, n / Ly) lattice (k != 0,
+ * |m| <= ceil(k_c Lx / 2 pi) + 1, K_set_generator.jl:7-9; the reference draws
+ * them with StatsBase.sample, Force_long.jl:235).  Batch n of a seed is a pure
+ * function of (seed, n): row i takes three uniforms from the SplitMix64
+ * finaliser of (seed, n, i, 0..2), one to choose between the m_x != 0 and the
+ * m_x = 0 parts of the lattice (weights S_x T_y and S_y, S = sum over m != 0,
+ * T = sum over all m of exp(-(2 pi m / L)^2 / 4 alpha)) and two for m_x, m_y by
+ * inverse CDF, so the draw is exact without rejection.  With
+ * QEM_RESAMPLE_KSET every long-range call draws the next batch on the device
+ * (the batch counter, reset by qem_sample_kset, is in device memory), and
+ * qem_get_kset returns the rows of the latest call's batch (the current
+ * k-set before the first call); qem_kset_batch reports the counter (the
+ * number of long-range calls since qem_sample_kset).  qem_draw_kset computes
+ * rows [row0, row0 + P) of batch n for a box and alpha on the host, without a
+ * handle or a GPU. */
 qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K);
 qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P);
 qem_status qem_get_kset(const qem_handle *h, double *k3_out, int32_t cap, int32_t *P, double *sum_K);
+qem_status qem_kset_batch(const qem_handle *h, uint64_t *n);
+qem_status qem_draw_kset(const qem_params *p, uint64_t seed, uint64_t n, int64_t row0, int32_t P, double *k3,
+                         double *sum_K);
 
 /* Most k-vectors of one k-set (the k-space passes put 16 k-vectors per block
  * along a grid dimension of at most 65535 blocks). */
@@ -226,7 +245,7 @@ qem_status qem_potential_energy(qem_handle *h, int32_t N, const double *xyz, con
  * gF: 3N doubles or NULL (zero).  Always evaluated in FP64, whatever the
  * handle's precision, with the neighbour-list rules of the forward call and
  * the handle's current k-set (a k-set is sampled if none exists; with
- * QEM_RESAMPLE_KSET the backward uses the k-set of the latest forward call).
+ * QEM_RESAMPLE_KSET the backward uses the batch of the latest forward call).
  * The derivatives are those of the discretised quantities, so the
  * quadrature limits' dependence on the image distances (Julia cutoff mode)
  * is included; the k = 0 force is piecewise constant in z and contributes no
@@ -305,7 +324,9 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  *   box), with one step recorded once as a CUDA graph and replayed.  On
  *   return xyz and v hold the final state and F the final forces; the call
  *   synchronises and checks the status.  Neighbour lists are rebuilt every
- *   step and each system keeps its current k-set for the whole run.
+ *   step; a system with QEM_RESAMPLE_KSET draws a fresh k batch every step
+ *   (on the device, inside the recorded step), the others keep their current
+ *   k-set for the whole run.
  * qem_batch_autotune: times the graph-replayed force evaluation for stream
  *   pool widths 1, 2, 4, ... up to min(B, 128) and keeps the fastest;
  *   returns the width and its time per batch evaluation (ms).

@@ -83,6 +83,8 @@ def load(build: bool = False):
         "qem_set_kset": (C.c_int32, [H, dp, C.c_int32, C.c_double]),
         "qem_sample_kset": (C.c_int32, [H, C.c_uint64, C.c_int32]),
         "qem_get_kset": (C.c_int32, [H, dp, C.c_int32, ip, dp]),
+        "qem_kset_batch": (C.c_int32, [H, C.POINTER(C.c_uint64)]),
+        "qem_draw_kset": (C.c_int32, [PP, C.c_uint64, C.c_uint64, C.c_int64, C.c_int32, dp, dp]),
         "qem_exact_kset_rows": (C.c_int32, [C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64,
                                             C.POINTER(C.c_int64)]),
         "qem_set_kset_weighted": (C.c_int32, [H, dp, dp, C.c_int32]),

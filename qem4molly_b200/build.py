@@ -40,16 +40,41 @@ def _stale() -> bool:
 
 
 def build_lib(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compiles each .cu file to an object (in parallel, under _build/) and
+    links them into libqem.so; no relocatable device code is needed, since no
+    kernel calls device code of another file."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"),
+             *(extra or [])]
+    jobs = []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        jobs.append((obj, [nvcc(), *flags, "-c", src, "-o", obj]))
+
+    def run(job):
+        if verbose:
+            print(" ".join(job[1]))
+        return subprocess.run(job[1], capture_output=not verbose, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(run, jobs))
+    for (obj, cmd), r in zip(jobs, results):
+        if r.returncode != 0:
+            if r.stderr:
+                sys.stderr.write(r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+        if verbose is False and r.stderr and "ptxas" in r.stderr:
+            sys.stderr.write(r.stderr)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", tmp, *sources()]
-    if extra:
-        cmd[1:1] = list(extra)
+    link = [nvcc(), *ARCH, "-shared", "-o", tmp, *[o for o, _ in jobs]]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -51,19 +51,8 @@ __global__ void k_vv_kick(int n3, double *__restrict__ v, double *__restrict__ F
 // numbers come from a counter-based generator: the SplitMix64 finaliser
 // (Steele, Lea and Flood, OOPSLA 2014; Vigna's constants) of
 // seed + golden-ratio increments of (step, particle, draw), so every draw is
-// a pure function of (seed, step, i, draw) and a replayed graph draws new
-// numbers through the step counter in device memory.
-__host__ __device__ inline uint64_t mix64(uint64_t z)
-{
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-    return z ^ (z >> 31);
-}
-__host__ __device__ inline uint64_t draw64(uint64_t seed, uint64_t step, uint64_t i, uint64_t k)
-{
-    const uint64_t G = 0x9e3779b97f4a7c15ULL;
-    return mix64(mix64(mix64(seed + G * (step + 1)) + G * (i + 1)) + G * (k + 1));
-}
+// a pure function of (seed, step, i, draw) (draw64, qem_internal.cuh) and a
+// replayed graph draws new numbers through the step counter in device memory.
 // uniform in (0, 1]: 53 random bits
 __device__ inline double unit53(uint64_t r) { return ((double)(r >> 11) + 1.0) * 0x1.0p-53; }
 

@@ -80,16 +80,6 @@ void gauss_legendre(int n, double *x, double *w)
     if (n % 2 == 1) x[n / 2] = 0.0;
 }
 
-// splitmix64 (Steele, Lea, Flood 2014): seeded stream of 64-bit words
-inline uint64_t splitmix64(uint64_t &s)
-{
-    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-    return z ^ (z >> 31);
-}
-inline double uniform01(uint64_t &s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
-
 struct Prof {
     bool on = false;
     std::vector<cudaEvent_t> pool;
@@ -141,10 +131,17 @@ struct qem_handle {
     int shard_rank = 0, shard_world = 1;
     uint64_t cfg_version = 0;  // bumped by k-set and shard changes
     int long_max_ks = QEM_LONG_MAX_KS;  // cap on the k-slices of the long-range force pass
-    uint64_t rng = 0x51ed5eedULL;
-    std::vector<double> cdfx, cdfy;
-    long mxmax = 0, mymax = 0;
+    // random-batch sampler (KSampler): seed of the batches, host copy of its
+    // cumulative tables, their device copy and the device batch counter (the
+    // number of long-range evaluations since the last qem_sample_kset)
+    uint64_t kseed = 0x51ed5eedULL;
+    std::vector<double> ktab_host;
+    KSampler ksamp{};
     double sampler_sumK = 0;
+    double kmax_lattice = 0;  // largest |k| the sampler can draw
+    DevBuf ktab, kctr;
+    bool ktab_on_dev = false;
+    bool kctr_reset = true;   // the device counter must be set to 0 before the next draw
     double kmax = 0;
     // geometry / constants
     CellGeom geom;
@@ -283,6 +280,41 @@ static qem_status validate(const qem_params *p, std::string &why)
     return QEM_OK;
 }
 
+// separable k sampler of the box and alpha of p: w(m) = exp(-(2 pi m / L)^2 /
+// (4 alpha)), |m| <= ceil(k_c L / 2 pi) + 1 (K_set_generator.jl:7-9);
+// cumulative tables over all m and over m != 0 per axis (KSampler), sum_K
+// (K_set_generator.jl:28) and the largest |k| of the lattice
+static void make_sampler(const qem_params &p, KSampler &S, std::vector<double> &tab, double &sumK, double &kmax)
+{
+    const double k_c = 2.0 * sqrt(-4.0 * p.alpha * log(p.accuracy));  // K_set_generator.jl:7
+    const int Mx = (int)ceil(k_c * p.Lx / (2.0 * QEM_PI)) + 1, My = (int)ceil(k_c * p.Ly / (2.0 * QEM_PI)) + 1;
+    S = KSampler{};
+    S.Mx = Mx;
+    S.My = My;
+    S.Lx = p.Lx;
+    S.Ly = p.Ly;
+    tab.clear();
+    tab.reserve(4 * (size_t)(Mx + My) + 2);
+    auto cdf = [&](int M, double L, bool skip0, double &sum) {
+        double c = 0;
+        for (int m = -M; m <= M; m++) {
+            if (skip0 && m == 0) continue;
+            const double k = 2.0 * QEM_PI * m / L;
+            c += exp(-k * k / (4.0 * p.alpha));
+            tab.push_back(c);
+        }
+        sum = c;
+    };
+    cdf(Mx, p.Lx, false, S.Tx);
+    cdf(Mx, p.Lx, true, S.Sx);
+    cdf(My, p.Ly, false, S.Ty);
+    cdf(My, p.Ly, true, S.Sy);
+    S.tab = tab.data();
+    sumK = S.Sx + S.Sy + S.Sx * S.Sy;
+    const double kxm = 2.0 * QEM_PI * Mx / p.Lx, kym = 2.0 * QEM_PI * My / p.Ly;
+    kmax = sqrt(kxm * kxm + kym * kym);
+}
+
 static void build_consts(qem_handle *h)
 {
     const qem_params &p = h->p;
@@ -352,50 +384,52 @@ static void build_consts(qem_handle *h)
     g.ncx = ncx; g.ncy = ncy;
     g.inv_lcx = ncx / p.Lx; g.inv_lcy = ncy / p.Ly;
     h->ncell = ncx * ncy;
-    // separable k sampler: p(m) ~ exp(-(2 pi m / L)^2 / (4 alpha)), |m| <= ceil(k_c L / 2 pi) + 1
-    const double k_c = 2.0 * sqrt(-4.0 * p.alpha * log(p.accuracy));  // K_set_generator.jl:7
-    h->mxmax = (long)ceil(k_c * p.Lx / (2.0 * QEM_PI)) + 1;
-    h->mymax = (long)ceil(k_c * p.Ly / (2.0 * QEM_PI)) + 1;
-    auto cdf = [&](long mmax, double L, std::vector<double> &out) {
-        out.resize(2 * mmax + 1);
-        double s = 0;
-        for (long m = -mmax; m <= mmax; m++) {
-            const double k = 2.0 * QEM_PI * m / L;
-            s += exp(-k * k / (4.0 * p.alpha));
-            out[m + mmax] = s;
-        }
-        return s;
-    };
-    const double Sx = cdf(h->mxmax, p.Lx, h->cdfx), Sy = cdf(h->mymax, p.Ly, h->cdfy);
-    h->sampler_sumK = Sx * Sy - 1.0;  // = S_x + S_y + S_x S_y with m = 0 excluded (K_set_generator.jl:28)
+    make_sampler(p, h->ksamp, h->ktab_host, h->sampler_sumK, h->kmax_lattice);
 }
 
+static bool resampling(const qem_handle *h) { return (h->p.mode_flags & QEM_RESAMPLE_KSET) != 0; }
+
+// rows [0, P) of batch n of the handle's sampler (host copy of the draw the
+// per-k constants kernel makes on the device: the same bits)
+static void batch_rows(const qem_handle *h, uint64_t n, int P, std::vector<double> &k3)
+{
+    KSampler S = h->ksamp;
+    S.tab = h->ktab_host.data();
+    S.seed = h->kseed;
+    k3.resize(3 * (size_t)P);
+    for (int i = 0; i < P; i++) ksample_row(S, n, i, k3[3 * i], k3[3 * i + 1], k3[3 * i + 2]);
+}
+
+// batch 0 of the sampler with the handle's seed becomes the current k-set;
+// with QEM_RESAMPLE_KSET the device counter restarts at 0, so the next
+// long-range call draws this same batch on the device, and call n batch n
 static void sample_kset(qem_handle *h, int P)
 {
-    const qem_params &p = h->p;
-    h->kset.resize(3 * (size_t)P);
+    batch_rows(h, 0, P, h->kset);
     h->kwt.clear();
     double kmax = 0;
-    for (int i = 0; i < P;) {
-        const double ux = uniform01(h->rng) * h->cdfx.back(), uy = uniform01(h->rng) * h->cdfy.back();
-        const long mx = (long)(std::upper_bound(h->cdfx.begin(), h->cdfx.end(), ux) - h->cdfx.begin()) - h->mxmax;
-        const long my = (long)(std::upper_bound(h->cdfy.begin(), h->cdfy.end(), uy) - h->cdfy.begin()) - h->mymax;
-        if (mx == 0 && my == 0) continue;
-        if (mx < -h->mxmax || mx > h->mxmax || my < -h->mymax || my > h->mymax) continue;
-        const double kx = 2.0 * QEM_PI * mx / p.Lx, ky = 2.0 * QEM_PI * my / p.Ly;
-        const double k = sqrt(kx * kx + ky * ky);
-        h->kset[3 * i] = kx;
-        h->kset[3 * i + 1] = ky;
-        h->kset[3 * i + 2] = k;
-        kmax = std::max(kmax, k);
-        i++;
-    }
+    for (int i = 0; i < P; i++) kmax = std::max(kmax, h->kset[3 * i + 2]);
     h->P = P;
     h->sum_K = h->sampler_sumK;
-    h->kmax = kmax;
+    h->kmax = resampling(h) ? h->kmax_lattice : kmax;
     h->has_kset = true;
     h->kset_dirty = true;
+    h->kctr_reset = true;
     h->cfg_version++;
+}
+
+// device batch counter (number of long-range calls since qem_sample_kset);
+// the caller has no work in flight on the handle (calls synchronise)
+static bool read_batch_counter(const qem_handle *h, uint64_t *n)
+{
+    *n = 0;
+    if (!h->kctr.p || h->kctr_reset) return true;
+    unsigned long long v = 0;
+    if (cudaSetDevice(h->p.device) != cudaSuccess ||
+        cudaMemcpy(&v, h->kctr.p, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    *n = v;
+    return true;
 }
 
 // device buffers of the long range for N particles, Pk k-vectors, nch chunks
@@ -575,16 +609,24 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     int mk_lstart = -1, mk_lprep = -1, mk_lforce = -1;
     h->counts[2] = 0;
     if (do_long) {
+        // QEM_RESAMPLE_KSET: a fresh batch on every call (Force_long.jl:235),
+        // drawn on the device from (seed, batch counter) by the per-k constants
+        // kernel; the counter lives in device memory, so replayed graphs draw
+        // new batches as well
+        const bool draw = resampling(h);
         if (async) {
-            if ((h->p.rbe_p > 0 && !h->has_kset) || h->kset_dirty)
+            if ((h->p.rbe_p > 0 && !h->has_kset) || h->kset_dirty || (draw && (!h->ktab_on_dev || h->kctr_reset)))
                 return fail(h, QEM_ERR_NO_KSET, "async evaluation: the k-set must be on the device (synchronous call first)");
         } else if (!h->has_kset && h->p.rbe_p > 0) {
             sample_kset(h, h->p.rbe_p);
-        } else if ((h->p.mode_flags & QEM_RESAMPLE_KSET) && h->p.rbe_p > 0) {
-            sample_kset(h, h->p.rbe_p);
+        }
+        if (draw) {  // uniform sum_K / P weights of the sampler
+            h->kwt.clear();
+            h->sum_K = h->sampler_sumK;
         }
         const int Pall = h->has_kset ? h->P : 0;
-        if (prec == QEM_FP32_FIX && Pall > 0 && h->kmax * h->p.Lz > 120.0)
+        const double kmax = draw ? h->kmax_lattice : h->kmax;
+        if (prec == QEM_FP32_FIX && Pall > 0 && kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
         // this rank's rows of the k-set, weighted as part of all Pall rows
         const int k_lo = (int)((int64_t)Pall * h->shard_rank / h->shard_world);
@@ -599,13 +641,38 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
             if (ls != QEM_OK) return ls;
         }
         b.skip_k0 = h->shard_rank != 0;
-        b.zlim = prec == QEM_FP32_FIX && Pk > 0 ? qem_fp32_zlim(h->kmax) : 0.0;
+        b.zlim = prec == QEM_FP32_FIX && Pk > 0 ? qem_fp32_zlim(kmax) : 0.0;
+        if (draw && Pall > 0) {
+            if (!async) {  // sampler tables and batch counter on the device (before the fork)
+                CU(grow(h->ktab, sizeof(double) * h->ktab_host.size()));
+                CU(grow(h->kctr, sizeof(unsigned long long)));
+                if (!h->ktab_on_dev) {
+                    CU(cudaMemcpyAsync(h->ktab.p, h->ktab_host.data(), sizeof(double) * h->ktab_host.size(),
+                                       cudaMemcpyHostToDevice, s));
+                    h->ktab_on_dev = true;
+                }
+                if (h->kctr_reset) {
+                    CU(cudaMemsetAsync(h->kctr.p, 0, sizeof(unsigned long long), s));
+                    h->kctr_reset = false;
+                }
+            }
+            b.draw_ctr = ptr<unsigned long long>(h->kctr);
+            b.sampler = h->ksamp;
+            b.sampler.tab = ptr<double>(h->ktab);
+            b.sampler.seed = h->kseed;
+            b.sampler.row0 = k_lo;
+            b.kwt = nullptr;
+        }
         if (concurrent) {  // fork after pack (positions) and the energy-partial clear
             CU(cudaEventRecord(h->ev_fork, s));
             CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
         }
         mk_lstart = h->prof.mark(sl);
-        if ((h->kset_dirty || h->kin_lo != k_lo || h->kin_hi != k_hi) && Pk > 0) {
+        if (draw) {  // the rows [k_lo, k_hi) of this call's batch are drawn into kin on the device
+            h->kset_dirty = false;
+            h->kin_lo = k_lo;
+            h->kin_hi = k_hi;
+        } else if ((h->kset_dirty || h->kin_lo != k_lo || h->kin_hi != k_hi) && Pk > 0) {
             CU(cudaMemcpyAsync(h->kin.p, h->kset.data() + 3 * (size_t)k_lo, sizeof(double) * 3 * Pk,
                                cudaMemcpyHostToDevice, sl));
             if (!h->kwt.empty())
@@ -639,6 +706,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
             // order of ties and comes from the first pass.
             CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
                                 ptr<double>(h->zkey), ptr<double>(h->zkey2), sl, true));
+            b.draw_ctr = nullptr;  // the second pass reuses the rows the first one drew
             for (int stage = 0; stage < 2; stage++)
                 CU(qem_launch_long(prec, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
                                    h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch,
@@ -771,7 +839,7 @@ static bool graph_eligible(const qem_handle *h, int N, const double *xyz, const 
                            const double *energy, uint32_t terms, int mem)
 {
     if (energy || h->prof.on || N <= 0 || !xyz || !q || !F || (terms & ~QEM_TERM_ALL) ||
-        (h->p.mode_flags & (QEM_STALE_NEIGHBORS | QEM_RESAMPLE_KSET)))
+        (h->p.mode_flags & QEM_STALE_NEIGHBORS))
         return false;
     if (mem == QEM_MEM_DEVICE) return true;
     const size_t n3 = sizeof(double) * 3 * (size_t)N;
@@ -1002,7 +1070,7 @@ void qem_destroy(qem_handle *h)
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
-                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw};
+                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -1132,7 +1200,7 @@ qem_status qem_sample_kset(qem_handle *h, uint64_t seed, int32_t P)
     if (!h) return QEM_ERR_ARG;
     if (P < 0) return fail(h, QEM_ERR_ARG, "P < 0");
     if (P > QEM_MAX_KSET) return fail(h, QEM_ERR_RANGE, "more k-vectors than QEM_MAX_KSET");
-    h->rng = seed;
+    h->kseed = seed;
     sample_kset(h, P);
     return QEM_OK;
 }
@@ -1141,8 +1209,45 @@ qem_status qem_get_kset(const qem_handle *h, double *k3_out, int32_t cap, int32_
 {
     if (!h) return QEM_ERR_ARG;
     if (P) *P = h->P;
-    if (sum_K) *sum_K = h->sum_K;
-    if (k3_out && cap > 0) memcpy(k3_out, h->kset.data(), sizeof(double) * 3 * (size_t)std::min(cap, h->P));
+    if (sum_K) *sum_K = resampling(h) && h->has_kset ? h->sampler_sumK : h->sum_K;
+    if (!k3_out || cap <= 0) return QEM_OK;
+    uint64_t n = 0;
+    if (resampling(h) && h->has_kset) {  // the batch of the latest long-range call
+        if (!read_batch_counter(h, &n)) return QEM_ERR_CUDA;
+    }
+    if (n > 0) {
+        std::vector<double> k3;
+        batch_rows(h, n - 1, h->P, k3);
+        memcpy(k3_out, k3.data(), sizeof(double) * 3 * (size_t)std::min(cap, h->P));
+    } else {
+        memcpy(k3_out, h->kset.data(), sizeof(double) * 3 * (size_t)std::min(cap, h->P));
+    }
+    return QEM_OK;
+}
+
+qem_status qem_kset_batch(const qem_handle *h, uint64_t *n)
+{
+    if (!h || !n) return QEM_ERR_ARG;
+    *n = 0;
+    if (!resampling(h) || !h->has_kset) return QEM_OK;
+    return read_batch_counter(h, n) ? QEM_OK : QEM_ERR_CUDA;
+}
+
+qem_status qem_draw_kset(const qem_params *p, uint64_t seed, uint64_t n, int64_t row0, int32_t P, double *k3,
+                         double *sum_K)
+{
+    if (!p || P < 0 || row0 < 0 || (P > 0 && !k3) || !finite_pos(p->Lx) || !finite_pos(p->Ly) ||
+        !finite_pos(p->alpha) || !(p->accuracy > 0 && p->accuracy < 1))
+        return QEM_ERR_ARG;
+    const double nmax = 2.0 * sqrt(-4.0 * p->alpha * log(p->accuracy)) * std::max(p->Lx, p->Ly) / (2.0 * QEM_PI);
+    if (!(nmax < 1e7)) return QEM_ERR_RANGE;
+    KSampler S;
+    std::vector<double> tab;
+    double sK = 0, kmax = 0;
+    make_sampler(*p, S, tab, sK, kmax);
+    S.seed = seed;
+    for (int i = 0; i < P; i++) ksample_row(S, n, row0 + i, k3[3 * i], k3[3 * i + 1], k3[3 * i + 2]);
+    if (sum_K) *sum_K = sK;
     return QEM_OK;
 }
 
@@ -1376,6 +1481,16 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
 
     if (do_long) {
         if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+        uint64_t nb = 0;
+        if (resampling(h) && h->has_kset) {  // the batch of the latest forward call
+            if (!read_batch_counter(h, &nb)) return fail(h, QEM_ERR_CUDA, "reading the k batch counter");
+            if (nb > 0) {
+                batch_rows(h, nb - 1, h->P, h->kset);
+                h->kwt.clear();
+                h->sum_K = h->sampler_sumK;
+                h->kset_dirty = true;
+            }
+        }
         const int Pk = h->has_kset ? h->P : 0;
         const int LCH = qem_long_chunk();
         const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;

@@ -77,6 +77,86 @@ struct KForce {
 };
 
 // ---------------------------------------------------------------------------
+// counter-based random numbers: the SplitMix64 finaliser (Steele, Lea and
+// Flood, OOPSLA 2014; Vigna's constants) of seed + golden-ratio increments of
+// (a, b, c), so every draw is a pure function of (seed, a, b, c) and host and
+// device compute the same words
+// ---------------------------------------------------------------------------
+__host__ __device__ inline uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+__host__ __device__ inline uint64_t draw64(uint64_t seed, uint64_t a, uint64_t b, uint64_t c)
+{
+    const uint64_t G = 0x9e3779b97f4a7c15ULL;
+    return mix64(mix64(mix64(seed + G * (a + 1)) + G * (b + 1)) + G * (c + 1));
+}
+// uniform in [0, 1): 53 random bits
+__host__ __device__ inline double unit53_lo(uint64_t r) { return (double)(r >> 11) * 0x1.0p-53; }
+
+// Random-batch k sampler (K_set_generator.jl:5-45 + StatsBase.sample,
+// Force_long.jl:235): k = 2 pi (m_x / L_x, m_y / L_y), (m_x, m_y) != (0, 0),
+// |m| <= M, drawn with probability exp(-k^2 / 4 alpha) / sum_K.  The weight
+// is a product w_x(m_x) w_y(m_y), so the draw is exact without rejection:
+// with S_x = sum_{m != 0} w_x and T_y = sum_m w_y (w_y(0) = 1), the pairs with
+// m_x != 0 carry S_x T_y and those with m_x = 0, m_y != 0 carry S_y; one
+// uniform picks the part, two more pick m_x and m_y by inverse CDF.
+// tab holds four cumulative weight tables, m ascending: x over all m
+// (2 Mx + 1), x over m != 0 (2 Mx), y over all m (2 My + 1), y over m != 0 (2 My).
+struct KSampler {
+    const double *tab;   // device (or host) address of the tables
+    int Mx, My;
+    double Lx, Ly;
+    double Sx, Tx, Sy, Ty;  // sums over m != 0 (S) and over all m (T) per axis
+    uint64_t seed;
+    int64_t row0;           // first row of this rank's share (the device k rows start there)
+};
+
+// smallest i in [0, n) with c[i] > u (n - 1 if none): inverse CDF of an
+// ascending cumulative table
+__host__ __device__ inline int cdf_pick(const double *c, int n, double u)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (c[mid] > u) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// row `row` of batch n: (kx, ky, |k|)
+__host__ __device__ inline void ksample_row(const KSampler &S, uint64_t n, int64_t row, double &kx, double &ky,
+                                            double &k)
+{
+    const double *cx_all = S.tab, *cx_nz = cx_all + 2 * S.Mx + 1;
+    const double *cy_all = cx_nz + 2 * S.Mx, *cy_nz = cy_all + 2 * S.My + 1;
+    const double u0 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 0));
+    const double u1 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 1));
+    const double u2 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 2));
+    const double A = S.Sx * S.Ty;  // weight of m_x != 0
+    int mx, my;
+    if (S.Mx > 0 && u0 * (A + S.Sy) < A) {
+        const int i = cdf_pick(cx_nz, 2 * S.Mx, u1 * S.Sx);
+        mx = i < S.Mx ? i - S.Mx : i - S.Mx + 1;
+        my = cdf_pick(cy_all, 2 * S.My + 1, u2 * S.Ty) - S.My;
+    } else {
+        mx = 0;
+        const int i = cdf_pick(cy_nz, 2 * S.My, u2 * S.Sy);
+        my = i < S.My ? i - S.My : i - S.My + 1;
+    }
+    kx = 2.0 * QEM_PI * (double)mx / S.Lx;
+    ky = 2.0 * QEM_PI * (double)my / S.Ly;
+#ifdef __CUDA_ARCH__
+    k = sqrt(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)));  // no contraction: the host gets the same bits
+#else
+    k = sqrt(kx * kx + ky * ky);
+#endif
+}
+
+// ---------------------------------------------------------------------------
 // host-side launch wrappers (defined in the .cu files)
 // ---------------------------------------------------------------------------
 cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *pos, int *cell, CellGeom g,
@@ -199,6 +279,11 @@ struct LongBuffers {
     const double *kwt = nullptr;  // P per-k weights (exact k-sum); nullptr: sum_K / P for every k
     double zlim = 0.0;    // FP32 path: largest |z - Lz/2| whose e^{+-k (z - Lz/2)} stays in FP32
                           // range for every k (QEM_ST_RANGE beyond); 0: no check
+    // per-call random batch: when draw_ctr is set, the per-k constants kernel
+    // first draws row sampler.row0 + m of batch *draw_ctr into kin (the rows
+    // of this call), and the last kernel of the pass advances *draw_ctr
+    unsigned long long *draw_ctr = nullptr;
+    KSampler sampler{};
 };
 // zlim of the FP32 k-space path for a k-set whose largest |k| is kmax:
 // e^{+-k (z - Lz/2)} <= e^{60}, so that sums over many particles stay finite

@@ -66,11 +66,24 @@ struct LM<double> {
 // wk, esc: the force and energy weights of every k (random batch, sum_K / P
 // folded in); with per-k weights kwt (exact k-sum) wk = kwt / wden and
 // esc = -kwt / eden instead
-__device__ __forceinline__ void kconst_one(int m, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz,
+// ctr != nullptr: row m is first drawn (row S.row0 + m of batch *ctr) and
+// written to kin, then its constants are formed from it
+__device__ __forceinline__ void kconst_one(int m, double *__restrict__ kin, KConst *__restrict__ kc, double Lz,
                                            double g12, double wk, double esc, const double *__restrict__ kwt,
-                                           double wden, double eden)
+                                           double wden, double eden, const KSampler &S,
+                                           const unsigned long long *__restrict__ ctr)
 {
-    const double kx = kin[3 * m], ky = kin[3 * m + 1], k = kin[3 * m + 2];
+    double kx, ky, k;
+    if (ctr) {
+        ksample_row(S, *ctr, S.row0 + m, kx, ky, k);
+        kin[3 * m] = kx;
+        kin[3 * m + 1] = ky;
+        kin[3 * m + 2] = k;
+    } else {
+        kx = kin[3 * m];
+        ky = kin[3 * m + 1];
+        k = kin[3 * m + 2];
+    }
     KConst K;
     K.kx_2pi = kx / (2.0 * QEM_PI);
     K.ky_2pi = ky / (2.0 * QEM_PI);
@@ -84,11 +97,12 @@ __device__ __forceinline__ void kconst_one(int m, const double *__restrict__ kin
     kc[m] = K;
 }
 
-__global__ void k_kconst(int P, const double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
-                         double wk, double esc, const double *__restrict__ kwt, double wden, double eden)
+__global__ void k_kconst(int P, double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
+                         double wk, double esc, const double *__restrict__ kwt, double wden, double eden,
+                         const KSampler S, const unsigned long long *__restrict__ ctr)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m < P) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden);
+    if (m < P) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr);
 }
 
 // z-ordered SoA copy of the particles
@@ -129,13 +143,14 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
                                                           float *__restrict__ qf, double *__restrict__ qd,
                                                           double *__restrict__ qscan, double fscale,
                                                           double *__restrict__ k0, int P,
-                                                          const double *__restrict__ kin, KConst *__restrict__ kc,
+                                                          double *__restrict__ kin, KConst *__restrict__ kc,
                                                           double Lz, double g12, double wk, double esc,
                                                           const double *__restrict__ kwt, double wden, double eden,
-                                                          double zlim, unsigned *status)
+                                                          double zlim, unsigned *status, const KSampler S,
+                                                          const unsigned long long *__restrict__ ctr)
 {
     __shared__ double warp_tot[32];
-    for (int m = threadIdx.x; m < P; m += 1024) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden);
+    for (int m = threadIdx.x; m < P; m += 1024) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr);
     for (int m = threadIdx.x; m < N; m += 1024) {
         const double4 p = pos[zperm[m]];
         zrange_check(p.z - h, zlim, status);
@@ -668,11 +683,14 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     }
 }
 
-// F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term
+// F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term; ctr: the batch
+// counter of a per-call random batch, advanced once here, after every read of
+// it (the per-k constants kernel ran earlier on the same stream)
 __global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, const double *__restrict__ k0,
-                         const int *__restrict__ zperm, double *__restrict__ F3)
+                         const int *__restrict__ zperm, double *__restrict__ F3, unsigned long long *ctr)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctr && m == 0) *ctr += 1;
     if (m >= N) return;
     double fx = 0, fy = 0, fz = 0;
     for (int ks = 0; ks < ks_n; ks++) {
@@ -1135,7 +1153,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const double esc = P > 0 ? -(sum_K / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
         k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, b.qscan, fscale,
                                              b.k0, P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                             2.0 * eps0 * Lx * Ly, zlim, status);
+                                             2.0 * eps0 * Lx * Ly, zlim, status, b.sampler, b.draw_ctr);
         if (P > 0) {
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
@@ -1165,7 +1183,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
             const double wk = (sum_K / P) / (Lx * Ly * eps0);
             const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
             k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                                  2.0 * eps0 * Lx * Ly);
+                                                  2.0 * eps0 * Lx * Ly, b.sampler, b.draw_ctr);
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
@@ -1199,7 +1217,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
             k_lforce_f32<false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
                                                   b.Epart);
     }
-    k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3);
+    k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3, b.draw_ctr);
     return cudaGetLastError();
 }
 

@@ -106,3 +106,118 @@ def test_params_layout_and_gamma_above_one_rules(lib):
     assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.05, precision=L.QEM_FP32_FIX) == 1
     assert _create(lib, **base, mode_flags=L.QEM_PYTHON_MODE, pv_eps=0.05, N_t=4) == 1     # N_1 = 0
     assert _create(lib, Lz=2.0, gamma_up=1.0, gamma_down=1.0) == 1                         # the pole at k = 0
+
+
+# ---- the random-batch sampler (host restatement of the device draw) ----------
+U64 = np.uint64
+
+
+def _mix64(z):
+    z = (z ^ (z >> U64(30))) * U64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> U64(27))) * U64(0x94D049BB133111EB)
+    return z ^ (z >> U64(31))
+
+
+def _draw64(seed, a, b, c):
+    G = U64(0x9E3779B97F4A7C15)
+    with np.errstate(over="ignore"):
+        return _mix64(_mix64(_mix64(seed + G * (a + U64(1))) + G * (b + U64(1))) + G * (c + U64(1)))
+
+
+def sampler_rows(Lx, Ly, alpha, accuracy, seed, n, row0, P):
+    """numpy restatement of the library's batch draw: three SplitMix64 uniforms
+    per row, the m_x != 0 / m_x = 0 part, then inverse CDFs (math.exp is the
+    C library's exp, as in the library's tables)."""
+    import math
+
+    k_c = 2.0 * math.sqrt(-4.0 * alpha * math.log(accuracy))
+    M = [int(math.ceil(k_c * L / (2.0 * math.pi))) + 1 for L in (Lx, Ly)]
+
+    def cdf(Mi, L, skip0):
+        c, out = 0.0, []
+        for m in range(-Mi, Mi + 1):
+            if skip0 and m == 0:
+                continue
+            k = 2.0 * math.pi * m / L
+            c += math.exp(-k * k / (4.0 * alpha))
+            out.append(c)
+        return np.array(out)
+
+    cxa, cxn, cya, cyn = cdf(M[0], Lx, False), cdf(M[0], Lx, True), cdf(M[1], Ly, False), cdf(M[1], Ly, True)
+    Sx, Tx, Sy, Ty = cxn[-1], cxa[-1], cyn[-1], cya[-1]
+    rows = np.arange(row0, row0 + P, dtype=U64)
+    s = np.full(P, seed, dtype=U64)
+    nn = np.full(P, n, dtype=U64)
+    u = [(_draw64(s, nn, rows, np.full(P, j, dtype=U64)) >> U64(11)).astype(np.float64) * 2.0**-53 for j in range(3)]
+    A = Sx * Ty
+    partx = u[0] * (A + Sy) < A
+    pick = lambda c, v: np.minimum(np.searchsorted(c, v, side="right"), len(c) - 1)
+    ix = pick(cxn, u[1] * Sx)
+    mx = np.where(partx, np.where(ix < M[0], ix - M[0], ix - M[0] + 1), 0)
+    iy_all = pick(cya, u[2] * Ty) - M[1]
+    iyn = pick(cyn, u[2] * Sy)
+    my = np.where(partx, iy_all, np.where(iyn < M[1], iyn - M[1], iyn - M[1] + 1))
+    kx = 2.0 * np.pi * mx.astype(np.float64) / Lx
+    ky = 2.0 * np.pi * my.astype(np.float64) / Ly
+    return np.stack([kx, ky, np.sqrt(kx * kx + ky * ky)], 1), Sx + Sy + Sx * Sy
+
+
+def _draw(lib, Lx, Ly, alpha, seed, n, row0, P, accuracy=1e-6):
+    p = L.default_params()
+    p.Lx, p.Ly, p.alpha, p.accuracy = Lx, Ly, alpha, accuracy
+    k3 = np.zeros((max(P, 1), 3))
+    sK = C.c_double()
+    assert lib.qem_draw_kset(C.byref(p), seed, n, row0, P, k3.ctypes.data_as(C.POINTER(C.c_double)),
+                             C.byref(sK)) == 0
+    return k3[:P], sK.value
+
+
+@pytest.mark.parametrize("Lx,Ly,alpha", [(1000.0, 1000.0, 0.1), (30.0, 45.0, 0.1), (5.0, 400.0, 0.02)])
+def test_draw_kset_equals_its_restatement(lib, Lx, Ly, alpha):
+    """qem_draw_kset (the host copy of the device draw) against an independent
+    numpy restatement, bit for bit, for several batches and row offsets; sum_K
+    is K_set_generator.jl:28."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle as O
+
+    for seed, n, row0 in [(7, 0, 0), (7, 1, 0), (123456789, 41, 250), (2**63 + 5, 2**40, 3)]:
+        k3, sK = _draw(lib, Lx, Ly, alpha, seed, n, row0, 500)
+        r3, rsK = sampler_rows(Lx, Ly, alpha, 1e-6, seed, n, row0, 500)
+        np.testing.assert_array_equal(k3, r3)
+        assert sK == rsK
+    assert np.isclose(sK, O.kset_generator(Lx, Ly, alpha, 1e-6)[2], rtol=1e-12)
+    a, _ = _draw(lib, Lx, Ly, alpha, 7, 0, 0, 300)
+    b, _ = _draw(lib, Lx, Ly, alpha, 7, 1, 0, 300)
+    c, _ = _draw(lib, Lx, Ly, alpha, 7, 0, 100, 200)
+    assert not np.array_equal(a, b)
+    np.testing.assert_array_equal(a[100:], c)
+    assert np.all(a[:, 2] > 0)
+
+
+def test_draw_kset_distribution(lib):
+    """The draws follow exp(-k^2 / 4 alpha) / sum_K on the lattice without k = 0
+    (K_set_generator.jl:30-41): chi-square against the oracle's table."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle as O
+
+    Lx = Ly = 30.0
+    k3, _ = _draw(lib, Lx, Ly, 0.1, 99, 3, 0, 200_000)
+    K, P, _ = O.kset_generator(Lx, Ly, 0.1, 1e-6)
+    m = np.rint(k3[:, :2] * Lx / (2 * np.pi)).astype(int)
+    assert not np.any((m[:, 0] == 0) & (m[:, 1] == 0))
+    mref = np.rint(K[:, :2] * Lx / (2 * np.pi)).astype(int)
+    key = lambda a: a[:, 0] * 1000 + a[:, 1]
+    pref = dict(zip(key(mref), P.astype(np.float64)))
+    vals, cnt = np.unique(key(m), return_counts=True)
+    expected = np.array([pref[v] for v in vals]) * len(m)
+    sel = expected > 50
+    chi2 = np.sum((cnt[sel] - expected[sel]) ** 2 / expected[sel])
+    assert chi2 / sel.sum() < 1.5
+    # the mass of the rare cells is right too
+    assert abs(cnt[~sel].sum() - expected[~sel].sum()) < 5 * np.sqrt(max(expected[~sel].sum(), 1.0)) + 5
