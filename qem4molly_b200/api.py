@@ -30,6 +30,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib as L
+from . import _lib as _qem  # the constructors below take the reference's argument `L` (the box)
 
 
 def _mode_flags(mode: str) -> int:
@@ -282,7 +283,7 @@ class QEM_short:
         self.iter_period, self.gamma_1, self.gamma_2 = iter_period, gamma_1, gamma_2
         self.eps_0, self.accuracy, self.N_t = eps_0, accuracy, N_t
         self.n_steps = 0
-        flags = _mode_flags(mode) | (L.QEM_STALE_NEIGHBORS if stale_neighbors else 0)
+        flags = _mode_flags(mode) | (_qem.QEM_STALE_NEIGHBORS if stale_neighbors else 0)
         self.engine = Engine(L_box=self.L, alpha=alpha, r_cutoff=r_cutoff, gamma_1=gamma_1, gamma_2=gamma_2,
                              eps_0=eps_0, accuracy=accuracy, N_t=N_t, rbe_p=0, iter_period=iter_period,
                              mode_flags=flags, precision=_precision(precision), device=device)
@@ -300,7 +301,7 @@ class QEM_long:
         self.L, self.k_cutoff, self.z_list = tuple(L), k_cutoff, list(z_list)
         self.gamma_1, self.gamma_2, self.eps_0, self.accuracy = gamma_1, gamma_2, eps_0, accuracy
         self.alpha, self.rbe_mode, self.rbe_p = alpha, rbe_mode, rbe_p
-        flags = _mode_flags(mode) | (L.QEM_RESAMPLE_KSET if (resample and rbe_mode) else 0)
+        flags = _mode_flags(mode) | (_qem.QEM_RESAMPLE_KSET if (resample and rbe_mode) else 0)
         # the short-range cutoff is irrelevant for the long range; any value < L/2 is valid
         self.engine = Engine(L_box=self.L, alpha=alpha, r_cutoff=0.25 * min(self.L[0], self.L[1]),
                              gamma_1=gamma_1, gamma_2=gamma_2, eps_0=eps_0, accuracy=accuracy,

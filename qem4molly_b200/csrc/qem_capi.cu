@@ -369,9 +369,17 @@ static void build_consts(qem_handle *h)
     }
     c.Nt2 = (p.N_t + 1) / 2;
     for (int m = 0; m < c.Nt2; m++) {
-        const int a = 2 * m, b = 2 * m + 1;
-        c.xf2[m] = make_float2((float)x[a], b < p.N_t ? (float)x[b] : -1.0f);
-        c.wf2[m] = make_float2((float)w[a], b < p.N_t ? (float)w[b] : 0.0f);
+        // node pair (2m, 2m + 1); an odd N_t ends with a node at t = 0 of weight 0
+        double t[2], wn[2];
+        for (int j = 0; j < 2; j++) {
+            const int n = 2 * m + j;
+            t[j] = n < p.N_t ? 1.0 + x[n] : 0.0;
+            wn[j] = n < p.N_t ? w[n] : 0.0;
+        }
+        c.tf2[m] = make_float2((float)t[0], (float)t[1]);
+        c.wf2[m] = make_float2((float)wn[0], (float)wn[1]);
+        c.wtf2[m] = make_float2((float)(wn[0] * t[0]), (float)(wn[1] * t[1]));
+        c.rtf2[m] = make_float2(t[0] > 0 ? (float)(1.0 / sqrt(t[0])) : 0.0f, t[1] > 0 ? (float)(1.0 / sqrt(t[1])) : 0.0f);
     }
     // in-plane cells of side >= r_cutoff
     CellGeom &g = h->geom;

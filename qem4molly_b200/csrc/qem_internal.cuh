@@ -34,10 +34,13 @@ struct ShortConsts {
     double wall_cut[2], wall_sig2[2], wall_eps[2], wall_pos[2], wall_dir[2];
     // Gauss-Legendre nodes/weights on [-1, 1]: FP32 as node pairs (2m, 2m+1)
     // for the packed FP32x2 loop, an odd N_t padded with (x = -1, w = 0),
-    // i.e. a node at k = 0 of weight zero; FP64 as plain arrays
+    // i.e. a node at k = 0 of weight zero; FP64 as plain arrays.  The FP32
+    // loop reads node n of an interval [0, K] as k = h t_n, h = K / 2,
+    // t_n = 1 + x_n, and takes w_n t_n and 1 / sqrt(t_n) (0 at t_n = 0)
+    // from tables as well
     int Nt2;              // (N_t + 1) / 2
     int shard_world;      // W >= 1; the self terms and walls belong to rank 0
-    float2 xf2[QEM_MAX_NT / 2], wf2[QEM_MAX_NT / 2];
+    float2 tf2[QEM_MAX_NT / 2], wf2[QEM_MAX_NT / 2], wtf2[QEM_MAX_NT / 2], rtf2[QEM_MAX_NT / 2];
     double xd[QEM_MAX_NT], wd[QEM_MAX_NT];
     // gamma_1 gamma_2 > 1: regularised quadrature (FP64), family 0 Gauss, 1 point;
     // sub-interval t of family f has norm_n[f][t] nodes at norm_xw[norm_off[f][t]]
@@ -375,24 +378,44 @@ __device__ __forceinline__ float cos_ftz(float x)
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+__device__ __forceinline__ float sin_ftz(float x)
+{
+    float r;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // Bessel J0 and J1 in FP32 at two arguments x = (x0, x1) at once, one per
-// packed lane, from the polynomial approximations of Abramowitz & Stegun,
-// Handbook of Mathematical Functions, 9.4.1 / 9.4.4 (|x| <= 3) and 9.4.3 /
-// 9.4.6 (x >= 3; modulus/phase form); published absolute error <= 5e-8 (J0)
-// and <= 4e-8 (J1), i.e. at FP32 rounding level.  The coefficients are
-// rescaled so the small-x series run in y = x^2 (A&S use (x/3)^2) and the
-// large-x series in u = 1/x (A&S use 3/x).  A branch runs when either lane
-// needs it and each lane keeps its own branch's result.  Large-x phases
-// theta0,1 = x - (pi/4, 3 pi/4) + (p0, p1) are reduced modulo 2 pi by
-// n = round(theta / 2 pi) (adding and subtracting 1.5 * 2^23, valid while
-// |theta| / 2 pi < 2^22) and a two-term Cody-Waite split of 2 pi.
+// packed lane; R = x^{-1/2} is supplied by the caller.
+//  * x < 3: the polynomial approximations of Abramowitz & Stegun, Handbook of
+//    Mathematical Functions, 9.4.1 / 9.4.4 (published absolute error <= 5e-8
+//    for J0, <= 1.3e-8 for J1), coefficients rescaled to run in y = x^2 (A&S
+//    use (x/3)^2).
+//  * x >= 3: the Hankel asymptotic form with fitted amplitudes: t = x - pi/4,
+//    u = 1/x, w = u^2,
+//        J0 = R (P0(w) cos t + u Q0(w) sin t),  J1 = R (P1(w) sin t + u Q1(w) cos t),
+//    P of degree 5 and Q of degree 4, near-minimax fits on w in (0, 1/9] made
+//    by gen_bessel_pq.py in this directory (sqrt(2/pi) and the signs folded
+//    in); one sine and one cosine of t serve both orders.  Error of the whole
+//    FP32 evaluation (that script's emulation): <= 1.1e-7 on [3, 25].
+//    t is reduced modulo 2 pi by n = round(t / 2 pi) (adding and subtracting
+//    1.5 * 2^23, valid while |t| / 2 pi < 2^22) and a two-term split of 2 pi.
+// A branch runs when either lane needs it and each lane keeps its own
+// branch's result.
 namespace bj {
 __host__ __device__ constexpr float s9(double c, int j) { return (float)(c / (j == 0 ? 1.0 : j == 1 ? 9.0 : j == 2 ? 81.0 : j == 3 ? 729.0 : j == 4 ? 6561.0 : j == 5 ? 59049.0 : 531441.0)); }
-__host__ __device__ constexpr float s3(double c, int j) { return (float)(c * (j == 0 ? 1.0 : j == 1 ? 3.0 : j == 2 ? 9.0 : j == 3 ? 27.0 : j == 4 ? 81.0 : j == 5 ? 243.0 : 729.0)); }
+// gen_bessel_pq.py: coefficients of w^0 .. w^deg
+constexpr float P0_0 = 7.978845024e-01f, P0_1 = -5.607697060e-02f, P0_2 = 8.693327505e-02f,
+                P0_3 = -3.358948571e-01f, P0_4 = 1.346355509e+00f, P0_5 = -2.857244828e+00f;
+constexpr float Q0_0 = 9.973312039e-02f, Q0_1 = -5.799857766e-02f, Q0_2 = 1.549632535e-01f,
+                Q0_3 = -5.666049405e-01f, Q0_4 = 1.216355152e+00f;
+constexpr float P1_0 = 7.978846274e-01f, P1_1 = 9.347446406e-02f, P1_2 = -1.121584213e-01f,
+                P1_3 = 4.034436691e-01f, P1_4 = -1.577854617e+00f, P1_5 = 3.316100318e+00f;
+constexpr float Q1_0 = 2.992038999e-01f, Q1_1 = -8.131090927e-02f, Q1_2 = 1.916038321e-01f,
+                Q1_3 = -6.738063288e-01f, Q1_4 = 1.426397851e+00f;
 }  // namespace bj
 
-__device__ __forceinline__ void bessel01_x2(float2 x, float2 &J0, float2 &J1)
+__device__ __forceinline__ void bessel01_x2(float2 x, float2 R, float2 &J0, float2 &J1)
 {
     using namespace bj;
     const bool s0 = x.x < 3.0f, s1 = x.y < 3.0f;
@@ -412,40 +435,33 @@ __device__ __forceinline__ void bessel01_x2(float2 x, float2 &J0, float2 &J1)
         J1 = mul2(x, fma2(y, b, f2s(0.5f)));
     }
     if (!(s0 && s1)) {
-        const float2 r = f2(rsqrt_ftz(x.x), rsqrt_ftz(x.y));
-        const float2 u = mul2(r, r);  // 1 / x
-        float2 f = fma2(u, f2s(s3(0.00014476, 6)), f2s(s3(-0.00072805, 5)));
-        f = fma2(u, f, f2s(s3(0.00137237, 4)));
-        f = fma2(u, f, f2s(s3(-0.00009512, 3)));
-        f = fma2(u, f, f2s(s3(-0.00552740, 2)));
-        f = fma2(u, f, f2s(s3(-0.00000077, 1)));
-        f = fma2(u, f, f2s(0.79788456f));
-        float2 g = fma2(u, f2s(s3(-0.00020033, 6)), f2s(s3(0.00113653, 5)));
-        g = fma2(u, g, f2s(s3(-0.00249511, 4)));
-        g = fma2(u, g, f2s(s3(0.00017105, 3)));
-        g = fma2(u, g, f2s(s3(0.01659667, 2)));
-        g = fma2(u, g, f2s(s3(0.00000156, 1)));
-        g = fma2(u, g, f2s(0.79788456f));
-        // phase corrections p = t P(t), t = 3u: u (3^(j+1) c_j) u^j
-        float2 p = fma2(u, f2s(s3(0.00013558, 6)), f2s(s3(-0.00029333, 5)));
-        p = fma2(u, p, f2s(s3(-0.00054125, 4)));
-        p = fma2(u, p, f2s(s3(0.00262573, 3)));
-        p = fma2(u, p, f2s(s3(-0.00003954, 2)));
-        p = fma2(u, p, f2s(s3(-0.04166397, 1)));
-        float2 q = fma2(u, f2s(s3(-0.00029166, 6)), f2s(s3(0.00079824, 5)));
-        q = fma2(u, q, f2s(s3(0.00074348, 4)));
-        q = fma2(u, q, f2s(s3(-0.00637879, 3)));
-        q = fma2(u, q, f2s(s3(0.00005650, 2)));
-        q = fma2(u, q, f2s(s3(0.12499612, 1)));
-        float2 th0 = fma2(u, p, add2(x, f2s(-0.78539816f)));
-        float2 th1 = fma2(u, q, add2(x, f2s(-2.35619449f)));
+        const float2 u = mul2(R, R);  // 1 / x
+        const float2 w = mul2(u, u);
+        float2 p0 = fma2(w, f2s(P0_5), f2s(P0_4));
+        p0 = fma2(w, p0, f2s(P0_3));
+        p0 = fma2(w, p0, f2s(P0_2));
+        p0 = fma2(w, p0, f2s(P0_1));
+        p0 = fma2(w, p0, f2s(P0_0));
+        float2 p1 = fma2(w, f2s(P1_5), f2s(P1_4));
+        p1 = fma2(w, p1, f2s(P1_3));
+        p1 = fma2(w, p1, f2s(P1_2));
+        p1 = fma2(w, p1, f2s(P1_1));
+        p1 = fma2(w, p1, f2s(P1_0));
+        float2 q0 = fma2(w, f2s(Q0_4), f2s(Q0_3));
+        q0 = fma2(w, q0, f2s(Q0_2));
+        q0 = fma2(w, q0, f2s(Q0_1));
+        q0 = fma2(w, q0, f2s(Q0_0));
+        float2 q1 = fma2(w, f2s(Q1_4), f2s(Q1_3));
+        q1 = fma2(w, q1, f2s(Q1_2));
+        q1 = fma2(w, q1, f2s(Q1_1));
+        q1 = fma2(w, q1, f2s(Q1_0));
+        float2 t = add2(x, f2s(-0.78539816f));
         const float2 MAGIC = f2s(12582912.0f), INV2PI = f2s(0.15915494309189535f);
-        const float2 n0 = add2(fma2(th0, INV2PI, MAGIC), f2s(-12582912.0f));
-        const float2 n1 = add2(fma2(th1, INV2PI, MAGIC), f2s(-12582912.0f));
-        th0 = fma2(n0, f2s(1.7484555314695172e-07f), fma2(n0, f2s(-6.28318548202514648f), th0));
-        th1 = fma2(n1, f2s(1.7484555314695172e-07f), fma2(n1, f2s(-6.28318548202514648f), th1));
-        const float2 L0 = mul2(mul2(f, r), f2(cos_ftz(th0.x), cos_ftz(th0.y)));
-        const float2 L1 = mul2(mul2(g, r), f2(cos_ftz(th1.x), cos_ftz(th1.y)));
+        const float2 n = add2(fma2(t, INV2PI, MAGIC), f2s(-12582912.0f));
+        t = fma2(n, f2s(1.7484555314695172e-07f), fma2(n, f2s(-6.28318548202514648f), t));
+        const float2 S = f2(sin_ftz(t.x), sin_ftz(t.y)), C = f2(cos_ftz(t.x), cos_ftz(t.y));
+        const float2 L0 = mul2(R, fma2(p0, C, mul2(mul2(u, q0), S)));
+        const float2 L1 = mul2(R, fma2(p1, S, mul2(mul2(u, q1), C)));
         if (!s0) { J0.x = L0.x; J1.x = L1.x; }
         if (!s1) { J0.y = L0.y; J1.y = L1.y; }
     }

@@ -28,10 +28,11 @@
 //
 // FP32 path: per-pair set-up (minimum image, rho, image distances, quadrature
 // limits, closed-form image terms) and all cross-image sums in FP64; the
-// per-node integrands in FP32 with hardware exp / rcp / cos and the
-// Abramowitz-Stegun Bessel approximations, two nodes per packed FP32x2
-// instruction (the kernel is instruction-issue bound, and the packed
-// arithmetic halves the issue slots of everything but the MUFU operations).
+// per-node integrands in FP32 with hardware exp / rcp / sin / cos and
+// polynomial Bessel approximations (bessel01_x2), two nodes per packed FP32x2
+// instruction (the kernel is bound by FMA, MUFU and issue together, and the
+// packed arithmetic halves the issue slots of everything but the MUFU
+// operations).
 // The denominator D is formed as
 // (1 - g_u g_d) + g_u g_d (1 - e^{-t}) with (1 - g_u g_d) from FP64 and
 // 1 - e^{-t} evaluated without cancellation, so its relative error stays at
@@ -116,51 +117,60 @@ __device__ __forceinline__ void quad_f64(const ShortConsts &c, const Interval &v
 }
 
 // FP32 nodes two at a time in packed FP32x2 lanes (nodes 2m, 2m+1, Bessel
-// functions included); the exponentials as 2^(...) with log2(e) folded into
-// the per-interval constants; 1 - e^{-t} by its series below t = 0.5; the
-// two lanes' partial sums are added at the end.
+// functions included).  Node n of the interval [0, K] is k = h t_n
+// (h = K / 2, t_n = 1 + x_n), so every per-node quantity is t_n times an
+// interval constant: the exponentials as 2^(t ...) with log2(e) folded in,
+// x = k rho = t (h rho) and x^{-1/2} = (h rho)^{-1/2} / sqrt(t_n) from the
+// node table.  The sums run over (w_n t_n) e^{...} / D (and w_n e^{...} / D
+// for the energy); the interval's factors h^2 pf (h pf) are applied in FP64
+// by the caller.  1 - e^{-2 k L_z} is taken from its series below
+// 2 k L_z = 0.5; the two lanes' partial sums are added at the end.
 template <bool ENERGY, bool WITH_J1>
-__device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, float rho, float &Ir, float &Iz,
-                                         float &Iu)
+__device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
+                                         double &Iu)
 {
     constexpr double LOG2E = 1.4426950408889634;
-    const float2 h = f2s(0.5f * (float)v.K);
-    const float2 ae = f2s((float)(-LOG2E * v.ae)), c2 = f2s((float)(-LOG2E * v.c2)), pf = f2s((float)v.pf);
-    const float2 nt = f2s((float)(-LOG2E * c.twoLz));  // e^{-t} = 2^(k nt)
+    const double h = 0.5 * v.K;
+    const float2 hn = f2s((float)(-LOG2E * c.twoLz * h));  // e^{-2 k L_z} = 2^(t hn)
+    const float2 A1 = f2s((float)(-LOG2E * v.ae * h));      // e^{-k (a' + c2 k)} = 2^(t (A1 + t A2))
+    const float2 A2 = f2s((float)(-LOG2E * v.c2 * h * h));
     const float2 g12 = f2s((float)c.g12), omg = f2s((float)c.one_minus_g12);
-    const float2 rho2 = f2s(rho), twoLz = f2s((float)c.twoLz);
-    const float tsmall = (float)(-0.5 * LOG2E);         // k nt > tsmall  <=>  t < 0.5
+    const float2 tL = f2s((float)(c.twoLz * h));            // 2 k L_z = t tL
+    const float hrf = (float)(h * rho);
+    const float2 hr = f2s(hrf);                              // x = k rho = t hr
+    const float2 rs = f2s(WITH_J1 ? rsqrt_ftz(hrf) : 0.f);   // x^{-1/2} = rs / sqrt(t)
+    const float tsmall = (float)(-0.5 * LOG2E);              // t hn > tsmall  <=>  2 k L_z < 0.5
     float2 r = f2s(0.f), z = f2s(0.f), u = f2s(0.f);
 #pragma unroll NODE_UNROLL
     for (int m = 0; m < c.Nt2; m++) {
-        const float2 k = fma2(h, c.xf2[m], h);
-        const float2 w = mul2(h, c.wf2[m]);
-        const float2 s = mul2(k, nt);
-        float2 om = fma2(f2(ex2_approx(s.x), ex2_approx(s.y)), f2s(-1.0f), f2s(1.0f));  // 1 - e^{-t}
+        const float2 t = c.tf2[m];
+        const float2 s = mul2(t, hn);
+        float2 om = fma2(f2(ex2_approx(s.x), ex2_approx(s.y)), f2s(-1.0f), f2s(1.0f));  // 1 - e^{-2 k L_z}
         if (s.x > tsmall) {  // nodes ascend, so lane x holds the smaller k
-            const float2 t = mul2(k, twoLz);
-            const float2 tay = one_minus_exp_neg_series(t);
-            if (t.x < 0.5f) om.x = tay.x;
-            if (t.y < 0.5f) om.y = tay.y;
+            const float2 tt = mul2(t, tL);
+            const float2 tay = one_minus_exp_neg_series(tt);
+            if (tt.x < 0.5f) om.x = tay.x;
+            if (tt.y < 0.5f) om.y = tay.y;
         }
-        const float2 Dp = fma2(g12, om, omg);  // 1 - g12 e^{-t} > 0
-        const float2 ex = mul2(k, fma2(k, c2, ae));
-        const float2 G = mul2(mul2(pf, f2(ex2_approx(ex.x), ex2_approx(ex.y))),
-                              f2(fast_rcp(Dp.x), fast_rcp(Dp.y)));
-        const float2 wG = mul2(w, G);
-        const float2 cw = mul2(wG, k);
+        const float2 Dp = fma2(g12, om, omg);  // 1 - g12 e^{-2 k L_z} > 0
+        const float2 ex = mul2(t, fma2(t, A2, A1));
+        const float2 eD = mul2(f2(ex2_approx(ex.x), ex2_approx(ex.y)), f2(fast_rcp(Dp.x), fast_rcp(Dp.y)));
+        const float2 cw = mul2(c.wtf2[m], eD);
         if (WITH_J1) {
             float2 J0, J1;
-            bessel01_x2(mul2(k, rho2), J0, J1);
+            bessel01_x2(mul2(t, hr), mul2(rs, c.rtf2[m]), J0, J1);
             r = fma2(cw, J1, r);
             z = fma2(cw, J0, z);
-            if (ENERGY) u = fma2(wG, J0, u);
+            if (ENERGY) u = fma2(mul2(c.wf2[m], eD), J0, u);
         } else {
             z = add2(z, cw);
-            if (ENERGY) u = add2(u, wG);
+            if (ENERGY) u = fma2(c.wf2[m], eD, u);
         }
     }
-    Ir = r.x + r.y; Iz = z.x + z.y; Iu = u.x + u.y;
+    const double s2 = h * h * v.pf;
+    Ir = s2 * (double)(r.x + r.y);
+    Iz = s2 * (double)(z.x + z.y);
+    Iu = ENERGY ? h * v.pf * (double)(u.x + u.y) : 0.0;
 }
 
 // gamma_1 gamma_2 > 1 (python_lib Force_short_norm_njit.py:11-414,
@@ -243,9 +253,7 @@ __device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, do
     } else if (PREC == QEM_FP64) {
         quad_f64<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
     } else {
-        float r, z, u;
-        quad_f32<ENERGY, WITH_J1>(c, v, (float)rho, r, z, u);
-        Ir = r; Iz = z; Iu = u;
+        quad_f32<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
     }
 }
 

@@ -10,7 +10,10 @@ dielectric contrast where 1 - g_u g_d e^{-2 k L_z} loses digits).
 * FP64 GPU against the CPU oracle on sub-samples: short-range forces of the
   particles of a 150 x 150 window (the oracle evaluates the window plus an
   r_c halo; particles at least r_c inside compare) at <= 1e-11, and the long
-  range for all N on a 32-vector subset of the k-set at <= 1e-9.
+  range for all N on a 32-vector subset of the k-set at <= 1e-8 (the oracle
+  restates the reference's "total minus running sum" suffix sums,
+  Force_long.jl:97-98, which lose digits in proportion to e^{k L_z}: about
+  1e-9 .. 5e-9 for the larger k of a batch at L_z = 10).
 """
 import json
 import os
@@ -87,4 +90,4 @@ def test_config5_fp64_long_vs_oracle_ksubset(stress):
     F = e.forces(cfg["xyz"], cfg["q"], terms=L.QEM_TERM_LONG)
     p = O.params(cfg["L"], cfg["alpha"], cfg["r_cutoff"], cfg["gamma_down"], cfg["gamma_up"])
     Fo = O.F_long(p, cfg["xyz"], cfg["q"], k3, sK)
-    assert W.rel_err(F, Fo)[0] <= 1e-9
+    assert W.rel_err(F, Fo)[0] <= 1e-8
