@@ -367,6 +367,12 @@ static void build_consts(qem_handle *h)
             }
         }
     }
+    c.f_nlog2e_2Lz = (float)(-1.4426950408889634 * c.twoLz);
+    c.f_nlog2e_c2 = (float)(-1.4426950408889634 * c.inv4alpha);
+    c.f_2Lz = (float)c.twoLz;
+    c.f_g12 = (float)c.g12;
+    c.f_omg12 = (float)c.one_minus_g12;
+    c.bins_per_rc2 = 64.0 / c.rc2;  // RHO_BINS of k_short_pair
     c.Nt2 = (p.N_t + 1) / 2;
     for (int m = 0; m < c.Nt2; m++) {
         // node pair (2m, 2m + 1); an odd N_t ends with a node at t = 0 of weight 0

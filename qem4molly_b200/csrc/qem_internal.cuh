@@ -45,6 +45,10 @@ struct ShortConsts {
     // gamma_1 gamma_2 > 1: regularised quadrature (FP64), family 0 Gauss, 1 point;
     // sub-interval t of family f has norm_n[f][t] nodes at norm_xw[norm_off[f][t]]
     // and weights right after them
+    // FP32 factors of the node loop: -log2(e) 2 L_z, -log2(e) / (4 alpha),
+    // 2 L_z, g_u g_d, 1 - g_u g_d; RHO_BINS / r_c^2 of the pair grouping
+    float f_nlog2e_2Lz, f_nlog2e_c2, f_2Lz, f_g12, f_omg12;
+    double bins_per_rc2;
     int norm;
     double k0, pv_eps, kf_norm[2];
     int norm_n[2][4], norm_off[2][4];

@@ -22,7 +22,7 @@
 //   D = 1 - g_u g_d e^{-2 k L_z},
 // every interval is G = pf exp(-k (a' + c2 k)) / D for per-interval (pf, a', c2),
 // so the 8 intervals run through one rolled loop (small code, no instruction
-// cache misses).  Each block orders its 256 pairs by rho in shared memory
+// cache misses).  Each block groups its 256 pairs by rho in shared memory
 // before the quadrature, so the threads of a warp mostly take the same
 // Bessel branch; records are still written at the pair's own index.
 //
@@ -44,7 +44,8 @@ namespace {
 #ifndef QEM_PAIR_BLOCK
 #define QEM_PAIR_BLOCK 256
 #endif
-constexpr int PAIR_BLOCK = QEM_PAIR_BLOCK;  // pairs per block, ordered by rho in shared memory
+constexpr int PAIR_BLOCK = QEM_PAIR_BLOCK;  // pairs per block, grouped by rho in shared memory
+constexpr int RHO_BINS = 64;                // rho^2 bins of the grouping (a multiple of 32)
 // resident pair blocks per SM requested from the register allocator, and the
 // unroll factor of the FP32 node loop (tuning knobs; measured defaults)
 #ifndef QEM_PAIR_MINB
@@ -126,17 +127,20 @@ __device__ __forceinline__ void quad_f64(const ShortConsts &c, const Interval &v
 // by the caller.  1 - e^{-2 k L_z} is taken from its series below
 // 2 k L_z = 0.5; the two lanes' partial sums are added at the end.
 template <bool ENERGY, bool WITH_J1>
-__device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
+__device__ __forceinline__ void quad_f32(const ShortConsts &c, const Interval &v, float rho_f, double &Ir, double &Iz,
                                          double &Iu)
 {
-    constexpr double LOG2E = 1.4426950408889634;
+    constexpr float LOG2E = 1.4426950408889634f;
     const double h = 0.5 * v.K;
-    const float2 hn = f2s((float)(-LOG2E * c.twoLz * h));  // e^{-2 k L_z} = 2^(t hn)
-    const float2 A1 = f2s((float)(-LOG2E * v.ae * h));      // e^{-k (a' + c2 k)} = 2^(t (A1 + t A2))
-    const float2 A2 = f2s((float)(-LOG2E * v.c2 * h * h));
-    const float2 g12 = f2s((float)c.g12), omg = f2s((float)c.one_minus_g12);
-    const float2 tL = f2s((float)(c.twoLz * h));            // 2 k L_z = t tL
-    const float hrf = (float)(h * rho);
+    // interval constants in FP32 from one conversion of h (and of a'); the
+    // per-kernel factors come from ShortConsts
+    const float hf = (float)h;
+    const float2 hn = f2s(hf * c.f_nlog2e_2Lz);             // e^{-2 k L_z} = 2^(t hn)
+    const float2 A1 = f2s(hf * (-LOG2E) * (float)v.ae);     // e^{-k (a' + c2 k)} = 2^(t (A1 + t A2))
+    const float2 A2 = f2s(v.c2 != 0.0 ? hf * hf * c.f_nlog2e_c2 : 0.0f);
+    const float2 g12 = f2s(c.f_g12), omg = f2s(c.f_omg12);
+    const float2 tL = f2s(hf * c.f_2Lz);                     // 2 k L_z = t tL
+    const float hrf = hf * rho_f;
     const float2 hr = f2s(hrf);                              // x = k rho = t hr
     const float2 rs = f2s(WITH_J1 ? rsqrt_ftz(hrf) : 0.f);   // x^{-1/2} = rs / sqrt(t)
     const float tsmall = (float)(-0.5 * LOG2E);              // t hn > tsmall  <=>  2 k L_z < 0.5
@@ -244,8 +248,8 @@ __device__ void quad_norm_f64(const ShortConsts &c, const Interval &v, double rh
 }
 
 template <int PREC, bool ENERGY, bool WITH_J1>
-__device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, double rho, double &Ir, double &Iz,
-                                     double &Iu)
+__device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, double rho, float rho_f, double &Ir,
+                                     double &Iz, double &Iu)
 {
     if (PREC == QEM_FP64 && c.norm) {
         quad_norm_f64<WITH_J1>(c, v, rho, Ir, Iz);
@@ -253,7 +257,7 @@ __device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, do
     } else if (PREC == QEM_FP64) {
         quad_f64<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
     } else {
-        quad_f32<ENERGY, WITH_J1>(c, v, rho, Ir, Iz, Iu);
+        quad_f32<ENERGY, WITH_J1>(c, v, rho_f, Ir, Iz, Iu);
     }
 }
 
@@ -272,41 +276,52 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
                                                                            double *__restrict__ Upair,
                                                                            const ShortConsts c)
 {
-    __shared__ double skey[PAIR_BLOCK];
+    __shared__ int hist[RHO_BINS];
     __shared__ int sidx[PAIR_BLOCK];
     const int64_t Np = min(*np, cap);
     if ((int64_t)blockIdx.x * PAIR_BLOCK >= Np) return;  // whole block: before any barrier
     // this rank's block of the pair list (all of it unless sharded)
     const int64_t lo = Np * c.shard_rank / c.shard_world, hi = Np * (c.shard_rank + 1) / c.shard_world;
-    // 1. every thread loads one pair and its rho^2; order the block's pairs by rho^2
+    // 1. every thread loads one pair and its rho^2; the block's pairs are
+    // grouped by rho^2 (a counting sort into RHO_BINS bins of equal width,
+    // equal population for pairs uniform in the plane), so that the threads of
+    // a warp cross the Bessel branch point at nearly the same node.  The order
+    // inside a bin depends on the atomics, but every thread evaluates and
+    // writes its own pair, so the results do not.
     {
+        if (threadIdx.x < RHO_BINS) hist[threadIdx.x] = 0;
+        __syncthreads();
         const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + threadIdx.x;
-        double key = 1e300;
+        int bin = RHO_BINS - 1;
         if (p >= lo && p < hi) {
             const int2 ij = pairs[p];
             const double4 pi = pos[ij.x], pj = pos[ij.y];
             const double dx = min_image(pi.x - pj.x, c.Lx, c.invLx), dy = min_image(pi.y - pj.y, c.Ly, c.invLy);
-            key = dx * dx + dy * dy;
+            bin = min(RHO_BINS - 1, (int)((dx * dx + dy * dy) * c.bins_per_rc2));
         }
-        skey[threadIdx.x] = key;
-        sidx[threadIdx.x] = threadIdx.x;
+        const int slot = atomicAdd(&hist[bin], 1);
         __syncthreads();
-        for (int size = 2; size <= PAIR_BLOCK; size <<= 1) {
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                const int t = threadIdx.x;
-                const int partner = t ^ stride;
-                if (partner > t) {
-                    const bool up = ((t & size) == 0);
-                    const double ka = skey[t], kb = skey[partner];
-                    if ((ka > kb) == up) {
-                        skey[t] = kb; skey[partner] = ka;
-                        const int ia = sidx[t];
-                        sidx[t] = sidx[partner]; sidx[partner] = ia;
-                    }
-                }
-                __syncthreads();
+        if (threadIdx.x < 32) {  // exclusive scan of the bin counts (RHO_BINS / 32 per lane)
+            constexpr int PER = RHO_BINS / 32;
+            int v[PER], tot = 0;
+#pragma unroll
+            for (int j = 0; j < PER; j++) {
+                v[j] = tot;
+                tot += hist[threadIdx.x * PER + j];
             }
+            int x = tot;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, x, d);
+                if ((int)threadIdx.x >= d) x += t;
+            }
+            const int base = x - tot;
+#pragma unroll
+            for (int j = 0; j < PER; j++) hist[threadIdx.x * PER + j] = base + v[j];
         }
+        __syncthreads();
+        sidx[hist[bin] + slot] = threadIdx.x;
+        __syncthreads();
     }
     const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + sidx[threadIdx.x];
     if (p >= Np) return;
@@ -330,6 +345,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
         return;
     }
     const double rho = sqrt(rho2);
+    const float rho_f = (float)rho;
     const double zi = pi.z, zj = pj.z;
     const double zn = fabs(zi - zj), zp = zi + zj;
     const double s = jl_sign(zi - zj);
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
         const double si = (l == 0) ? -s : (l == 1) ? -1.0 : (l == 2) ? 1.0 : s;  // greens_function.jl:24
         const double sj = (l == 1 || l == 2) ? si : -si;                          // the element seen from j
         double Ir, Iz, Iu;
-        quad<PREC, ENERGY, true>(c, interval(c, a, b, gauss), rho, Ir, Iz, Iu);
+        quad<PREC, ENERGY, true>(c, interval(c, a, b, gauss), rho, rho_f, Ir, Iz, Iu);
         const double sf = gauss ? 1.0 : -1.0;
         Fr += sf * Ir;
         Fzi -= sf * si * Iz;
@@ -392,7 +408,7 @@ __device__ void self_terms(const ShortConsts &c, double z, double q, double &Fz,
         const double b = (l == 0) ? 1.0 : (l == 1) ? c.g1 : (l == 2) ? c.g2 : c.g12;
         const double sa = (l == 1) ? -1.0 : (l == 2) ? 1.0 : 0.0;
         double Ir, Iz, Iu;
-        quad<PREC, ENERGY, false>(c, interval(c, a, b, gauss), 0.0, Ir, Iz, Iu);
+        quad<PREC, ENERGY, false>(c, interval(c, a, b, gauss), 0.0, 0.0f, Ir, Iz, Iu);
         // -Fp1 + Fg; with g12 > 1 the reference adds the point part with the
         // opposite sign (Force_short_norm_njit.py:330-331), reproduced
         const double sf = (gauss || (PREC == QEM_FP64 && c.norm)) ? 1.0 : -1.0;
