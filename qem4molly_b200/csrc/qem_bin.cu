@@ -725,13 +725,17 @@ __global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__re
 }
 
 // ---------------------------------------------------------------------------
-// z order: bitonic sort of 1024-element tiles in shared memory, then merge
-// passes by co-ranking.  Keys are (z, index): a total order, so the result is
-// the stable ascending order of z.  Non-finite z was zeroed by k_pack.  REV
-// orders equal z by descending index instead (the second order of the
-// equal-z tie mode).
+// z order.  Keys are (z, index): a total order, so the result is the stable
+// ascending order of z (sortperm, QEM_long.jl:39-40); non-finite z was zeroed
+// by k_pack.  REV orders equal z by descending index instead (the second
+// order of the equal-z tie mode).  Tiles of ZTILE keys are sorted by rank
+// (each thread counts the keys of its tile that precede its own), then runs
+// are merged ZWAY at a time: every key counts, by binary search, the keys
+// that precede it in the other runs of its group.  With distinct keys both
+// steps place every key exactly.
 // ---------------------------------------------------------------------------
-constexpr int ZTILE = 1024;
+constexpr int ZTILE = 256;
+constexpr int ZWAY = 8;
 
 template <bool REV>
 __device__ __forceinline__ bool zless(double za, int ia, double zb, int ib)
@@ -740,45 +744,28 @@ __device__ __forceinline__ bool zless(double za, int ia, double zb, int ib)
 }
 
 template <bool REV>
-__global__ void k_ztile(int N, const double4 *__restrict__ pos, double *__restrict__ key, int *__restrict__ idx)
+__global__ void __launch_bounds__(ZTILE) k_ztile(int N, const double4 *__restrict__ pos, double *__restrict__ key,
+                                                 int *__restrict__ idx)
 {
     __shared__ double sk[ZTILE];
     __shared__ int si[ZTILE];
-    int base = blockIdx.x * ZTILE;
-    for (int t = threadIdx.x; t < ZTILE; t += blockDim.x) {
-        int i = base + t;
-        if (i < N) {
-            sk[t] = pos[i].z;
-            si[t] = i;
-        } else {
-            sk[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
-            si[t] = 0x7fffffff;
-        }
+    const int base = blockIdx.x * ZTILE;
+    const int i = base + threadIdx.x;
+    double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
+    int me = 0x7fffffff;
+    if (i < N) {
+        z = pos[i].z;
+        me = i;
     }
+    sk[threadIdx.x] = z;
+    si[threadIdx.x] = me;
     __syncthreads();
-    for (int size = 2; size <= ZTILE; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int t = threadIdx.x; t < ZTILE / 2; t += blockDim.x) {
-                int lo = 2 * t - (t & (stride - 1));
-                int hi = lo + stride;
-                bool up = ((lo & size) == 0);
-                double ka = sk[lo], kb = sk[hi];
-                int ia = si[lo], ib = si[hi];
-                bool swap = up ? zless<REV>(kb, ib, ka, ia) : zless<REV>(ka, ia, kb, ib);
-                if (swap) {
-                    sk[lo] = kb; sk[hi] = ka;
-                    si[lo] = ib; si[hi] = ia;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    for (int t = threadIdx.x; t < ZTILE; t += blockDim.x) {
-        int i = base + t;
-        if (i < N) {
-            key[i] = sk[t];
-            idx[i] = si[t];
-        }
+    int rank = 0;
+#pragma unroll 8
+    for (int j = 0; j < ZTILE; j++) rank += zless<REV>(sk[j], si[j], z, me) ? 1 : 0;
+    if (i < N) {
+        key[base + rank] = z;
+        idx[base + rank] = me;
     }
 }
 
@@ -786,35 +773,28 @@ template <bool REV>
 __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
                          double *__restrict__ key_out, int *__restrict__ idx_out)
 {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
-    int run = p / width;
-    int lstart = (run & ~1) * width;
-    int rstart = lstart + width;
-    int lend = min(rstart, N), rend = min(rstart + width, N);
-    double kz = key[p];
-    int ki = idx[p];
-    int pos_out;
-    if ((run & 1) == 0) {
-        // left element: count right-run elements strictly before it
-        int lo = rstart, hi = rend;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
+    const int run = p / width;
+    const int gstart = (run - run % ZWAY) * width;  // first key of this group of ZWAY runs
+    const double kz = key[p];
+    const int ki = idx[p];
+    int pos = gstart + (p - run * width);  // own rank inside the run
+#pragma unroll 1
+    for (int r = 0; r < ZWAY; r++) {
+        const int rs = gstart + r * width;
+        if (rs >= N) break;
+        if (rs == run * width) continue;
+        int lo = rs, hi = min(rs + width, N);
+        while (lo < hi) {  // keys of run r that precede (kz, ki)
+            const int mid = (lo + hi) >> 1;
             if (zless<REV>(key[mid], idx[mid], kz, ki)) lo = mid + 1;
             else hi = mid;
         }
-        pos_out = lstart + (p - lstart) + (lo - rstart);
-    } else {
-        int lo = lstart, hi = lend;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (zless<REV>(key[mid], idx[mid], kz, ki)) lo = mid + 1;
-            else hi = mid;
-        }
-        pos_out = lstart + (p - rstart) + (lo - lstart);
+        pos += lo - rs;
     }
-    key_out[pos_out] = kz;
-    idx_out[pos_out] = ki;
+    key_out[pos] = kz;
+    idx_out[pos] = ki;
 }
 
 inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
@@ -843,13 +823,14 @@ size_t qem_scan_tmp_bytes(int n) { return sizeof(double) * (size_t)(nblk(n, SCAN
 int qem_scan_launches(int n) { return n <= SCAN_SMALL_MAX_INT ? 1 : 3; }
 int qem_scan_f64_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
 
-int qem_zsort_launches(int N)
+static int zsort_passes(int N)
 {
-    if (N <= 0) return 0;
     int passes = 0;
-    for (int w = ZTILE; w < N; w <<= 1) passes++;
-    return 1 + passes;
+    for (int64_t w = ZTILE; w < N; w *= ZWAY) passes++;
+    return passes;
 }
+
+int qem_zsort_launches(int N) { return N <= 0 ? 0 : 1 + zsort_passes(N); }
 
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
@@ -947,23 +928,17 @@ cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, d
                              cudaStream_t s, bool rev_ties)
 {
     if (N <= 0) return cudaSuccess;
-    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
-    else k_ztile<false><<<nblk(N, ZTILE), 256, 0, s>>>(N, pos, zkey, zperm);
-    double *ka = zkey, *kb = zkey_tmp;
-    int *ia = zperm, *ib = ztmp;
-    int passes = 0;
-    for (int w = ZTILE; w < N; w <<= 1) {
-        if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
-        else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, w, ka, ia, kb, ib);
+    // ping-pong so that the last pass writes (zkey, zperm)
+    const int passes = zsort_passes(N);
+    double *ka = (passes & 1) ? zkey_tmp : zkey, *kb = (passes & 1) ? zkey : zkey_tmp;
+    int *ia = (passes & 1) ? ztmp : zperm, *ib = (passes & 1) ? zperm : ztmp;
+    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), ZTILE, 0, s>>>(N, pos, ka, ia);
+    else k_ztile<false><<<nblk(N, ZTILE), ZTILE, 0, s>>>(N, pos, ka, ia);
+    for (int64_t w = ZTILE; w < N; w *= ZWAY) {
+        if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);
+        else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);
         double *tk = ka; ka = kb; kb = tk;
         int *ti = ia; ia = ib; ib = ti;
-        passes++;
-    }
-    if (passes & 1) {
-        cudaError_t e = cudaMemcpyAsync(zperm, ia, sizeof(int) * N, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess) return e;
-        e = cudaMemcpyAsync(zkey, ka, sizeof(double) * N, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }

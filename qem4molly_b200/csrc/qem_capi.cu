@@ -154,6 +154,8 @@ struct qem_handle {
         status, Eout, Fpart, pos_c;
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
+    DevBuf zX32, zY32;          // z-ordered box fractions of the FP32 k-space phases
+    bool kset_lattice = true;   // every row of the current k-set is 2 pi (m / Lx, n / Ly)
     // adjoint pass
     DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh, normxw;
     cudaStream_t s2 = nullptr;  // side stream of the long range
@@ -420,6 +422,7 @@ static void batch_rows(const qem_handle *h, uint64_t n, int P, std::vector<doubl
 static void sample_kset(qem_handle *h, int P)
 {
     batch_rows(h, 0, P, h->kset);
+    h->kset_lattice = true;
     h->kwt.clear();
     double kmax = 0;
     for (int i = 0; i < P; i++) kmax = std::max(kmax, h->kset[3 * i + 2]);
@@ -473,6 +476,12 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
     CU(grow(h->kf, sizeof(KForce<double>) * std::max(Pk, 1)));
     CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
     CU(grow(h->Flong, sizeof(double) * 3 * N));
+    if (h->p.precision == QEM_FP32_FIX) {
+        CU(grow(h->zX32, sizeof(uint32_t) * N));
+        CU(grow(h->zY32, sizeof(uint32_t) * N));
+        b.zX = ptr<uint32_t>(h->zX32);
+        b.zY = ptr<uint32_t>(h->zY32);
+    }
     b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
     b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
     b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
@@ -642,6 +651,9 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         const double kmax = draw ? h->kmax_lattice : h->kmax;
         if (prec == QEM_FP32_FIX && Pall > 0 && kmax * h->p.Lz > 120.0)
             return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
+        if (prec == QEM_FP32_FIX && Pall > 0 && !draw && !h->kset_lattice)
+            return fail(h, QEM_ERR_ARG, "the FP32 k-space path takes lattice k-vectors 2 pi (m / Lx, n / Ly) only "
+                                        "(K_set_generator.jl:19-25); use QEM_FP64 for other rows");
         // this rank's rows of the k-set, weighted as part of all Pall rows
         const int k_lo = (int)((int64_t)Pall * h->shard_rank / h->shard_world);
         const int k_hi = (int)((int64_t)Pall * (h->shard_rank + 1) / h->shard_world);
@@ -1084,7 +1096,8 @@ void qem_destroy(qem_handle *h)
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
-                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr};
+                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr, &h->zX32,
+                      &h->zY32};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -1104,6 +1117,17 @@ void qem_destroy(qem_handle *h)
 
 const char *qem_last_error(const qem_handle *h) { return h ? h->err.c_str() : "NULL handle"; }
 const char *qem_status_string(qem_status s) { return status_str(s); }
+
+// whether every row is a lattice vector 2 pi (m / Lx, n / Ly) (integer m, n
+// to 1e-6), as the FP32 k-space phases (fixed-point, lattice_phase) need
+static bool lattice_rows(const double *k3, int P, double Lx, double Ly)
+{
+    for (int i = 0; i < P; i++) {
+        const double m = k3[3 * i] * Lx / (2.0 * QEM_PI), n = k3[3 * i + 1] * Ly / (2.0 * QEM_PI);
+        if (!(fabs(m) < 1e9 && fabs(n) < 1e9) || fabs(m - rint(m)) > 1e-6 || fabs(n - rint(n)) > 1e-6) return false;
+    }
+    return true;
+}
 
 // rows (kx, ky, |k|) with |k| > 0; returns the largest |k| or -1
 static double check_krows(const double *k3, int P)
@@ -1126,6 +1150,7 @@ qem_status qem_set_kset(qem_handle *h, const double *k3, int32_t P, double sum_K
     const double kmax = check_krows(k3, P);
     if (kmax < 0) return fail(h, QEM_ERR_ARG, "k-set rows must be (kx, ky, |k|) with |k| > 0 (Force_long.jl:7)");
     h->kset.assign(k3, k3 + 3 * (size_t)P);
+    h->kset_lattice = lattice_rows(k3, P, h->p.Lx, h->p.Ly);
     h->kwt.clear();
     h->P = P;
     h->sum_K = sum_K;
@@ -1149,6 +1174,7 @@ qem_status qem_set_kset_weighted(qem_handle *h, const double *k3, const double *
         sw += w[i];
     }
     h->kset.assign(k3, k3 + 3 * (size_t)P);
+    h->kset_lattice = lattice_rows(k3, P, h->p.Lx, h->p.Ly);
     h->kwt.assign(w, w + P);
     h->P = P;
     h->sum_K = sw;

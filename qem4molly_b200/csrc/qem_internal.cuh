@@ -71,7 +71,19 @@ struct KConst {
     double fx, fy;          // kx / k, ky / k
     double wk;              // (sum_K / P) / (Lx Ly eps_0)
     double ek;              // energy weight -(sum_K / P) / (2 eps_0 Lx Ly) / k
+    int mx, my;             // lattice indices: k = 2 pi (mx / Lx, my / Ly) (FP32 path)
 };
+
+// FP32 k-space phase in turns from 32-bit fixed-point fractions X = x / Lx,
+// Y = y / Ly (units of 2^-32) and the lattice indices of k: mx X + my Y is
+// exact modulo 2^32, i.e. modulo one turn.  Returned as an angle in
+// [-pi, pi): the top 23 bits of the phase (rounded) become the mantissa of a
+// float in [1, 2), with half a turn added so that 1.5 maps to phase 0.
+__device__ __forceinline__ float lattice_phase(int mx, int my, uint32_t X, uint32_t Y)
+{
+    const uint32_t ph = (uint32_t)mx * X + (uint32_t)my * Y + 0x80000100u;  // + half a turn, + rounding
+    return (__uint_as_float((ph >> 9) | 0x3f800000u) - 1.5f) * 6.28318530717958648f;
+}
 
 // Per-k constants of the long-range force pass in its own precision
 // (written by the chunk-scan kernel from the structure-sum totals):
@@ -263,6 +275,7 @@ cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, d
 cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s);
 struct LongBuffers {
     double *zx, *zy;      // z-ordered in-plane coordinates (FP64, phases)
+    uint32_t *zX = nullptr, *zY = nullptr;  // x / Lx, y / Ly as 32-bit fixed-point fractions (FP32 phases)
     float *zhf;           // z - Lz/2 (FP32 path)
     double *zhd;          // z - Lz/2 (FP64 path)
     float *qf;

@@ -71,7 +71,7 @@ struct LM<double> {
 __device__ __forceinline__ void kconst_one(int m, double *__restrict__ kin, KConst *__restrict__ kc, double Lz,
                                            double g12, double wk, double esc, const double *__restrict__ kwt,
                                            double wden, double eden, const KSampler &S,
-                                           const unsigned long long *__restrict__ ctr)
+                                           const unsigned long long *__restrict__ ctr, double Lx_2pi, double Ly_2pi)
 {
     double kx, ky, k;
     if (ctr) {
@@ -87,6 +87,8 @@ __device__ __forceinline__ void kconst_one(int m, double *__restrict__ kin, KCon
     KConst K;
     K.kx_2pi = kx / (2.0 * QEM_PI);
     K.ky_2pi = ky / (2.0 * QEM_PI);
+    K.mx = (int)rint(kx * Lx_2pi);
+    K.my = (int)rint(ky * Ly_2pi);
     K.k = k;
     K.W = exp(-0.5 * k * Lz);  // sqrt(exp(-k L_z)); squared on use
     K.g = 0.5 / (g12 * exp(-2.0 * k * Lz) - 1.0);
@@ -99,10 +101,10 @@ __device__ __forceinline__ void kconst_one(int m, double *__restrict__ kin, KCon
 
 __global__ void k_kconst(int P, double *__restrict__ kin, KConst *__restrict__ kc, double Lz, double g12,
                          double wk, double esc, const double *__restrict__ kwt, double wden, double eden,
-                         const KSampler S, const unsigned long long *__restrict__ ctr)
+                         const KSampler S, const unsigned long long *__restrict__ ctr, double Lx_2pi, double Ly_2pi)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m < P) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr);
+    if (m < P) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr, Lx_2pi, Ly_2pi);
 }
 
 // z-ordered SoA copy of the particles
@@ -113,15 +115,28 @@ __device__ __forceinline__ void zrange_check(double zh, double zlim, unsigned *s
     if (zlim > 0.0 && !(fabs(zh) <= zlim)) atomicOr(status, QEM_ST_RANGE);
 }
 
+// x / L as a 32-bit fixed-point fraction of the box (the wrapped position)
+__device__ __forceinline__ uint32_t box_fraction(double x, double invL)
+{
+    double f = x * invL;
+    f -= floor(f);
+    return (uint32_t)__double2ull_rn(f * 4294967296.0);  // 2^32 (f rounding up to 1) wraps to 0
+}
+
 __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__restrict__ zperm, double h,
                           double *__restrict__ zx, double *__restrict__ zy, float *__restrict__ zhf,
                           double *__restrict__ zhd, float *__restrict__ qf, double *__restrict__ qd, double zlim,
-                          unsigned *status)
+                          unsigned *status, uint32_t *__restrict__ zX, uint32_t *__restrict__ zY, double invLx,
+                          double invLy)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= N) return;
     const double4 p = pos[zperm[m]];
     zrange_check(p.z - h, zlim, status);
+    if (zX) {
+        zX[m] = box_fraction(p.x, invLx);
+        zY[m] = box_fraction(p.y, invLy);
+    }
     zx[m] = p.x;
     zy[m] = p.y;
     zhd[m] = p.z - h;
@@ -147,13 +162,20 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
                                                           double Lz, double g12, double wk, double esc,
                                                           const double *__restrict__ kwt, double wden, double eden,
                                                           double zlim, unsigned *status, const KSampler S,
-                                                          const unsigned long long *__restrict__ ctr)
+                                                          const unsigned long long *__restrict__ ctr,
+                                                          uint32_t *__restrict__ zX, uint32_t *__restrict__ zY,
+                                                          double invLx, double invLy, double Lx_2pi, double Ly_2pi)
 {
     __shared__ double warp_tot[32];
-    for (int m = threadIdx.x; m < P; m += 1024) kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr);
+    for (int m = threadIdx.x; m < P; m += 1024)
+        kconst_one(m, kin, kc, Lz, g12, wk, esc, kwt, wden, eden, S, ctr, Lx_2pi, Ly_2pi);
     for (int m = threadIdx.x; m < N; m += 1024) {
         const double4 p = pos[zperm[m]];
         zrange_check(p.z - h, zlim, status);
+        if (zX) {
+            zX[m] = box_fraction(p.x, invLx);
+            zY[m] = box_fraction(p.y, invLy);
+        }
         zx[m] = p.x;
         zy[m] = p.y;
         zhd[m] = p.z - h;
@@ -219,6 +241,26 @@ struct Quad4 {
     }
 };
 
+// a thread's PPT particles in z order, FP32 path: in-plane positions as
+// 32-bit fixed-point box fractions (lattice_phase)
+struct QuadF {
+    uint32_t X[PPT], Y[PPT];
+    float z[PPT], q[PPT];
+    __device__ __forceinline__ void load(int N, int m0, const uint32_t *zX, const uint32_t *zY, const float *zh,
+                                         const float *qv)
+    {
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const int m = m0 + j;
+            const bool ok = m < N;
+            X[j] = ok ? zX[m] : 0u;
+            Y[j] = ok ? zY[m] : 0u;
+            z[j] = ok ? zh[m] : 0.f;
+            q[j] = ok ? qv[m] : 0.f;  // q = 0 makes padding particles contribute nothing
+        }
+    }
+};
+
 template <typename Real>
 __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double *__restrict__ zx,
                                              const double *__restrict__ zy, const Real *__restrict__ zh,
@@ -268,15 +310,15 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
 // particles' sums for the block's KPB k-vectors in shared memory, and one
 // tree reduction over the block's threads finishes all KPB x 4 totals (one
 // barrier per tree level instead of two barriers and a warp reduction per k).
-__global__ void __launch_bounds__(LT) k_ltot_f32(int N, int P, int nch, const double *__restrict__ zx,
-                                                 const double *__restrict__ zy, const float *__restrict__ zh,
+__global__ void __launch_bounds__(LT) k_ltot_f32(int N, int P, int nch, const uint32_t *__restrict__ zX,
+                                                 const uint32_t *__restrict__ zY, const float *__restrict__ zh,
                                                  const float *__restrict__ qv, const KConst *__restrict__ kc,
                                                  double *__restrict__ tot)
 {
     constexpr float LOG2E = 1.4426950408889634f;
     __shared__ float part[KPB * 4][LT + 1];  // +1: rows on different banks
-    Quad4<float> P4;
-    P4.load(N, blockIdx.x * LCH + threadIdx.x * PPT, zx, zy, zh, qv);
+    QuadF P4;
+    P4.load(N, blockIdx.x * LCH + threadIdx.x * PPT, zX, zY, zh, qv);
     const int k0 = blockIdx.y * KPB;
     const int nk = min(KPB, P - k0);
     for (int kk = 0; kk < nk; kk++) {
@@ -285,9 +327,8 @@ __global__ void __launch_bounds__(LT) k_ltot_f32(int N, int P, int nch, const do
         float v[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
-            const double t = frac_turns(fma(K.kx_2pi, P4.x[j], K.ky_2pi * P4.y[j]));
             float s, c;
-            __sincosf((float)t * 6.28318530717958648f, &s, &c);
+            __sincosf(lattice_phase(K.mx, K.my, P4.X[j], P4.Y[j]), &s, &c);
             const float e = kl * P4.z[j];
             const float ep = P4.q[j] * ex2_approx(e), em = P4.q[j] * ex2_approx(-e);
             v[0] = fmaf(ep, c, v[0]);
@@ -522,8 +563,8 @@ __global__ void __launch_bounds__(LT, sizeof(Real) == 4 ? LF_MINB : 4) k_lforce(
 // processed.
 template <bool ENERGY>
 __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nch, int ks_n,
-                                                           const double *__restrict__ zx,
-                                                           const double *__restrict__ zy,
+                                                           const uint32_t *__restrict__ zX,
+                                                           const uint32_t *__restrict__ zY,
                                                            const float *__restrict__ zh, const float *__restrict__ qv,
                                                            const KConst *__restrict__ kc,
                                                            const KForce<float> *__restrict__ kf,
@@ -535,9 +576,9 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     __shared__ float wsh[2][4][NW];
     __shared__ double ered[NW];
     __shared__ double Facc[3 * PPT][LT];  // FP64 sums of the FP32 batches (registers stay free)
-    Quad4<float> P4;
+    QuadF P4;
     const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
-    P4.load(N, m0, zx, zy, zh, qv);
+    P4.load(N, m0, zX, zY, zh, qv);
     const float2 z2[2] = {f2(P4.z[0], P4.z[1]), f2(P4.z[2], P4.z[3])};
     const float2 q2[2] = {f2(P4.q[0], P4.q[1]), f2(P4.q[2], P4.q[3])};
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -550,11 +591,12 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     float2 bx[2] = {f2s(0.f), f2s(0.f)}, by[2] = {f2s(0.f), f2s(0.f)}, bz[2] = {f2s(0.f), f2s(0.f)};
     double E = 0;
     // constants of k = kidx, fetched one iteration ahead
-    double kxn = 0, kyn = 0, ekn = 0;
+    int mxn = 0, myn = 0;
+    double ekn = 0;
     float4 Kan = make_float4(0, 0, 0, 0), Kbn = Kan, On = Kan;
     auto fetch = [&](int k) {
-        kxn = kc[k].kx_2pi;
-        kyn = kc[k].ky_2pi;
+        mxn = kc[k].mx;
+        myn = kc[k].my;
         if (ENERGY) ekn = kc[k].ek;
         const float4 *kk = reinterpret_cast<const float4 *>(kf + k);
         Kan = kk[0];  // k, wfx, wfy, wk
@@ -563,7 +605,8 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
     };
     if (kb < ke) fetch(kb);
     for (int kidx = kb; kidx < ke; kidx++) {
-        const double kx2 = kxn, ky2 = kyn, ek = ekn;
+        const int mx = mxn, my = myn;
+        const double ek = ekn;
         const float4 Ka = Kan, Kb = Kbn, O = On;
         if (kidx + 1 < ke) fetch(kidx + 1);
         const int buf = (kidx - kb) & 1;
@@ -575,8 +618,7 @@ __global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nc
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int j = 2 * pp + h;
-                const double t = frac_turns(fma(kx2, P4.x[j], ky2 * P4.y[j]));
-                __sincosf((float)t * 6.28318530717958648f, &ss[h], &cc[h]);
+                __sincosf(lattice_phase(mx, my, P4.X[j], P4.Y[j]), &ss[h], &cc[h]);
             }
             c2[pp] = f2(cc[0], cc[1]);
             s2[pp] = f2(ss[0], ss[1]);
@@ -1146,6 +1188,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
 {
     if (N <= 0) return cudaSuccess;
     const double zlim = precision == QEM_FP64 ? 0.0 : b.zlim;
+    uint32_t *zX = precision == QEM_FP64 ? nullptr : b.zX, *zY = precision == QEM_FP64 ? nullptr : b.zY;
     if (stage == 0 && !energy && N <= LONG_PREP_SMALL) {
         const double h = 0.5 * Lz;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
@@ -1153,13 +1196,14 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const double esc = P > 0 ? -(sum_K / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
         k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, b.qscan, fscale,
                                              b.k0, P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                             2.0 * eps0 * Lx * Ly, zlim, status, b.sampler, b.draw_ctr);
+                                             2.0 * eps0 * Lx * Ly, zlim, status, b.sampler, b.draw_ctr, zX, zY, 1.0 / Lx,
+                                             1.0 / Ly, Lx / (2.0 * QEM_PI), Ly / (2.0 * QEM_PI));
         if (P > 0) {
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
-                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
+                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zX, b.zY, b.zhf, b.qf, b.kc, b.tot);
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
@@ -1172,7 +1216,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     if (stage == 0) {
         const double h = 0.5 * Lz;
         k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, zlim,
-                                               status);
+                                               status, zX, zY, 1.0 / Lx, 1.0 / Ly);
         cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
         if (e != cudaSuccess) return e;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
@@ -1183,12 +1227,13 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
             const double wk = (sum_K / P) / (Lx * Ly * eps0);
             const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
             k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                                  2.0 * eps0 * Lx * Ly, b.sampler, b.draw_ctr);
+                                                  2.0 * eps0 * Lx * Ly, b.sampler, b.draw_ctr, Lx / (2.0 * QEM_PI),
+                                                  Ly / (2.0 * QEM_PI));
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
-                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhf, b.qf, b.kc, b.tot);
+                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zX, b.zY, b.zhf, b.qf, b.kc, b.tot);
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
@@ -1211,10 +1256,10 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const KForce<float> *kf = (const KForce<float> *)b.kf;
         const float *of = (const float *)b.off;
         if (energy)
-            k_lforce_f32<true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
+            k_lforce_f32<true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zX, b.zY, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
                                                  b.Epart);
         else
-            k_lforce_f32<false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zx, b.zy, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
+            k_lforce_f32<false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zX, b.zY, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
                                                   b.Epart);
     }
     k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3, b.draw_ctr);

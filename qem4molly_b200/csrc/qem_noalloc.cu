@@ -50,7 +50,9 @@ constexpr size_t O_K0 = O_QD + al(sizeof(double) * NA_MAX_N);
 constexpr size_t O_ZHF = O_K0 + al(sizeof(double) * NA_MAX_N);
 constexpr size_t O_QF = O_ZHF + al(sizeof(float) * NA_MAX_N);
 constexpr size_t O_QSCAN = O_QF + al(sizeof(float) * NA_MAX_N);
-constexpr size_t O_KIN = O_QSCAN + al(sizeof(double) * (NA_MAX_N + 1));
+constexpr size_t O_ZX32 = O_QSCAN + al(sizeof(double) * (NA_MAX_N + 1));
+constexpr size_t O_ZY32 = O_ZX32 + al(sizeof(uint32_t) * NA_MAX_N);
+constexpr size_t O_KIN = O_ZY32 + al(sizeof(uint32_t) * NA_MAX_N);
 constexpr size_t O_KC = O_KIN + al(sizeof(double) * 3 * NA_MAX_P);
 constexpr size_t O_TOT = O_KC + al(sizeof(KConst) * NA_MAX_P);
 constexpr size_t O_OFF = O_TOT + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
@@ -110,6 +112,13 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
         kmax = std::max(kmax, k);
     }
     if (p->precision == QEM_FP32_FIX && P > 0 && kmax * p->Lz > 120.0) return QEM_ERR_RANGE;
+    if (p->precision == QEM_FP32_FIX) {  // the FP32 phases are fixed-point lattice phases
+        for (int i = 0; i < P; i++) {
+            const double m = k3[3 * i] * p->Lx / (2.0 * QEM_PI), n = k3[3 * i + 1] * p->Ly / (2.0 * QEM_PI);
+            if (!(fabs(m) < 1e9 && fabs(n) < 1e9) || fabs(m - rint(m)) > 1e-6 || fabs(n - rint(n)) > 1e-6)
+                return reject("QEM_FP32_FIX takes lattice k-vectors 2 pi (m / Lx, n / Ly) only");
+        }
+    }
     if (qem_long_chunk() != NA_CH) return reject("scratch layout does not match the long-range chunk size");
     if (cudaSetDevice(p->device) != cudaSuccess) return QEM_ERR_CUDA;
     unsigned char *S = nullptr;
@@ -143,6 +152,8 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
     b.Fpart = (double *)(S + O_FPART);
     b.Eks = b.Epart + (size_t)b.ks * nch + (NA_MAX_N + 255) / 256;
     b.stmp = S + O_STMP; b.stmp_bytes = STMP_BYTES;
+    b.zX = (uint32_t *)(S + O_ZX32);
+    b.zY = (uint32_t *)(S + O_ZY32);
     b.zlim = p->precision == QEM_FP32_FIX && P > 0 ? qem_fp32_zlim(kmax) : 0.0;
     for (int stage = 0; stage < 2 && e == cudaSuccess; stage++)
         e = qem_launch_long(p->precision, false, N, P, pos, zperm, b, p->Lx, p->Ly, p->Lz, p->gamma_down, p->gamma_up,
