@@ -413,6 +413,7 @@ __global__ void k_pairs(int N, const double4 *__restrict__ pos_c, const int *__r
 // ---------------------------------------------------------------------------
 // pair list, at least 3 cells along x and y: one warp per owner cell
 // ---------------------------------------------------------------------------
+constexpr int PL_MAXB = QEM_PL_MAXB;  // candidate batches of 32 whose hit masks the count pass keeps
 // The five cells of the half stencil in visiting order: own cell, then
 // (0,+1), (+1,-1), (+1,0), (+1,+1) -- the order of k_pairs.
 __device__ __forceinline__ void half_offset(int d, int &ox, int &oy)
@@ -435,7 +436,10 @@ __device__ __forceinline__ int wrap_cell(int n, int m) { return n < 0 ? n + m : 
 // incoming entry straight to its final slot, so the incoming lists come out
 // in ascending pair order without atomics or a sort.  A (candidate,
 // direction) entry belongs to exactly one owner cell, hence to one warp, and
-// owner blocks of more than 32 owners carry it over in place.
+// owner blocks of more than 32 owners carry it over in place.  The count pass
+// also keeps every owner's hit mask of its first PL_MAXB candidate batches
+// (hmask[owner position * PL_MAXB + batch]), so the fill pass tests distances
+// only in cells with more than 32 * PL_MAXB candidates.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__restrict__ pos_c,
                                                     const int *__restrict__ cstart, const int *__restrict__ clist,
@@ -443,7 +447,7 @@ __global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__
                                                     const int64_t *__restrict__ poff, int2 *__restrict__ pairs,
                                                     int64_t cap, int *__restrict__ in_slot,
                                                     const int64_t *__restrict__ in_off, int *__restrict__ in_list,
-                                                    unsigned *status)
+                                                    unsigned *status, unsigned *__restrict__ hmask)
 {
     const int c = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -474,6 +478,10 @@ __global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__
         }
         for (int v0 = 0; v0 < tot; v0 += 32) {
             const int v = v0 + lane;
+            const int bt = v0 >> 5;  // candidate batch
+            const bool stored = bt < PL_MAXB;
+            unsigned my_mask = 0;    // lane k: owner k's hits in this batch
+            if (FILL && stored && lane < no) my_mask = hmask[(size_t)(o0 + lane) * PL_MAXB + bt];
             int d = -1, s = 0;
             {
                 int acc = 0;
@@ -498,8 +506,16 @@ __global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__
             int r = 0;
             for (int k = 0; k < no; k++) {
                 const int t = o0 + k;
-                const bool hit = valid && (d != 0 || s > t) && rho2_exact(pos_c[t], pj, g) <= rc2;
-                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                unsigned m;
+                bool hit;
+                if (FILL && stored) {
+                    m = __shfl_sync(0xffffffffu, my_mask, k);
+                    hit = (m >> lane) & 1u;
+                } else {
+                    hit = valid && (d != 0 || s > t) && rho2_exact(pos_c[t], pj, g) <= rc2;
+                    m = __ballot_sync(0xffffffffu, hit);
+                    if (!FILL && lane == k) my_mask = m;
+                }
                 if (FILL) {
                     const int64_t base = __shfl_sync(0xffffffffu, my_next, k);
                     const int io = __shfl_sync(0xffffffffu, my_i, k);
@@ -522,6 +538,7 @@ __global__ void __launch_bounds__(128) k_pairs_cell(int ncell, const double4 *__
                 int &w = in_slot[(size_t)5 * s + d];
                 w = (FILL || blk > 0) ? w + r : r;
             }
+            if (!FILL && stored && lane < no) hmask[(size_t)(o0 + lane) * PL_MAXB + bt] = my_mask;
         }
         if (!FILL && lane < no) pcount[o0 + lane] = my_cnt;
     }
@@ -886,7 +903,8 @@ cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *p
 cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const int *cell, const int *cell_start,
                                  const int *cell_list, CellGeom g, double rc2, int *pcount, int64_t *poff,
                                  int2 *pairs, int64_t cap, int *in_cnt, int *in_slot, int64_t *in_off, int *in_list,
-                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s)
+                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, unsigned *hmask,
+                                 cudaStream_t s)
 {
     if (N <= 0) return cudaSuccess;
     cudaError_t e;
@@ -895,12 +913,12 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
     if (g.ncx >= 3 && g.ncy >= 3 && (int64_t)N >= 2 * (int64_t)ncell) {
         const int nb = nblk((int64_t)ncell * 32, 128);
         k_pairs_cell<false><<<nb, 128, 0, s>>>(ncell, pos_c, cell_start, cell_list, g, rc2, pcount, nullptr, nullptr,
-                                               0, in_slot, nullptr, nullptr, nullptr);
+                                               0, in_slot, nullptr, nullptr, nullptr, hmask);
         if ((e = scan_impl<int, int64_t>(pcount, poff, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
         k_in_base<<<nblk(N, 256), 256, 0, s>>>(N, cell_list, cell, g, poff + N, cap, in_slot, in_cnt, status);
         if ((e = scan_impl<int, int64_t>(in_cnt, in_off, N, scan_tmp, scan_tmp_bytes, s)) != cudaSuccess) return e;
         k_pairs_cell<true><<<nb, 128, 0, s>>>(ncell, pos_c, cell_start, cell_list, g, rc2, nullptr, poff, pairs, cap,
-                                              in_slot, in_off, in_list, status);
+                                              in_slot, in_off, in_list, status, hmask);
         return cudaGetLastError();
     }
     // one thread per owner (over the full deduplicated stencil when there are

@@ -155,6 +155,7 @@ struct qem_handle {
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
     DevBuf zX32, zY32;          // z-ordered box fractions of the FP32 k-space phases
+    DevBuf hmask;               // pair-list hit masks (count pass -> fill pass)
     bool kset_lattice = true;   // every row of the current k-set is 2 pi (m / Lx, n / Ly)
     // adjoint pass
     DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh, normxw;
@@ -510,6 +511,7 @@ static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s
     CU(grow(h->pcount, sizeof(int) * N));
     CU(grow(h->poff, sizeof(int64_t) * (N + 1)));
     CU(grow(h->pos_c, sizeof(double4) * N));
+    CU(grow(h->hmask, sizeof(unsigned) * QEM_PL_MAXB * (size_t)N));
     // pair capacity: last count + 25 %, first time from the mean density; the
     // count stays on the device (no host round trip inside the call)
     if (h->pair_cap <= 0) {
@@ -531,7 +533,8 @@ static qem_status build_pairs(qem_handle *h, int N, unsigned *st, cudaStream_t s
     CU(qem_launch_pair_list(N, h->ncell, ptr<double4>(h->pos_c), ptr<int>(h->cell), ptr<int>(h->cell_start),
                             ptr<int>(h->cell_list), h->geom, h->sc.rc2, ptr<int>(h->pcount), ptr<int64_t>(h->poff),
                             ptr<int2>(h->pairs), cap, ptr<int>(h->in_cnt), ptr<int>(h->in_fill),
-                            ptr<int64_t>(h->in_off), ptr<int>(h->in_list), st, h->scan_tmp.p, h->scan_tmp.cap, s));
+                            ptr<int64_t>(h->in_off), ptr<int>(h->in_list), st, h->scan_tmp.p, h->scan_tmp.cap,
+                            ptr<unsigned>(h->hmask), s));
     h->pairs_N = N;
     h->pairs_valid = true;
     return QEM_OK;
@@ -1097,7 +1100,7 @@ void qem_destroy(qem_handle *h)
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
                       &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr, &h->zX32,
-                      &h->zY32};
+                      &h->zY32, &h->hmask};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);

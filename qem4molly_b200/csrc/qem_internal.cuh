@@ -190,10 +190,13 @@ cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *p
 // most cap pairs stored (QEM_ST_OVERFLOW beyond), in_cnt / in_off per
 // particle with in_list in ascending pair order and in_off[N] <= cap (no
 // incoming entries at all after an overflow); in_slot is scratch of 5 N ints
+// hmask: QEM_PL_MAXB hit masks per particle (scratch of the one-warp-per-cell passes)
+constexpr int QEM_PL_MAXB = 8;
 cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const int *cell, const int *cell_start,
                                  const int *cell_list, CellGeom g, double rc2, int *pcount, int64_t *poff,
                                  int2 *pairs, int64_t cap, int *in_cnt, int *in_slot, int64_t *in_off, int *in_list,
-                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, cudaStream_t s);
+                                 unsigned *status, void *scan_tmp, size_t scan_tmp_bytes, unsigned *hmask,
+                                 cudaStream_t s);
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 cudaError_t qem_scan_f64_excl(const double *in, double *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t qem_scan_tmp_bytes(int n);
