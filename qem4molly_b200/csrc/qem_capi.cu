@@ -150,11 +150,11 @@ struct qem_handle {
     // device scratch
     DevBuf xyz, q, F, pos, cell, cell_cnt, cell_start, cell_fill, cell_list, pos_of, pcount, poff, pairs, R, Upair,
         in_cnt, in_off, in_fill, in_list, scan_tmp;
-    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhf, zhd, qf, qd, k0, qscan, kc, kin, kw, tot, off, Utot, kf, Epart,
+    DevBuf zperm, ztmp, zkey, zkey2, zx, zy, zhd, qd, k0, qscan, kc, kin, kw, tot, off, Utot, kf, Epart,
         status, Eout, Fpart, pos_c;
     int64_t pair_cap = 0;       // capacity of pairs / R / in_list (grown on overflow)
     DevBuf scan_tmp2, Flong;    // long-range scan scratch and forces (side stream)
-    DevBuf zX32, zY32;          // z-ordered box fractions of the FP32 k-space phases
+    DevBuf zP32;                // z-ordered FP32 records of the lane-per-k passes
     DevBuf hmask;               // pair-list hit masks (count pass -> fill pass)
     bool kset_lattice = true;   // every row of the current k-set is 2 pi (m / Lx, n / Ly)
     // adjoint pass
@@ -463,9 +463,7 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
     CU(grow(h->zkey2, sizeof(double) * N));
     CU(grow(h->zx, sizeof(double) * N));
     CU(grow(h->zy, sizeof(double) * N));
-    CU(grow(h->zhf, sizeof(float) * N));
     CU(grow(h->zhd, sizeof(double) * N));
-    CU(grow(h->qf, sizeof(float) * N));
     CU(grow(h->qd, sizeof(double) * N));
     CU(grow(h->k0, sizeof(double) * N));
     CU(grow(h->qscan, sizeof(double) * (N + 1)));
@@ -478,14 +476,12 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
     CU(grow(h->scan_tmp2, qem_scan_tmp_bytes(std::max(N, 1)) + 64));
     CU(grow(h->Flong, sizeof(double) * 3 * N));
     if (h->p.precision == QEM_FP32_FIX) {
-        CU(grow(h->zX32, sizeof(uint32_t) * N));
-        CU(grow(h->zY32, sizeof(uint32_t) * N));
-        b.zX = ptr<uint32_t>(h->zX32);
-        b.zY = ptr<uint32_t>(h->zY32);
+        CU(grow(h->zP32, sizeof(uint4) * N));
+        b.zP = ptr<uint4>(h->zP32);
     }
     b.zx = ptr<double>(h->zx); b.zy = ptr<double>(h->zy);
-    b.zhf = ptr<float>(h->zhf); b.zhd = ptr<double>(h->zhd);
-    b.qf = ptr<float>(h->qf); b.qd = ptr<double>(h->qd);
+    b.zhd = ptr<double>(h->zhd);
+    b.qd = ptr<double>(h->qd);
     b.k0 = ptr<double>(h->k0); b.qscan = ptr<double>(h->qscan);
     b.kc = ptr<KConst>(h->kc); b.kin = ptr<double>(h->kin);
     b.kwt = h->kwt.empty() ? nullptr : ptr<double>(h->kw);
@@ -621,7 +617,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
     // k-slices of the force pass, from the size of the whole k-set (or of the
     // batch about to be drawn); small systems with many k-vectors get up to
     // QEM_LONG_MAX_KS slices so that the pass still fills the GPU
-    const int ks = qem_long_ksplit(nch, std::max(h->has_kset ? h->P : h->p.rbe_p, 1), h->long_max_ks);
+    const int ks = qem_long_ksplit(nch, std::max(h->has_kset ? h->P : h->p.rbe_p, 1), h->long_max_ks, prec);
     const size_t nEpart = (size_t)nbS + (size_t)ks * nch + nb0 + std::max(P, h->p.rbe_p) + 8;
     CU(grow(h->Epart, sizeof(double) * nEpart));
     double *Ep = ptr<double>(h->Epart);
@@ -1095,12 +1091,12 @@ void qem_destroy(qem_handle *h)
     DevBuf *bufs[] = {&h->xyz, &h->q, &h->F, &h->pos, &h->cell, &h->cell_cnt, &h->cell_start, &h->cell_fill,
                       &h->cell_list, &h->pos_of, &h->pcount, &h->poff, &h->pairs, &h->R, &h->Upair, &h->in_cnt,
                       &h->in_off, &h->in_fill, &h->in_list, &h->scan_tmp, &h->zperm, &h->ztmp, &h->zkey, &h->zkey2,
-                      &h->zx, &h->zy, &h->zhf, &h->zhd, &h->qf, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin, &h->kw,
+                      &h->zx, &h->zy, &h->zhd, &h->qd, &h->k0, &h->qscan, &h->kc, &h->kin, &h->kw,
                       &h->tot, &h->off, &h->Utot, &h->kf, &h->Epart, &h->status, &h->Eout, &h->Fpart,
                       &h->pos_c, &h->scan_tmp2, &h->Flong, &h->gF, &h->gxyz, &h->gq, &h->RA, &h->gam,
                       &h->gout, &h->zgx, &h->zgy, &h->zgz, &h->w1, &h->w2, &h->ws1, &h->ws2, &h->atot, &h->aoff,
-                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr, &h->zX32,
-                      &h->zY32, &h->hmask};
+                      &h->lam, &h->ggk, &h->Gpart, &h->gFh, &h->normxw, &h->ktab, &h->kctr, &h->zP32,
+                      &h->hmask};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : h->prof.pool) cudaEventDestroy(e);
@@ -1537,7 +1533,7 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         const int Pk = h->has_kset ? h->P : 0;
         const int LCH = qem_long_chunk();
         const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;
-        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), h->long_max_ks);
+        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), h->long_max_ks, QEM_FP64);
         CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks * nch + nb0 + std::max(Pk, 1) + 8)));
         LongBuffers b;
         {

@@ -278,10 +278,9 @@ cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, d
 cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s);
 struct LongBuffers {
     double *zx, *zy;      // z-ordered in-plane coordinates (FP64, phases)
-    uint32_t *zX = nullptr, *zY = nullptr;  // x / Lx, y / Ly as 32-bit fixed-point fractions (FP32 phases)
-    float *zhf;           // z - Lz/2 (FP32 path)
-    double *zhd;          // z - Lz/2 (FP64 path)
-    float *qf;
+    uint4 *zP = nullptr;  // FP32 path: per particle {x / Lx, y / Ly as 32-bit fixed-point box fractions
+                          // (the lattice_phase inputs), z - Lz/2, q as FP32 bits}
+    double *zhd;          // z - Lz/2
     double *qd;
     double *k0;           // per z-ordered particle: q (Q_below - Q_above) / (2 Lx Ly eps_0)
     double *qscan;        // exclusive scan of q in z order
@@ -314,7 +313,7 @@ inline double qem_fp32_zlim(double kmax) { return kmax > 0 ? 60.0 / kmax : 0.0; 
 // number of k slices for nch chunks and P k-vectors (at most max_ks); the
 // per-slice force partials take ks x N x 3 doubles, and ks x nch stays near
 // one wave of force-pass blocks, so they stay below ~15 MB at any N
-int qem_long_ksplit(int nch, int P, int max_ks);
+int qem_long_ksplit(int nch, int P, int max_ks, int precision);
 constexpr int QEM_LONG_MAX_KS = 64;
 // stage 0: z-ordered gather, k = 0 term, per-k constants, chunk totals and
 // their scan; stage 1: the k-sliced force pass, added into F3.

@@ -11,23 +11,30 @@
 //                 src/python_lib/Sigma_Gamma_func_njit.py:8-69
 //
 // Layout: particles in z order (stable sortperm), SoA, chunks of LCH = 512
-// consecutive particles; a thread owns PPT = 4 consecutive particles.
-//   1. k_ltot   grid (chunk, k-group): per (k, chunk) sums of
-//               u = q e^{k(z-h)} e^{i k.rho} and v = q e^{-k(z-h)} e^{i k.rho}
-//               (h = L_z / 2 keeps both exponentials inside FP32 range).
+// consecutive particles.
+//   1. totals   per (k, chunk) sums of u = q e^{k(z-h)} e^{i k.rho} and
+//               v = q e^{-k(z-h)} e^{i k.rho} (h = L_z / 2 keeps both
+//               exponentials inside FP32 range): k_ltot (FP64, a thread per
+//               PPT = 4 particles, block reductions per k) or k_ltot_lk
+//               (FP32, a lane per k walking the chunk).
 //   2. k_lscan  one warp per k: FP64 exclusive scan of the chunk totals,
-//               forward for u (particles below) and backward for v (above).
-//   3. k_lforce grid (chunk, k-slice): per k, serial scans over the thread's
-//               4 particles, one warp shuffle scan of the thread totals and a
-//               4-warp prefix give every particle its prefix (A, B) and suffix
-//               (C, D) sums; Fl_non_sort + Fl_sort + Flz_self are formed in
-//               registers and summed over the slice's k in FP64.
+//               forward for u (particles below) and backward for v (above),
+//               and the per-k force constants.
+//   3. force    FP64 k_lforce: grid (chunk, k-slice), per k serial scans over
+//               a thread's 4 particles, a warp shuffle scan and a 4-warp
+//               prefix give every particle its prefix (A, B) and suffix (C, D)
+//               sums.  FP32 k_lforce_lk: a lane per k walks the chunk with
+//               running sums and one cross-lane sum over k per particle.
+//               Fl_non_sort + Fl_sort + Flz_self are formed in registers.
 //   4. k_lfinal per particle: sum of the k-slices + the k = 0 term, added to F
 //               in the original particle order (fixed order: deterministic).
+// The FP32 phases k.rho are exact fixed-point lattice phases (lattice_phase).
 // The suffix sums C, D are summed directly from above instead of the
 // reference's "total minus running sum" (Force_long.jl:97-98), which is the
-// same quantity without the cancellation that makes it useless in FP32.
-// Phases are reduced in FP64 turns before the FP32 sine/cosine; the per-k
+// same quantity without the cancellation that makes it useless in FP32 (the
+// FP32 force pass takes total minus running sum only inside a chunk that is
+// thin in z against k, where the cancellation is bounded).
+// Phases are reduced in FP64 turns before the FP64 sine/cosine; the per-k
 // denominators 0.5 / (g_u g_d e^{-2 k L_z} - 1) are FP64.
 #include "qem_internal.cuh"
 
@@ -46,6 +53,9 @@ constexpr int LKB = 8;          // k-vectors per FP32 accumulation batch of the 
 #define QEM_LF_MINB 8
 #endif
 constexpr int LF_MINB = QEM_LF_MINB;  // resident FP32 force-pass blocks per SM (register budget)
+#ifndef QEM_LK_WARPS
+#define QEM_LK_WARPS 24
+#endif
 
 // t - round(t) for |t| < 2^51 turns: rounding by adding and subtracting
 // 1.5 * 2^52 (two FP64 adds)
@@ -123,26 +133,28 @@ __device__ __forceinline__ uint32_t box_fraction(double x, double invL)
     return (uint32_t)__double2ull_rn(f * 4294967296.0);  // 2^32 (f rounding up to 1) wraps to 0
 }
 
+// the FP32 record of a particle: {x / Lx, y / Ly as fixed-point box fractions, z - h, q}
+__device__ __forceinline__ uint4 f32_record(const double4 &p, double h, double invLx, double invLy)
+{
+    return make_uint4(box_fraction(p.x, invLx), box_fraction(p.y, invLy), __float_as_uint((float)(p.z - h)),
+                      __float_as_uint((float)p.w));
+}
+
+// zP != nullptr (FP32 path): the packed records of the lane-per-k passes
 __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__restrict__ zperm, double h,
-                          double *__restrict__ zx, double *__restrict__ zy, float *__restrict__ zhf,
-                          double *__restrict__ zhd, float *__restrict__ qf, double *__restrict__ qd, double zlim,
-                          unsigned *status, uint32_t *__restrict__ zX, uint32_t *__restrict__ zY, double invLx,
-                          double invLy)
+                          double *__restrict__ zx, double *__restrict__ zy, double *__restrict__ zhd,
+                          double *__restrict__ qd, double zlim, unsigned *status, uint4 *__restrict__ zP,
+                          double invLx, double invLy)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= N) return;
     const double4 p = pos[zperm[m]];
     zrange_check(p.z - h, zlim, status);
-    if (zX) {
-        zX[m] = box_fraction(p.x, invLx);
-        zY[m] = box_fraction(p.y, invLy);
-    }
+    if (zP) zP[m] = f32_record(p, h, invLx, invLy);
     zx[m] = p.x;
     zy[m] = p.y;
     zhd[m] = p.z - h;
-    zhf[m] = (float)(p.z - h);
     qd[m] = p.w;
-    qf[m] = (float)p.w;
 }
 
 // Stage 0 before the totals for a small system without energy, in one
@@ -154,8 +166,7 @@ constexpr int LONG_PREP_SMALL = 8192;
 __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *__restrict__ pos,
                                                           const int *__restrict__ zperm, double h,
                                                           double *__restrict__ zx, double *__restrict__ zy,
-                                                          float *__restrict__ zhf, double *__restrict__ zhd,
-                                                          float *__restrict__ qf, double *__restrict__ qd,
+                                                          double *__restrict__ zhd, double *__restrict__ qd,
                                                           double *__restrict__ qscan, double fscale,
                                                           double *__restrict__ k0, int P,
                                                           double *__restrict__ kin, KConst *__restrict__ kc,
@@ -163,8 +174,8 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
                                                           const double *__restrict__ kwt, double wden, double eden,
                                                           double zlim, unsigned *status, const KSampler S,
                                                           const unsigned long long *__restrict__ ctr,
-                                                          uint32_t *__restrict__ zX, uint32_t *__restrict__ zY,
-                                                          double invLx, double invLy, double Lx_2pi, double Ly_2pi)
+                                                          uint4 *__restrict__ zP, double invLx, double invLy,
+                                                          double Lx_2pi, double Ly_2pi)
 {
     __shared__ double warp_tot[32];
     for (int m = threadIdx.x; m < P; m += 1024)
@@ -172,16 +183,11 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
     for (int m = threadIdx.x; m < N; m += 1024) {
         const double4 p = pos[zperm[m]];
         zrange_check(p.z - h, zlim, status);
-        if (zX) {
-            zX[m] = box_fraction(p.x, invLx);
-            zY[m] = box_fraction(p.y, invLy);
-        }
+        if (zP) zP[m] = f32_record(p, h, invLx, invLy);
         zx[m] = p.x;
         zy[m] = p.y;
         zhd[m] = p.z - h;
-        zhf[m] = (float)(p.z - h);
         qd[m] = p.w;
-        qf[m] = (float)p.w;
     }
     __syncthreads();
     qem_block_scan_excl_small<double, double>(qd, qscan, N, warp_tot);
@@ -241,26 +247,6 @@ struct Quad4 {
     }
 };
 
-// a thread's PPT particles in z order, FP32 path: in-plane positions as
-// 32-bit fixed-point box fractions (lattice_phase)
-struct QuadF {
-    uint32_t X[PPT], Y[PPT];
-    float z[PPT], q[PPT];
-    __device__ __forceinline__ void load(int N, int m0, const uint32_t *zX, const uint32_t *zY, const float *zh,
-                                         const float *qv)
-    {
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            const int m = m0 + j;
-            const bool ok = m < N;
-            X[j] = ok ? zX[m] : 0u;
-            Y[j] = ok ? zY[m] : 0u;
-            z[j] = ok ? zh[m] : 0.f;
-            q[j] = ok ? qv[m] : 0.f;  // q = 0 makes padding particles contribute nothing
-        }
-    }
-};
-
 template <typename Real>
 __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double *__restrict__ zx,
                                              const double *__restrict__ zy, const Real *__restrict__ zh,
@@ -303,54 +289,6 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
             tot[((int64_t)kidx * nch + blockIdx.x) * 4 + threadIdx.x] = sum;
         }
         __syncthreads();
-    }
-}
-
-// FP32 chunk totals, same sums as k_ltot<float>: each thread keeps its four
-// particles' sums for the block's KPB k-vectors in shared memory, and one
-// tree reduction over the block's threads finishes all KPB x 4 totals (one
-// barrier per tree level instead of two barriers and a warp reduction per k).
-__global__ void __launch_bounds__(LT) k_ltot_f32(int N, int P, int nch, const uint32_t *__restrict__ zX,
-                                                 const uint32_t *__restrict__ zY, const float *__restrict__ zh,
-                                                 const float *__restrict__ qv, const KConst *__restrict__ kc,
-                                                 double *__restrict__ tot)
-{
-    constexpr float LOG2E = 1.4426950408889634f;
-    __shared__ float part[KPB * 4][LT + 1];  // +1: rows on different banks
-    QuadF P4;
-    P4.load(N, blockIdx.x * LCH + threadIdx.x * PPT, zX, zY, zh, qv);
-    const int k0 = blockIdx.y * KPB;
-    const int nk = min(KPB, P - k0);
-    for (int kk = 0; kk < nk; kk++) {
-        const KConst K = kc[k0 + kk];
-        const float kl = (float)K.k * LOG2E;
-        float v[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            float s, c;
-            __sincosf(lattice_phase(K.mx, K.my, P4.X[j], P4.Y[j]), &s, &c);
-            const float e = kl * P4.z[j];
-            const float ep = P4.q[j] * ex2_approx(e), em = P4.q[j] * ex2_approx(-e);
-            v[0] = fmaf(ep, c, v[0]);
-            v[1] = fmaf(ep, s, v[1]);
-            v[2] = fmaf(em, c, v[2]);
-            v[3] = fmaf(em, s, v[3]);
-        }
-#pragma unroll
-        for (int r = 0; r < 4; r++) part[4 * kk + r][threadIdx.x] = v[r];
-    }
-    __syncthreads();
-    const int rows = 4 * nk;
-    for (int stride = LT / 2; stride > 0; stride >>= 1) {
-        for (int idx = threadIdx.x; idx < rows * stride; idx += LT) {
-            const int row = idx / stride, col = idx - row * stride;
-            part[row][col] += part[row][col + stride];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x < rows) {
-        const int kk = threadIdx.x >> 2, r = threadIdx.x & 3;
-        tot[((int64_t)(k0 + kk) * nch + blockIdx.x) * 4 + r] = (double)part[threadIdx.x][0];
     }
 }
 
@@ -557,171 +495,260 @@ __global__ void __launch_bounds__(LT, sizeof(Real) == 4 ? LF_MINB : 4) k_lforce(
     }
 }
 
-// FP32 force pass, same terms as k_lforce: the thread's four particles run as
-// two packed FP32x2 pairs (0, 1), (2, 3) through the per-particle algebra,
-// and the next k-vector's constants are fetched while the current one is
-// processed.
-template <bool ENERGY>
-__global__ void __launch_bounds__(LT, LF_MINB) k_lforce_f32(int N, int P, int nch, int ks_n,
-                                                           const uint32_t *__restrict__ zX,
-                                                           const uint32_t *__restrict__ zY,
-                                                           const float *__restrict__ zh, const float *__restrict__ qv,
-                                                           const KConst *__restrict__ kc,
-                                                           const KForce<float> *__restrict__ kf,
-                                                           const float *__restrict__ off, double *__restrict__ Fpart,
-                                                           double *__restrict__ Epart)
+// ---------------------------------------------------------------------------
+// FP32 k-space passes with one lane per k-vector.  Every lane walks the
+// particles of a chunk in z order (warp-uniform loads of packed records
+// {X, Y, z - L_z/2, q}), so the sum over the particles below (A) is a running
+// sum in the lane -- no scans across threads, no barriers -- and the only
+// exchange between lanes is the sum over k of each particle's force: after
+// every KG particles the lanes' KG x 3 partial forces pass through a padded
+// per-warp shared transpose, and lanes 0 .. 3 KG - 1 each add up one column
+// in a fixed order.  Inside a chunk that is thin in z against the largest k
+// of the warp (k dz <= THIN), the sum over the particles above (C) is the
+// chunk's FP64 total minus the running sum of v, whose cancellation is bounded
+// by e^{k dz}; a thicker chunk takes C from a second, descending walk, and
+// each walk then forms its own half of the force.
+// ---------------------------------------------------------------------------
+constexpr int KG = 8;           // particles per cross-lane reduction of the force pass
+constexpr int KTT = 128;        // threads (k-vectors) per block of the totals pass
+constexpr int KFW = 4;          // warps per block of the force pass
+constexpr float THIN = 1.0f;    // largest k * (chunk z extent) of the one-walk path
+
+// chunk totals: lane k sums u = q e^{k (z-h)} e^{i k.rho} and v = q e^{-k (z-h)}
+// e^{i k.rho} over the chunk, in FP32 over 16 particles at a time, in FP64 across
+__global__ void __launch_bounds__(KTT) k_ltot_lk(int N, int P, int nch, const uint4 *__restrict__ zp,
+                                                 const KConst *__restrict__ kc, double *__restrict__ tot)
 {
-    static_assert(PPT == 4, "two packed particle pairs per thread");
     constexpr float LOG2E = 1.4426950408889634f;
-    __shared__ float wsh[2][4][NW];
-    __shared__ double ered[NW];
-    __shared__ double Facc[3 * PPT][LT];  // FP64 sums of the FP32 batches (registers stay free)
-    QuadF P4;
-    const int m0 = blockIdx.x * LCH + threadIdx.x * PPT;
-    P4.load(N, m0, zX, zY, zh, qv);
-    const float2 z2[2] = {f2(P4.z[0], P4.z[1]), f2(P4.z[2], P4.z[3])};
-    const float2 q2[2] = {f2(P4.q[0], P4.q[1]), f2(P4.q[2], P4.q[3])};
+    const int c = blockIdx.x, m0 = c * LCH, n = min(LCH, N - m0);
+    const int k = blockIdx.y * KTT + threadIdx.x;
+    if (k >= P) return;
+    const int mx = kc[k].mx, my = kc[k].my;
+    const float kl = (float)kc[k].k * LOG2E;
+    const uint4 *pp = zp + m0;
+    double U0 = 0, U1 = 0, U2 = 0, U3 = 0;
+    for (int j0 = 0; j0 < n; j0 += 16) {
+        const int je = min(n, j0 + 16);
+        float2 a0 = f2s(0.f), a1 = f2s(0.f), a2 = f2s(0.f), a3 = f2s(0.f);
+#pragma unroll 4
+        for (int j = j0; j < je; j += 2) {
+            const uint4 r0 = pp[j];
+            const uint4 r1 = j + 1 < je ? pp[j + 1] : make_uint4(0u, 0u, 0u, 0u);  // q = 0: no contribution
+            float s0, c0, s1, c1;
+            __sincosf(lattice_phase(mx, my, r0.x, r0.y), &s0, &c0);
+            __sincosf(lattice_phase(mx, my, r1.x, r1.y), &s1, &c1);
+            const float2 e = mul2(f2s(kl), f2(__uint_as_float(r0.z), __uint_as_float(r1.z)));
+            const float2 q = f2(__uint_as_float(r0.w), __uint_as_float(r1.w));
+            const float2 ep = mul2(q, f2(ex2_approx(e.x), ex2_approx(e.y)));
+            const float2 em = mul2(q, f2(ex2_approx(-e.x), ex2_approx(-e.y)));
+            const float2 C = f2(c0, c1), S = f2(s0, s1);
+            a0 = fma2(ep, C, a0);
+            a1 = fma2(ep, S, a1);
+            a2 = fma2(em, C, a2);
+            a3 = fma2(em, S, a3);
+        }
+        U0 += (double)a0.x + (double)a0.y;
+        U1 += (double)a1.x + (double)a1.y;
+        U2 += (double)a2.x + (double)a2.y;
+        U3 += (double)a3.x + (double)a3.y;
+    }
+    double *T = tot + ((int64_t)k * nch + c) * 4;
+    T[0] = U0;
+    T[1] = U1;
+    T[2] = U2;
+    T[3] = U3;
+}
+
+// one lane's k-vector for the force pass (zeros for lanes past P: no force)
+struct LaneK {
+    int mx = 0, my = 0;
+    float kl = 0.f, wfx = 0.f, wfy = 0.f, wk = 0.f, s1r = 0.f, s1i = 0.f, s2r = 0.f, s2i = 0.f;
+    double ek = 0.0;
+};
+
+// one walk over the chunk's particles.  MODE 0: ascending, A and C together
+// (C = chunk total above the first particle minus the running sum of v);
+// MODE 1: ascending, A only (the e_- b half of the force); MODE 2:
+// descending, C only (the e_+ a half).  Partial forces (without the factor q
+// of the particle) are reduced over the warp's lanes every KG particles and
+// written (init) or added to Fo; returns the lane's energy sum (before e_k).
+template <int MODE, bool ENERGY>
+__device__ __forceinline__ float lk_walk(const uint4 *__restrict__ pp, int n, const LaneK &K, float Ar, float Ai,
+                                         float Cr, float Ci, float (*tr)[3 * KG + 1], int lane, double *Fo,
+                                         bool init)
+{
+    const float2 mh = f2s(-0.5f);
+    float Esum = 0.f;
+    const int nblk = (n + KG - 1) / KG;
+#pragma unroll 1
+    for (int bq = 0; bq < nblk; bq++) {
+        const int b = MODE == 2 ? nblk - 1 - bq : bq;
+        const int j0 = b * KG;
+        float f[3 * KG];
+#pragma unroll
+        for (int h = 0; h < KG / 2; h++) {
+            const int hh = MODE == 2 ? KG / 2 - 1 - h : h;  // the descending walk takes pairs from the top
+            const int j = j0 + 2 * hh;
+            const uint4 r0 = j < n ? pp[j] : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 r1 = j + 1 < n ? pp[j + 1] : make_uint4(0u, 0u, 0u, 0u);
+            float s0, c0, s1, c1;
+            __sincosf(lattice_phase(K.mx, K.my, r0.x, r0.y), &s0, &c0);
+            __sincosf(lattice_phase(K.mx, K.my, r1.x, r1.y), &s1, &c1);
+            const float2 e = mul2(f2s(K.kl), f2(__uint_as_float(r0.z), __uint_as_float(r1.z)));
+            const float2 q = f2(__uint_as_float(r0.w), __uint_as_float(r1.w));
+            const float2 ep = f2(ex2_approx(e.x), ex2_approx(e.y)), em = f2(ex2_approx(-e.x), ex2_approx(-e.y));
+            const float2 C = f2(c0, c1), S = f2(s0, s1);
+            float2 im1, re2, pz = f2s(0.f);
+            if (MODE != 2) {  // exclusive prefix from below: A_j, A_{j+1} = A_j + u_j
+                const float2 qep = mul2(q, ep);
+                const float2 ur = mul2(qep, C), ui = mul2(qep, S);
+                const float2 A2r = f2(Ar, Ar + ur.x), A2i = f2(Ai, Ai + ui.x);
+                Ar = A2r.y + ur.y;
+                Ai = A2i.y + ui.y;
+                const float2 br = fma2(A2r, mh, f2s(K.s2r)), bi = fma2(A2i, mh, f2s(K.s2i));
+                const float2 mr = mul2(em, br), mi = mul2(em, bi);
+                if (MODE == 0) {  // C_j = (total above the chunk's first particle) - sum_{i <= j} v_i
+                    const float2 qem = mul2(q, em);
+                    const float2 vr = mul2(qem, C), vi = mul2(qem, S);
+                    const float c0r = Cr - vr.x, c0i = Ci - vi.x;
+                    const float2 C2r = f2(c0r, c0r - vr.y), C2i = f2(c0i, c0i - vi.y);
+                    Cr = C2r.y;
+                    Ci = C2i.y;
+                    const float2 ar = fma2(C2r, mh, f2s(K.s1r)), ai = fma2(C2i, mh, f2s(K.s1i));
+                    const float2 pr = mul2(ep, ar), pi = mul2(ep, ai);
+                    const float2 x1r = add2(pr, mr), x1i = add2(pi, mi);
+                    const float2 x2r = fma2(mr, f2s(-1.f), pr), x2i = fma2(mi, f2s(-1.f), pi);
+                    im1 = fma2(mul2(S, f2s(-1.f)), x1r, mul2(C, x1i));  // Im[e^{-i theta} (e+ a + e- b)]
+                    re2 = fma2(S, x2i, mul2(C, x2r));                   // Re[e^{-i theta} (e+ a - e- b)]
+                    if (ENERGY) {
+                        const float2 zr = fma2(em, A2r, mul2(ep, C2r)), zi = fma2(em, A2i, mul2(ep, C2i));
+                        pz = fma2(C, zr, mul2(S, zi));
+                    }
+                } else {
+                    im1 = fma2(mul2(S, f2s(-1.f)), mr, mul2(C, mi));   // Im[e^{-i theta} e- b]
+                    re2 = mul2(fma2(S, mi, mul2(C, mr)), f2s(-1.f));    // Re[-e^{-i theta} e- b]
+                    if (ENERGY) pz = fma2(C, mul2(em, A2r), mul2(S, mul2(em, A2i)));
+                }
+                if (ENERGY) {  // -q^2 - q Re[e^{-i theta}(e- A + e+ C)] (Energy_long_range_njit.py:10-24)
+                    const float2 t = fma2(mul2(q, f2s(-1.f)), pz, mul2(mul2(q, q), f2s(-1.f)));
+                    Esum += t.x + t.y;
+                }
+            } else {  // exclusive suffix from above, particles j+1 then j: C_{j+1}, C_j = C_{j+1} + v_{j+1}
+                const float2 qem = mul2(q, em);
+                const float2 vr = mul2(qem, C), vi = mul2(qem, S);
+                const float2 C2r = f2(Cr + vr.y, Cr), C2i = f2(Ci + vi.y, Ci);
+                Cr = C2r.x + vr.x;
+                Ci = C2i.x + vi.x;
+                const float2 ar = fma2(C2r, mh, f2s(K.s1r)), ai = fma2(C2i, mh, f2s(K.s1i));
+                const float2 pr = mul2(ep, ar), pi = mul2(ep, ai);
+                im1 = fma2(mul2(S, f2s(-1.f)), pr, mul2(C, pi));  // Im[e^{-i theta} e+ a]
+                re2 = fma2(S, pi, mul2(C, pr));                    // Re[e^{-i theta} e+ a]
+                if (ENERGY) {
+                    const float2 zp2 = fma2(C, mul2(ep, C2r), mul2(S, mul2(ep, C2i)));
+                    const float2 t = mul2(mul2(q, f2s(-1.f)), zp2);
+                    Esum += t.x + t.y;
+                }
+            }
+            f[6 * hh + 0] = K.wfx * im1.x;
+            f[6 * hh + 1] = K.wfy * im1.x;
+            f[6 * hh + 2] = K.wk * re2.x;
+            f[6 * hh + 3] = K.wfx * im1.y;
+            f[6 * hh + 4] = K.wfy * im1.y;
+            f[6 * hh + 5] = K.wk * re2.y;
+        }
+        // sum over the warp's lanes (k-vectors): lane l < 3 KG adds column l,
+        // the component l % 3 of particle j0 + l / 3
+#pragma unroll
+        for (int r = 0; r < 3 * KG; r++) tr[lane][r] = f[r];
+        __syncwarp();
+        const int nv = min(KG, n - j0);
+        if (lane < 3 * nv) {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+            for (int row = 0; row < 32; row += 4) {
+                s0 += tr[row][lane];
+                s1 += tr[row + 1][lane];
+                s2 += tr[row + 2][lane];
+                s3 += tr[row + 3][lane];
+            }
+            const float qj = __uint_as_float(pp[j0 + lane / 3].w);
+            const double v = (double)qj * (double)((s0 + s1) + (s2 + s3));
+            double *o = Fo + (int64_t)j0 * 3 + lane;
+            *o = init ? v : *o + v;
+        }
+        __syncwarp();
+    }
+    return Esum;
+}
+
+// force pass: warp t of chunk c (t = blockIdx.y KFW + w < ks_n) takes the
+// k-groups of 32 vectors g = t, t + ks_n, ... and writes slice t of Fpart
+// (z order, the particle's q applied) and of the energy partials
+template <bool ENERGY>
+__global__ void __launch_bounds__(32 * KFW) k_lforce_lk(int N, int P, int nch, int ks_n,
+                                                        const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
+                                                        const KForce<float> *__restrict__ kf,
+                                                        const float *__restrict__ off, const double *__restrict__ tot,
+                                                        double *__restrict__ Fpart, double *__restrict__ Epart)
+{
+    constexpr float LOG2E = 1.4426950408889634f;
+    __shared__ float tr[KFW][32][3 * KG + 1];  // +1: column reads on distinct banks
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int ks = blockIdx.y;
-    const int ng = (P + LKB - 1) / LKB;
-    const int kb = LKB * (int)((int64_t)ng * ks / ks_n);
-    const int ke = min(P, LKB * (int)((int64_t)ng * (ks + 1) / ks_n));
-#pragma unroll
-    for (int r = 0; r < 3 * PPT; r++) Facc[r][threadIdx.x] = 0.0;
-    float2 bx[2] = {f2s(0.f), f2s(0.f)}, by[2] = {f2s(0.f), f2s(0.f)}, bz[2] = {f2s(0.f), f2s(0.f)};
+    const int t = blockIdx.y * KFW + w;
+    if (t >= ks_n) return;  // whole warp; the kernel has no block barrier
+    const int c = blockIdx.x, m0 = c * LCH, n = min(LCH, N - m0);
+    const uint4 *pp = zp + m0;
+    const float dz = __uint_as_float(pp[n - 1].z) - __uint_as_float(pp[0].z);
+    double *Fo = Fpart + ((int64_t)t * N + m0) * 3;
+    const int G = (P + 31) / 32;
     double E = 0;
-    // constants of k = kidx, fetched one iteration ahead
-    int mxn = 0, myn = 0;
-    double ekn = 0;
-    float4 Kan = make_float4(0, 0, 0, 0), Kbn = Kan, On = Kan;
-    auto fetch = [&](int k) {
-        mxn = kc[k].mx;
-        myn = kc[k].my;
-        if (ENERGY) ekn = kc[k].ek;
-        const float4 *kk = reinterpret_cast<const float4 *>(kf + k);
-        Kan = kk[0];  // k, wfx, wfy, wk
-        Kbn = kk[1];  // s1r, s1i, s2r, s2i
-        On = *reinterpret_cast<const float4 *>(off + ((int64_t)k * nch + blockIdx.x) * 4);
-    };
-    if (kb < ke) fetch(kb);
-    for (int kidx = kb; kidx < ke; kidx++) {
-        const int mx = mxn, my = myn;
-        const double ek = ekn;
-        const float4 Ka = Kan, Kb = Kbn, O = On;
-        if (kidx + 1 < ke) fetch(kidx + 1);
-        const int buf = (kidx - kb) & 1;
-        float2 c2[2], s2[2], ep2[2], em2[2], ur[2], ui[2], vr[2], vi[2];
-        const float2 kl = f2s(Ka.x * LOG2E);
-#pragma unroll
-        for (int pp = 0; pp < 2; pp++) {
-            float cc[2], ss[2];
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int j = 2 * pp + h;
-                __sincosf(lattice_phase(mx, my, P4.X[j], P4.Y[j]), &ss[h], &cc[h]);
-            }
-            c2[pp] = f2(cc[0], cc[1]);
-            s2[pp] = f2(ss[0], ss[1]);
-            const float2 e = mul2(kl, z2[pp]);
-            ep2[pp] = f2(ex2_approx(e.x), ex2_approx(e.y));
-            em2[pp] = f2(ex2_approx(-e.x), ex2_approx(-e.y));
-            const float2 qp = mul2(q2[pp], ep2[pp]), qm = mul2(q2[pp], em2[pp]);
-            ur[pp] = mul2(qp, c2[pp]);
-            ui[pp] = mul2(qp, s2[pp]);
-            vr[pp] = mul2(qm, c2[pp]);
-            vi[pp] = mul2(qm, s2[pp]);
+    bool init = true;
+    for (int g = t; g < G; g += ks_n) {
+        const int k = 32 * g + lane;
+        LaneK K;
+        float Ar = 0.f, Ai = 0.f, Cr = 0.f, Ci = 0.f, Cor = 0.f, Coi = 0.f, kk = 0.f;
+        if (k < P) {
+            K.mx = kc[k].mx;
+            K.my = kc[k].my;
+            kk = (float)kc[k].k;
+            K.kl = kk * LOG2E;
+            if (ENERGY) K.ek = kc[k].ek;
+            const float4 *kf4 = reinterpret_cast<const float4 *>(kf + k);
+            const float4 Ka = kf4[0], Kb = kf4[1];  // (k, wfx, wfy, wk), (s1r, s1i, s2r, s2i)
+            K.wfx = Ka.y;
+            K.wfy = Ka.z;
+            K.wk = Ka.w;
+            K.s1r = Kb.x;
+            K.s1i = Kb.y;
+            K.s2r = Kb.z;
+            K.s2i = Kb.w;
+            const float4 O = *reinterpret_cast<const float4 *>(off + ((int64_t)k * nch + c) * 4);
+            const double *T = tot + ((int64_t)k * nch + c) * 4;
+            Ar = O.x;
+            Ai = O.y;
+            Cor = O.z;
+            Coi = O.w;
+            Cr = (float)((double)O.z + T[2]);  // v above the chunk's first particle: above the chunk + the chunk
+            Ci = (float)((double)O.w + T[3]);
         }
-        // exclusive prefix of u over the particles 0..3 (from below) and
-        // exclusive suffix of v (from above), as packed pairs
-        const float s01r = ur[0].x + ur[0].y, s01i = ui[0].x + ui[0].y;
-        const float2 Arl[2] = {f2(0.f, ur[0].x), f2(s01r, s01r + ur[1].x)};
-        const float2 Ail[2] = {f2(0.f, ui[0].x), f2(s01i, s01i + ui[1].x)};
-        const float tr = Arl[1].y + ur[1].y, ti = Ail[1].y + ui[1].y;
-        const float s23r = vr[1].y + vr[1].x, s23i = vi[1].y + vi[1].x;
-        const float2 Crl[2] = {f2(s23r + vr[0].y, s23r), f2(vr[1].y, 0.f)};
-        const float2 Cil[2] = {f2(s23i + vi[0].y, s23i), f2(vi[1].y, 0.f)};
-        const float br = Crl[0].x + vr[0].x, bi = Cil[0].x + vi[0].x;
-        // warp inclusive scans of the thread totals: forward for u, backward for v
-        float fr = tr, fi = ti, gr = br, gi = bi;
+        float kw = kk;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const float a1 = __shfl_up_sync(0xffffffffu, fr, d), a2 = __shfl_up_sync(0xffffffffu, fi, d);
-            const float b1 = __shfl_down_sync(0xffffffffu, gr, d), b2 = __shfl_down_sync(0xffffffffu, gi, d);
-            if (lane >= d) { fr += a1; fi += a2; }
-            if (lane + d < 32) { gr += b1; gi += b2; }
+        for (int d = 16; d > 0; d >>= 1) kw = fmaxf(kw, __shfl_xor_sync(0xffffffffu, kw, d));
+        float Es;
+        if (kw * dz <= THIN) {
+            Es = lk_walk<0, ENERGY>(pp, n, K, Ar, Ai, Cr, Ci, tr[w], lane, Fo, init);
+        } else {
+            Es = lk_walk<1, ENERGY>(pp, n, K, Ar, Ai, 0.f, 0.f, tr[w], lane, Fo, init);
+            Es += lk_walk<2, ENERGY>(pp, n, K, 0.f, 0.f, Cor, Coi, tr[w], lane, Fo, false);
         }
-        if (lane == 31) { wsh[buf][0][w] = fr; wsh[buf][1][w] = fi; }
-        if (lane == 0) { wsh[buf][2][w] = gr; wsh[buf][3][w] = gi; }
-        float xr = __shfl_up_sync(0xffffffffu, fr, 1), xi = __shfl_up_sync(0xffffffffu, fi, 1);
-        float yr = __shfl_down_sync(0xffffffffu, gr, 1), yi = __shfl_down_sync(0xffffffffu, gi, 1);
-        if (lane == 0) { xr = 0; xi = 0; }
-        if (lane == 31) { yr = 0; yi = 0; }
-        __syncthreads();
-#pragma unroll
-        for (int ww = 0; ww < NW; ww++) {
-            if (ww < w) { xr += wsh[buf][0][ww]; xi += wsh[buf][1][ww]; }
-            if (ww > w) { yr += wsh[buf][2][ww]; yi += wsh[buf][3][ww]; }
-        }
-        const float2 bAr = f2s(O.x + xr), bAi = f2s(O.y + xi), bCr = f2s(O.z + yr), bCi = f2s(O.w + yi);
-        const float2 mh = f2s(-0.5f), m1 = f2s(-1.f);
-#pragma unroll
-        for (int pp = 0; pp < 2; pp++) {
-            const float2 Ar = add2(bAr, Arl[pp]), Ai = add2(bAi, Ail[pp]);
-            const float2 Cr = add2(bCr, Crl[pp]), Ci = add2(bCi, Cil[pp]);
-            const float2 ar = fma2(Cr, mh, f2s(Kb.x)), ai = fma2(Ci, mh, f2s(Kb.y));
-            const float2 br_ = fma2(Ar, mh, f2s(Kb.z)), bi_ = fma2(Ai, mh, f2s(Kb.w));
-            const float2 pr = mul2(ep2[pp], ar), pi = mul2(ep2[pp], ai);
-            const float2 mr = mul2(em2[pp], br_), mi = mul2(em2[pp], bi_);
-            const float2 x1r = add2(pr, mr), x1i = add2(pi, mi);
-            const float2 x2r = fma2(mr, m1, pr), x2i = fma2(mi, m1, pi);
-            const float2 im1 = fma2(mul2(s2[pp], m1), x1r, mul2(c2[pp], x1i));  // Im[e^{-i theta} X1]
-            const float2 re2 = fma2(s2[pp], x2i, mul2(c2[pp], x2r));           // Re[e^{-i theta} X2]
-            bx[pp] = fma2(f2s(Ka.y), im1, bx[pp]);
-            by[pp] = fma2(f2s(Ka.z), im1, by[pp]);
-            bz[pp] = fma2(f2s(Ka.w), re2, bz[pp]);
-            if (ENERGY) {
-                // Energy_long_range_njit.py:10-24 (sorted part), Re[e^{-i theta}(em A + ep C)]
-                const float2 zr = fma2(em2[pp], Ar, mul2(ep2[pp], Cr)), zi = fma2(em2[pp], Ai, mul2(ep2[pp], Ci));
-                const float2 pz = fma2(c2[pp], zr, mul2(s2[pp], zi));
-                const float2 q = q2[pp];
-                E += ek * 0.5 * ((double)(-q.x * q.x - q.x * pz.x) + (double)(-q.y * q.y - q.y * pz.y));
-            }
-        }
-        if ((kidx + 1) % LKB == 0) {
-#pragma unroll
-            for (int pp = 0; pp < 2; pp++) {
-                Facc[6 * pp + 0][threadIdx.x] += (double)bx[pp].x;
-                Facc[6 * pp + 1][threadIdx.x] += (double)bx[pp].y;
-                Facc[6 * pp + 2][threadIdx.x] += (double)by[pp].x;
-                Facc[6 * pp + 3][threadIdx.x] += (double)by[pp].y;
-                Facc[6 * pp + 4][threadIdx.x] += (double)bz[pp].x;
-                Facc[6 * pp + 5][threadIdx.x] += (double)bz[pp].y;
-                bx[pp] = f2s(0.f); by[pp] = f2s(0.f); bz[pp] = f2s(0.f);
-            }
-        }
+        if (ENERGY) E += K.ek * 0.5 * (double)Es;
+        init = false;
     }
-#pragma unroll
-    for (int j = 0; j < PPT; j++) {
-        const int m = m0 + j;
-        const int pp = j >> 1, h = j & 1;
-        const float2 bxv = bx[pp], byv = by[pp], bzv = bz[pp];
-        if (m < N) {
-            const double q = (double)P4.q[j];
-            double *o = Fpart + ((int64_t)ks * N + m) * 3;
-            o[0] = q * (Facc[6 * pp + 0 + h][threadIdx.x] + (double)(h ? bxv.y : bxv.x));
-            o[1] = q * (Facc[6 * pp + 2 + h][threadIdx.x] + (double)(h ? byv.y : byv.x));
-            o[2] = q * (Facc[6 * pp + 4 + h][threadIdx.x] + (double)(h ? bzv.y : bzv.x));
-        }
-    }
+    if (init)  // no k-group for this warp (fewer groups than slices): a zero slice
+        for (int i = lane; i < 3 * n; i += 32) Fo[i] = 0.0;
     if (ENERGY) {
         for (int d = 16; d > 0; d >>= 1) E += __shfl_down_sync(0xffffffffu, E, d);
-        if (lane == 0) ered[w] = E;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double sum = 0;
-            for (int ww = 0; ww < NW; ww++) sum += ered[ww];
-            Epart[(int64_t)ks * nch + blockIdx.x] = sum;
-        }
+        if (lane == 0) Epart[(int64_t)t * nch + c] = E;
     }
 }
 
@@ -1169,8 +1196,17 @@ static int sm_count()
     return cached[d];
 }
 
-int qem_long_ksplit(int nch, int P, int max_ks)
+int qem_long_ksplit(int nch, int P, int max_ks, int precision)
 {
+    if (precision != QEM_FP64) {
+        // lane-per-k force pass: one warp per (chunk, slice), about QEM_LK_WARPS
+        // resident warps per SM in one wave, and at least one 32-vector
+        // k-group per warp
+        const int groups = P > 0 ? (P + 31) / 32 : 1;
+        int ks = (int)((int64_t)sm_count() * QEM_LK_WARPS / (int64_t)(nch > 0 ? nch : 1));
+        ks = ks < 1 ? 1 : (ks > max_ks ? max_ks : ks);
+        return ks < groups ? ks : groups;
+    }
     // as many whole k-slices of the nch chunks as fit in QEM_LF_WAVES_PCT / 100
     // waves of resident force-pass blocks, each slice with at least two k
     // groups of LKB vectors
@@ -1188,22 +1224,22 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
 {
     if (N <= 0) return cudaSuccess;
     const double zlim = precision == QEM_FP64 ? 0.0 : b.zlim;
-    uint32_t *zX = precision == QEM_FP64 ? nullptr : b.zX, *zY = precision == QEM_FP64 ? nullptr : b.zY;
+    uint4 *zP = precision == QEM_FP64 ? nullptr : b.zP;
     if (stage == 0 && !energy && N <= LONG_PREP_SMALL) {
         const double h = 0.5 * Lz;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
         const double wk = P > 0 ? (sum_K / P) / (Lx * Ly * eps0) : 0.0;
         const double esc = P > 0 ? -(sum_K / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
-        k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, b.qscan, fscale,
-                                             b.k0, P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                             2.0 * eps0 * Lx * Ly, zlim, status, b.sampler, b.draw_ctr, zX, zY, 1.0 / Lx,
+        k_long_prep_small<<<1, 1024, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhd, b.qd, b.qscan, fscale, b.k0, P,
+                                             b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
+                                             2.0 * eps0 * Lx * Ly, zlim, status, b.sampler, b.draw_ctr, zP, 1.0 / Lx,
                                              1.0 / Ly, Lx / (2.0 * QEM_PI), Ly / (2.0 * QEM_PI));
         if (P > 0) {
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
-                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zX, b.zY, b.zhf, b.qf, b.kc, b.tot);
+                k_ltot_lk<<<dim3(nch, nblk(P, KTT)), KTT, 0, s>>>(N, P, nch, b.zP, b.kc, b.tot);
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
@@ -1215,8 +1251,8 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     }
     if (stage == 0) {
         const double h = 0.5 * Lz;
-        k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhf, b.zhd, b.qf, b.qd, zlim,
-                                               status, zX, zY, 1.0 / Lx, 1.0 / Ly);
+        k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhd, b.qd, zlim, status, zP,
+                                               1.0 / Lx, 1.0 / Ly);
         cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
         if (e != cudaSuccess) return e;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
@@ -1233,7 +1269,7 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
-                k_ltot_f32<<<gt, LT, 0, s>>>(N, P, nch, b.zX, b.zY, b.zhf, b.qf, b.kc, b.tot);
+                k_ltot_lk<<<dim3(nch, nblk(P, KTT)), KTT, 0, s>>>(N, P, nch, b.zP, b.kc, b.tot);
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
@@ -1255,12 +1291,11 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     } else {
         const KForce<float> *kf = (const KForce<float> *)b.kf;
         const float *of = (const float *)b.off;
+        const dim3 gl(nch, nblk(b.ks, KFW));
         if (energy)
-            k_lforce_f32<true><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zX, b.zY, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
-                                                 b.Epart);
+            k_lforce_lk<true><<<gl, 32 * KFW, 0, s>>>(N, P, nch, b.ks, b.zP, b.kc, kf, of, b.tot, b.Fpart, b.Epart);
         else
-            k_lforce_f32<false><<<gf, LT, 0, s>>>(N, P, nch, b.ks, b.zX, b.zY, b.zhf, b.qf, b.kc, kf, of, b.Fpart,
-                                                  b.Epart);
+            k_lforce_lk<false><<<gl, 32 * KFW, 0, s>>>(N, P, nch, b.ks, b.zP, b.kc, kf, of, b.tot, b.Fpart, b.Epart);
     }
     k_lfinal<<<nblk(N, 256), 256, 0, s>>>(N, b.ks, b.Fpart, b.k0, zperm, F3, b.draw_ctr);
     return cudaGetLastError();

@@ -47,12 +47,9 @@ constexpr size_t O_ZY = O_ZX + al(sizeof(double) * NA_MAX_N);
 constexpr size_t O_ZHD = O_ZY + al(sizeof(double) * NA_MAX_N);
 constexpr size_t O_QD = O_ZHD + al(sizeof(double) * NA_MAX_N);
 constexpr size_t O_K0 = O_QD + al(sizeof(double) * NA_MAX_N);
-constexpr size_t O_ZHF = O_K0 + al(sizeof(double) * NA_MAX_N);
-constexpr size_t O_QF = O_ZHF + al(sizeof(float) * NA_MAX_N);
-constexpr size_t O_QSCAN = O_QF + al(sizeof(float) * NA_MAX_N);
-constexpr size_t O_ZX32 = O_QSCAN + al(sizeof(double) * (NA_MAX_N + 1));
-constexpr size_t O_ZY32 = O_ZX32 + al(sizeof(uint32_t) * NA_MAX_N);
-constexpr size_t O_KIN = O_ZY32 + al(sizeof(uint32_t) * NA_MAX_N);
+constexpr size_t O_QSCAN = O_K0 + al(sizeof(double) * NA_MAX_N);
+constexpr size_t O_ZP = O_QSCAN + al(sizeof(double) * (NA_MAX_N + 1));
+constexpr size_t O_KIN = O_ZP + al(sizeof(uint4) * NA_MAX_N);
 constexpr size_t O_KC = O_KIN + al(sizeof(double) * 3 * NA_MAX_P);
 constexpr size_t O_TOT = O_KC + al(sizeof(KConst) * NA_MAX_P);
 constexpr size_t O_OFF = O_TOT + al(sizeof(double) * 4 * (size_t)NA_MAX_P * NA_MAX_NCH);
@@ -140,20 +137,19 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
         e = qem_launch_zsort(N, pos, zperm, (int *)(S + O_ZTMP), (double *)(S + O_ZKEY), (double *)(S + O_ZKEY2), s);
     LongBuffers b;
     b.zx = (double *)(S + O_ZX); b.zy = (double *)(S + O_ZY);
-    b.zhf = (float *)(S + O_ZHF); b.zhd = (double *)(S + O_ZHD);
-    b.qf = (float *)(S + O_QF); b.qd = (double *)(S + O_QD);
+    b.zhd = (double *)(S + O_ZHD);
+    b.qd = (double *)(S + O_QD);
     b.k0 = (double *)(S + O_K0); b.qscan = (double *)(S + O_QSCAN);
     b.kc = (KConst *)(S + O_KC); b.kin = (double *)(S + O_KIN);
     b.tot = (double *)(S + O_TOT); b.off = (double *)(S + O_OFF); b.Utot = (double *)(S + O_UTOT);
     b.kf = S + O_KF;
     b.Epart = (double *)(S + O_EPART);
     const int nch = (N + NA_CH - 1) / NA_CH;
-    b.ks = qem_long_ksplit(nch, P, NA_MAX_KS);
+    b.ks = qem_long_ksplit(nch, P, NA_MAX_KS, p->precision);
     b.Fpart = (double *)(S + O_FPART);
     b.Eks = b.Epart + (size_t)b.ks * nch + (NA_MAX_N + 255) / 256;
     b.stmp = S + O_STMP; b.stmp_bytes = STMP_BYTES;
-    b.zX = (uint32_t *)(S + O_ZX32);
-    b.zY = (uint32_t *)(S + O_ZY32);
+    b.zP = (uint4 *)(S + O_ZP);
     b.zlim = p->precision == QEM_FP32_FIX && P > 0 ? qem_fp32_zlim(kmax) : 0.0;
     for (int stage = 0; stage < 2 && e == cudaSuccess; stage++)
         e = qem_launch_long(p->precision, false, N, P, pos, zperm, b, p->Lx, p->Ly, p->Lz, p->gamma_down, p->gamma_up,
