@@ -183,6 +183,51 @@ class RefEvaluator:
                 f"each), {seconds:.1f} s each")
 
 
+# ----------------------------------------------------------------------------- adjoint
+def backward_timing(lib, local, dev, K=10):
+    """qem_backward (FP64) on the differentiation workload -- config 3: N = 2e4,
+    |q| ~ U[0.5, 1.5] re-neutralised, Lx = Ly = 450, Lz = 10, gamma_up = 0.8,
+    gamma_down = -0.6, P = 500, loss = E + sum_i w_i . F_i with w ~ N(0, 1) --
+    on device buffers, beside the FP64 forward pass with energy it
+    differentiates (CUDA events, K calls each after two warm-up calls)."""
+    import numpy as np
+    import torch
+
+    from qem4molly_b200 import workloads as W
+
+    cfg = W.config3()
+    e = W.engine_for(cfg, "fp64", device=local)
+    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
+    q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
+    w = torch.tensor(np.random.default_rng(20261206).normal(size=cfg["xyz"].shape), dtype=torch.float64, device=dev)
+    gx, gq, F = torch.empty_like(x), torch.empty_like(q), torch.empty_like(x)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(K):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / K
+
+    ms_b = timed(lambda: e.backward_device(x, q, w, 1.0, gx, gq))
+    ms_f = timed(lambda: e.forces_device(x, q, F, energy=True))
+    p64 = C.c_double(0)
+    lib.qem_measure_fp64_peak(local, C.byref(p64))
+    e.close()
+    return {"workload": f"config 3: N={cfg['N']} Lx=Ly=450 Lz=10 gamma_up=0.8 gamma_down=-0.6 P={cfg['P']}, "
+                        "loss = E + sum_i w_i . F_i, gradients w.r.t. positions, charges and both gammas (FP64)",
+            "ms": ms_b, "value": 1000.0 / ms_b, "unit": "backward passes/s", "forward_fp64_energy_ms": ms_f,
+            "ratio_to_forward": ms_b / ms_f, "fp64_peak_tflops": p64.value,
+            "note": "device buffers; includes the neighbour list, the forward quantities the backward needs and "
+                    "the short- and long-range adjoint passes"}
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def run_ours(args):
     import numpy as np
@@ -294,6 +339,8 @@ def run_ours(args):
     e2e = {"value": world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(xh.numel() * 8 + qh.numel() * 8),
            "d2h_bytes_per_step": int(Fh.numel() * 8)}
 
+    backward = backward_timing(lib, local, dev)
+
     # roofline of the dominant kernel (short-range pair quadrature, FP32)
     Np = counts["pairs"]
     nodes = Np * 8 * cfg["N_t"]
@@ -327,7 +374,8 @@ def run_ours(args):
            "e2e": e2e, "gpu_launches": int(counts["launches"]) * args.steps, "roofline": roofline,
            "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64, "steps": K64},
            "speedup_vs_fp64": ms64 / ms32, "force_rel_err_vs_fp64": err, "force_max_err_vs_fp64_rms": err_max,
-           "kernel_ms": {"fp32": kt32, "fp64": kt64, "fp32_short_only": kt32_short}, "clocks": clk}
+           "kernel_ms": {"fp32": kt32, "fp64": kt64, "fp32_short_only": kt32_short}, "backward": backward,
+           "clocks": clk}
     if rank == 0 and world == 1:
         ref = RefEvaluator(cfg)
         t0 = time.perf_counter()

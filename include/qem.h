@@ -363,6 +363,9 @@ const char *qem_version(void);
  * kernels, which are bound by those two pipes.  Diagnostic; no reference
  * counterpart. */
 qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, double *mufu_tops);
+/* Measured FP64 FMA throughput (TFLOP/s) of `device`: the roofline
+ * denominator of the FP64 path and of qem_backward.  Diagnostic. */
+qem_status qem_measure_fp64_peak(int32_t device, double *fp64_tflops);
 
 #ifdef __cplusplus
 }

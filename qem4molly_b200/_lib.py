@@ -104,6 +104,7 @@ def load(build: bool = False):
         "qem_get_counts": (C.c_int32, [H, C.POINTER(C.c_int64), C.c_int32]),
         "qem_version": (C.c_char_p, []),
         "qem_measure_peaks": (C.c_int32, [C.c_int32, dp, dp]),
+        "qem_measure_fp64_peak": (C.c_int32, [C.c_int32, dp]),
         "qem_long_forces_noalloc": (C.c_int32, [PP, C.c_int32, vp, vp, C.c_int32, dp, C.c_double, vp, vp]),
         "qem_set_shard": (C.c_int32, [H, C.c_int32, C.c_int32]),
         "qem_batch_create": (C.c_int32, [C.c_int32, C.POINTER(H), ip, C.POINTER(vp)]),

@@ -64,7 +64,55 @@ __global__ void k_mufu_peak(int iters, float seed, float *out)
     if (s == 1234.5f) out[0] = s;
 }
 
+// FP64 FMA chains (the roofline denominator of the FP64 path and the adjoint)
+__global__ void k_dfma_peak(int iters, double seed, double *out)
+{
+    double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+           a7 = a0 + 7;
+    const double m = 0.9999999999, c = 1e-10;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+            a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+        }
+    }
+    const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 1234.5) out[0] = s;
+}
+
 }  // namespace
+
+extern "C" qem_status qem_measure_fp64_peak(int32_t device, double *fp64_tflops)
+{
+    if (!fp64_tflops) return QEM_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return QEM_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return QEM_ERR_CUDA;
+    double *d = nullptr;
+    if (cudaMalloc(&d, 64) != cudaSuccess) return QEM_ERR_CUDA;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 1024;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        float t = 0;
+        cudaEventRecord(a);
+        k_dfma_peak<<<blocks, threads>>>(iters, 1.0, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t, a, b);
+        if (rep > 0) best = std::min(best, t);
+    }
+    const cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return QEM_ERR_CUDA;
+    *fp64_tflops = 2.0 * (double)blocks * threads * iters * 16 * 8 / (best * 1e-3) * 1e-12;
+    return QEM_OK;
+}
 
 extern "C" qem_status qem_measure_peaks(int32_t device, double *fp32_tflops, double *mufu_tops)
 {

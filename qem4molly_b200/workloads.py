@@ -153,6 +153,8 @@ def main(argv=None):
                     help="round z to multiples of this spacing and evaluate with QEM_EQUAL_Z_TIES")
     ap.add_argument("--norm", action="store_true",
                     help="gamma_1 = gamma_2 = e with Lz = 2 (regularised quadrature, python mode, FP64)")
+    ap.add_argument("--backward", action="store_true",
+                    help="time qem_backward (FP64) for loss = E + sum_i w_i . F_i, w ~ N(0, 1), instead")
     a = ap.parse_args(argv)
     from . import _lib as L
 
@@ -176,6 +178,14 @@ def main(argv=None):
     x = torch.tensor(cfg["xyz"], dtype=torch.float64, device=dev)
     q = torch.tensor(cfg["q"], dtype=torch.float64, device=dev)
     F = torch.empty_like(x)
+    if a.backward:
+        w = torch.tensor(np.random.default_rng(SEED0 + 6).normal(size=cfg["xyz"].shape), device=dev)
+        gx, gq = torch.empty_like(x), torch.empty_like(q)
+        for _ in range(a.evals):
+            e.backward_device(x, q, w, 1.0, gx, gq)
+        torch.cuda.synchronize()
+        print(f"config {a.config}: N={len(cfg['q'])}, {a.evals} backward passes, |dL/dr|_max={gx.abs().max().item():.6e}")
+        return
     for _ in range(3):
         e.forces_device(x, q, F)
     torch.cuda.synchronize()

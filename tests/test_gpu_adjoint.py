@@ -165,3 +165,67 @@ def test_backward_host_device_and_torch_agree(case):
     gx, gq, _ = e.backward(cfg["xyz"], cfg["q"], gF, 0.7, terms=L.QEM_TERM_ALL)
     assert np.array_equal(x.grad.cpu().numpy(), gx)
     assert np.array_equal(q.grad.cpu().numpy(), gq)
+
+
+def test_adjoint_config3_full_size_vs_fd():
+    """Config 3 at its stated size: N = 2e4, |q| ~ U[0.5, 1.5] with random sign
+    re-neutralised, Lx = Ly = 450, Lz = 10, gamma_up = 0.8, gamma_down = -0.6,
+    P = 500; loss = E + sum_i w_i . F_i with w ~ N(0, 1) (seeded).  Each
+    derivative against central differences with Richardson extrapolation
+    (h = 1e-4 and 2e-4, error O(h^4)) to 1e-6 relative, on every checked
+    component whose derivative is not itself at the difference's noise level
+    (|fd| >= 1e-4 of the gradient's rms); at least 16 of the 20 position and
+    charge components, and both gammas, are checked."""
+    cfg = W.config3()
+    assert cfg["N"] == 20_000 and cfg["L"] == (450.0, 450.0, 10.0)
+    rng = np.random.default_rng(20261206)
+    gF = rng.normal(size=cfg["xyz"].shape)
+    e = W.engine_for(cfg, "fp64")
+    xyz, q, gE = cfg["xyz"].copy(), cfg["q"].copy(), 1.0
+    gx, gq, gg = e.backward(xyz, q, gF, gE)
+    sx, sq = np.sqrt(np.mean(gx ** 2)), np.sqrt(np.mean(gq ** 2))
+
+    def rich(shift):
+        d = []
+        for h in (H, 2 * H):
+            (xp, qp), (xm, qm) = shift(h), shift(-h)
+            d.append(_fd(e, xp, xm, qp, qm, gF, gE, L.QEM_TERM_ALL, h=h))
+        return (4 * d[0] - d[1]) / 3
+
+    checked, worst = 0, 0.0
+    for i in _safe_particles(cfg, 5, np.random.default_rng(7), h=2 * H):
+        for a in range(4):
+            def shift(h, i=i, a=a):
+                x2, q2 = xyz.copy(), q.copy()
+                if a < 3:
+                    x2[i, a] += h
+                else:
+                    q2[i] += h
+                return x2, q2
+            fd = rich(shift)
+            g = gx[i, a] if a < 3 else gq[i]
+            if abs(fd) < 1e-4 * (sx if a < 3 else sq):
+                continue
+            rel = abs(fd - g) / abs(fd)
+            worst = max(worst, rel)
+            assert rel <= 1e-6, (i, a, fd, g, rel)
+            checked += 1
+    assert checked >= 16, checked
+    k3, sum_K = e.get_kset()
+    for which, key in ((0, "gamma_down"), (1, "gamma_up")):
+        d = []
+        for h in (H, 2 * H):
+            out = []
+            for sgn in (1, -1):
+                c = dict(cfg)
+                c[key] = cfg[key] + sgn * h
+                ee = W.engine_for(c, "fp64")
+                ee.set_kset(k3, sum_K)
+                out.append(ee.forces(xyz, q, terms=L.QEM_TERM_ALL, energy=True))
+                ee.close()
+            d.append((float(np.sum(gF * (out[0][0] - out[1][0]))) + gE * (out[0][1] - out[1][1])) / (2 * h))
+        fd = (4 * d[0] - d[1]) / 3
+        rel = abs(fd - gg[which]) / abs(fd)
+        worst = max(worst, rel)
+        assert rel <= 1e-6, (key, fd, gg[which], rel)
+    print(f"config 3 adjoint: {checked} position/charge components and 2 gammas within {worst:.1e} relative")
