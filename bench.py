@@ -383,10 +383,30 @@ def run_ours(args):
         t_ref = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": 1.0 / t_ref, "unit": UNIT, "cores": ref.cores, "kind": "port",
                                "sample": ref.describe(1, t_ref)}
-    if rank == 0:
-        print(json.dumps(out), flush=True)
     e32.close()
     e64.close()
+    if world == 1:
+        # the two other workloads, recorded in this line too (each times its own steps with CUDA events)
+        import argparse
+
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = 300, 3
+        bo = run_batch(sub, quiet=True)
+        out["batch_md"] = {"metric": bo["metric"], "value": bo["value"], "unit": bo["unit"],
+                           "ms_per_step": bo["ms_per_step"], "steps": bo["steps"],
+                           "workload": bo["config"]["workload"], "kset": bo["config"]["kset"],
+                           "particles": bo["config"]["particles_per_gpu"], "batch_mode": bo["batch_mode"],
+                           "batch_forces_graph_ms": bo["batch_forces_graph_ms"],
+                           "particle_steps_per_s": bo["particle_steps_per_s"], "clocks": bo["clocks"]}
+        sub.steps = 30
+        xo = run_exact(sub, quiet=True, cpu_leg=False)
+        out["exact_ksum"] = {"metric": xo["metric"], "value": xo["value"], "unit": xo["unit"],
+                             "ms_per_step": xo["ms_per_step"], "steps": xo["steps"],
+                             "workload": xo["config"]["workload"], "fp64_value": xo["fp64"]["value"],
+                             "force_rel_err_vs_fp64": xo["force_rel_err_vs_fp64"],
+                             "mufu_frac": xo["roofline"]["frac"], "clocks": xo["clocks"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
 
@@ -395,10 +415,11 @@ def run_ours(args):
 
 
 # ----------------------------------------------------------------------------- batch workload
-def run_batch(args):
+def run_batch(args, quiet=False):
     import numpy as np
     import torch
 
+    from qem4molly_b200 import _lib as L
     from qem4molly_b200 import workloads as W
     from qem4molly_b200.api import Batch
 
@@ -407,7 +428,9 @@ def run_batch(args):
     torch.cuda.set_device(dev)
     tt = [time.perf_counter()]
     cfgs = W.config4(seed=None if rank == 0 else 20261203 + 4 + 1000 * rank)
-    engines = [W.engine_for(c, "fp32", seed=100 + i, device=local) for i, c in enumerate(cfgs)]
+    # a fresh random batch of k-vectors every step (Force_long.jl:235), drawn on the device
+    engines = [W.engine_for(c, "fp32", mode_flags=L.QEM_RESAMPLE_KSET, seed=100 + i, device=local)
+               for i, c in enumerate(cfgs)]
     tt.append(time.perf_counter())
     N = [c["N"] for c in cfgs]
     x = torch.tensor(np.concatenate([c["xyz"] for c in cfgs]), device=dev)
@@ -418,6 +441,7 @@ def run_batch(args):
     b.forces(x, q, F)
     tt.append(time.perf_counter())
     width, ms_eval = b.autotune(x, q, F)
+    mode = b.mode()
     tt.append(time.perf_counter())
     dt = 1e-3
     b.md(max(args.warmup, 3), dt, x, v, q, F)
@@ -459,21 +483,28 @@ def run_batch(args):
                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64fix", "data": "synthetic (seeded)",
                "config": {"workload": "256 slabs per GPU: N ~ U[200, 5000], density 0.01, Lz ~ U[5, 20], "
                                       "gamma ~ U(-0.95, 0.95)^2, alpha 0.1, r_c 10, P 200; dt 1e-3, unit masses",
-                          "systems": n_sys, "particles_per_gpu": int(sum(N)), "pool_width": width,
+                          "systems": n_sys, "particles_per_gpu": int(sum(N)),
+                          "kset": "a fresh seeded random batch of P k-vectors per system on every step",
                           "l2": "working set (< 100 MB) stays in L2 between steps; not flushed"},
+               "batch_mode": {"mode": mode["mode"], "pool_width": width, "ks_per_system": mode["ks"],
+                              "order": ["batch", "largest first"][mode["order"]],
+                              "launches_per_evaluation": mode["launches"], "why_not_fused": mode["why"]},
                "batch_forces_graph_ms": ms_eval, "eager_per_system_forces_ms": eager_ms,
                "particle_steps_per_s": args.steps * sum(N) * world * 1000.0 / ms,
                "andersen": {"kT": 1.0, "nu": 10.0, "steps": K_a, "ms_per_step": ms_a / K_a,
                             "value": K_a * 1000.0 / ms_a, "unit": "steps/s"},
                "clocks": clocks}
-        print(json.dumps(out), flush=True)
+        if not quiet:
+            print(json.dumps(out), flush=True)
+        return out
+    return None
 
 # ----------------------------------------------------------------------------- exact k-sum workload
 FLOPS_PER_K_TERM = 80   # op model per (k, particle) long-range term (FP32 flops)
 SFU_PER_K_TERM = 4      # MUFU ops per term in the same model
 
 
-def run_exact(args):
+def run_exact(args, quiet=False, cpu_leg=True):
     import numpy as np
     import torch
 
@@ -551,7 +582,7 @@ def run_exact(args):
                             "peak_source": "measured in this run (qem_measure_peaks)", "traffic": None},
                "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64},
                "force_rel_err_vs_fp64": err, "force_max_err_vs_fp64_rms": err_max, "clocks": clocks}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and cpu_leg:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
@@ -565,8 +596,9 @@ def run_exact(args):
         out["cpu_baseline"] = {"value": 1.0 / (t_s * P / n_s), "unit": "evals/s", "cores": cores, "kind": "port",
                                "sample": f"oracle FP64 on {cores} threads: {n_s} of {P} k-vectors over all {N} "
                                          f"particles ({t_s:.1f} s), extrapolated to the full k-set"}
-    if rank == 0:
+    if rank == 0 and not quiet:
         print(json.dumps(out), flush=True)
+    return out
 
 
 # ----------------------------------------------------------------------------- reference arm

@@ -176,7 +176,11 @@ const char *qem_status_string(qem_status s);
  * finaliser of (seed, n, i, 0..2), one to choose between the m_x != 0 and the
  * m_x = 0 parts of the lattice (weights S_x T_y and S_y, S = sum over m != 0,
  * T = sum over all m of exp(-(2 pi m / L)^2 / 4 alpha)) and two for m_x, m_y by
- * inverse CDF, so the draw is exact without rejection.  With
+ * inverse CDF, so the draw is exact without rejection.  The reference keeps
+ * the probabilities as Float32 (K_set_generator.jl:43), so points whose
+ * probability is at most 2^-150 are never drawn there; a row that lands on
+ * one (less than 2^-150 per row) takes the next three words (i, 3 t .. 3 t + 2)
+ * instead, at most 16 times.  With
  * QEM_RESAMPLE_KSET every long-range call draws the next batch on the device
  * (the batch counter, reset by qem_sample_kset, is in device memory), and
  * qem_get_kset returns the rows of the latest call's batch (the current
@@ -312,13 +316,31 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  * [off[s], off[s] + N[s]) of xyz (3 per particle), q, F and v, with off the
  * exclusive prefix sum of N.  The handles stay owned by the caller.
  *
+ * A batch evaluation runs one of two ways (qem_batch_set_mode):
+ *   QEM_BATCH_FUSED: eight launches for the whole batch -- one block per
+ *     system for pack, cells, pair list and z order; one launch per phase
+ *     (pair forces; long-range preparation, chunk totals, their scan, the
+ *     k-sliced force pass and the final sum; the gather) over a (system,
+ *     tile) work list.  Every system must take the small-system kernels in
+ *     FP32+fix: N <= 8192, fewer than two particles per cell on average (or
+ *     fewer than 3 cells along x or y), no equal-z tie mode, no shard, and
+ *     terms with both QEM_TERM_SHORT and QEM_TERM_LONG.  Each system's forces
+ *     are those of its own qem_forces call with the same k-slice count.
+ *   QEM_BATCH_POOL: every system's own pipeline, forked over a pool of
+ *     streams (any batch).
+ *   QEM_BATCH_AUTO (default): fused when every system qualifies, else the
+ *     pool; qem_batch_autotune may pick either.
+ *
  * qem_batch_forces: forces of every system (terms as in qem_forces).  The
- *   first call (and the first after a change of terms) runs each system
- *   synchronously to size its buffers and upload its k-set; later calls only
- *   enqueue work on `stream` (a pool of streams forked from it), allocate
- *   nothing and can be captured into a CUDA graph.  Device status (pair-list
- *   overflow, non-finite input, particle out of the slab) accumulates and is
- *   reported by qem_batch_check, which synchronises `stream`.
+ *   first call (and the first after a change of terms, of the mode, or of a
+ *   handle's buffers or k-set) runs each system synchronously to size its
+ *   buffers and upload its k-set, and builds the fused work lists; later
+ *   calls only enqueue work on `stream` (forked to a second stream, or to the
+ *   pool, and joined), allocate nothing and can be captured into a CUDA
+ *   graph.  Device status (pair-list overflow, non-finite input, particle out
+ *   of the slab) accumulates and is reported by qem_batch_check, which
+ *   synchronises `stream`; after an overflow the next qem_batch_forces sizes
+ *   every system again.
  * qem_batch_md: nsteps velocity-Verlet steps of every system (unit masses,
  *   x += v dt + F dt^2 / 2, v += (F + F') dt / 2, x and y wrapped into the
  *   box), with one step recorded once as a CUDA graph and replayed.  On
@@ -328,8 +350,18 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  *   (on the device, inside the recorded step), the others keep their current
  *   k-set for the whole run.
  * qem_batch_autotune: times the graph-replayed force evaluation for stream
- *   pool widths 1, 2, 4, ... up to min(B, 128) and keeps the fastest;
- *   returns the width and its time per batch evaluation (ms).
+ *   pool widths 1, 2, 4, ... up to min(B, 128) and, when the batch can run
+ *   fused, for the fused tilings (k-slices per system of the force pass: the
+ *   handle's own count or at most 1, 2, 4; work lists in batch order or
+ *   largest system first), and keeps the fastest; returns the pool width (0
+ *   when the fused phases won) and the time per batch evaluation (ms).
+ * qem_batch_set_mode: mode (QEM_BATCH_AUTO, _FUSED or _POOL), ks (k-slices
+ *   per system of the fused force pass, 0 = each handle's own) and order (0
+ *   batch order, 1 largest system first) of the fused work lists.  A fused
+ *   request for a batch that does not qualify fails at qem_batch_forces.
+ * qem_batch_get_mode: the way evaluations run now (QEM_BATCH_FUSED or
+ *   QEM_BATCH_POOL), ks, order, the kernel launches per fused evaluation
+ *   (-1 on the pool) and, when the batch cannot run fused, why (else "").
  * qem_batch_set_thermostat: the Andersen thermostat of the MD steps (Molly's
  *   AndersenThermostat(temp, coupling_const) in test/QEM_test.jl:53-56;
  *   python_lib Andersen.py:8-22): after each step every particle, with
@@ -353,6 +385,12 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
                               void *stream, int32_t *width, double *ms_per_eval);
 qem_status qem_batch_set_thermostat(qem_batch *b, double kT, double nu, uint64_t seed);
 qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step);
+#define QEM_BATCH_AUTO 0
+#define QEM_BATCH_FUSED 1
+#define QEM_BATCH_POOL 2
+qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order);
+qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *launches,
+                              const char **why);
 
 /* Library identity (version string and the compiled CUDA architecture). */
 const char *qem_version(void);

@@ -24,6 +24,7 @@ QEM_PYTHON_MODE = QEM_CUTOFF_PYTHON | QEM_DIR_MINIMAGE | QEM_PAIR_PHYSICAL
 QEM_FP64, QEM_FP32_FIX = 0, 1
 QEM_TERM_SHORT, QEM_TERM_LONG, QEM_TERM_LJ, QEM_TERM_ALL = 0x1, 0x2, 0x4, 0x7
 QEM_MEM_HOST, QEM_MEM_DEVICE = 0, 1
+QEM_BATCH_AUTO, QEM_BATCH_FUSED, QEM_BATCH_POOL = 0, 1, 2
 QEM_NOALLOC_MAX_N, QEM_NOALLOC_MAX_P = 32768, 512
 QEM_MAX_KSET = 1048560
 
@@ -115,6 +116,8 @@ def load(build: bool = False):
         "qem_batch_md": (C.c_int32, [vp, C.c_int32, C.c_double, vp, vp, vp, vp, C.c_uint32, vp]),
         "qem_batch_autotune": (C.c_int32, [vp, vp, vp, vp, C.c_uint32, vp, ip, dp]),
         "qem_batch_set_thermostat": (C.c_int32, [vp, C.c_double, C.c_double, C.c_uint64]),
+        "qem_batch_set_mode": (C.c_int32, [vp, C.c_int32, C.c_int32, C.c_int32]),
+        "qem_batch_get_mode": (C.c_int32, [vp, ip, ip, ip, ip, C.POINTER(C.c_char_p)]),
         "qem_batch_thermostat_step": (C.c_int32, [vp, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():

@@ -413,12 +413,28 @@ class Batch:
         return n.value
 
     def autotune(self, xyz, q, F, terms=L.QEM_TERM_ALL, stream=None):
-        """Chooses the stream-pool width; returns (width, ms per batch evaluation)."""
+        """Times the stream-pool widths and the fused tilings and keeps the fastest;
+        returns (pool width or 0 for the fused phases, ms per batch evaluation)."""
         w = C.c_int32()
         ms = C.c_double()
         self._check(self._lib.qem_batch_autotune(self._b, self._ptr(xyz), self._ptr(q), self._ptr(F), int(terms),
                                                  self._stream(xyz, stream), C.byref(w), C.byref(ms)))
         return w.value, ms.value
+
+    def set_mode(self, mode=L.QEM_BATCH_AUTO, ks=0, order=0):
+        """QEM_BATCH_AUTO / _FUSED / _POOL; ks: k-slices per system of the fused force
+        pass (0: each engine's own); order: 0 batch order, 1 largest system first."""
+        self._check(self._lib.qem_batch_set_mode(self._b, int(mode), int(ks), int(order)))
+
+    def mode(self):
+        """dict(mode, ks, order, launches, why) of the way evaluations run now."""
+        m, ks, order, n = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        why = C.c_char_p()
+        self._check(self._lib.qem_batch_get_mode(self._b, C.byref(m), C.byref(ks), C.byref(order), C.byref(n),
+                                                 C.byref(why)))
+        name = {L.QEM_BATCH_FUSED: "fused", L.QEM_BATCH_POOL: "pool"}.get(m.value, m.value)
+        return dict(mode=name, ks=ks.value, order=order.value, launches=n.value,
+                    why=(why.value or b"").decode())
 
 
 def forces(inter, sys, neighbors=None):

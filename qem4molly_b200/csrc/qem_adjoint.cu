@@ -4,12 +4,16 @@
 // For L = gE * E + sum_i gF_i . F_i the pass returns dL/dr_i, dL/dq_i and
 // dL/d(gamma_down, gamma_up).  Each unordered pair's contributions
 // (Force_short.jl:25-78 forces, Energy_short_range_njit.py:34-63 energy) are
-// a function of (dx, dy, z_i, z_j, gamma_down, gamma_up) times q_i q_j: the
-// pair kernel evaluates them in FP64 on Dual<6> numbers, which gives the
-// exact Jacobian of the discretised pair terms (the quadrature limits of the
-// Julia cutoff mode move with the image distances, and that dependence is
-// included), and contracts it with the pair's cotangents
-//   (gF_i - gF_j).(F_x, F_y) + gF_i,z F_z,i + gF_j,z F_z,j + gE U_ij.
+// a function of (dx, dy, z_i, z_j, gamma_down, gamma_up) times q_i q_j.  The
+// pair kernel contracts them with the pair's cotangents
+//   (gF_i - gF_j).(F_x, F_y) + gF_i,z F_z,i + gF_j,z F_z,j + gE U_ij
+// and returns the exact FP64 gradient of that contraction for the
+// discretised pair terms (the quadrature limits of the Julia cutoff mode
+// move with the image distances, and that dependence is included): the
+// contraction is linear in the interval integrals, so one scalar walk over
+// an interval's nodes gives its value and its partials with respect to the
+// limit, exponent, prefactor, g12 and rho, and only the few closed-form
+// terms around the quadrature run on Dual<6> numbers.
 // It writes one record per pair in the forward pass's (owner, other) layout;
 // a per-particle pass sums a particle's own and incoming records in a fixed
 // order, adds the self term (Force_short.jl:82-107, on Dual<3> numbers in
@@ -21,6 +25,10 @@
 namespace {
 
 constexpr int ADJ_BLOCK = 128;
+// resident blocks per SM the pair adjoint is compiled for (register cap)
+#ifndef QEM_ADJ_MINB
+#define QEM_ADJ_MINB 4
+#endif
 
 template <class T>
 __device__ __forceinline__ T point_limit_t(const ShortConsts &c, const T &a)
@@ -63,67 +71,60 @@ __device__ void quad_t(const ShortConsts &c, const T &K, const T &ae, double c2,
     Ir = r; Iz = z; Iu = u;
 }
 
-// unit-charge pair terms of F_short_ij (Force_short.jl:25-78) and the pair
-// energy, in the canonical orientation (i the lower index)
-template <class T>
-__device__ void pair_terms(const ShortConsts &c, const T &dx, const T &dy, const T &dxr, const T &dyr,
-                           const T &zi, const T &zj, const T &g1, const T &g2, T &Fx, T &Fy, T &Fz_i, T &Fz_j,
-                           T &U)
+// One interval of the pair quadrature, contracted with the loss: with
+//   G(k) = pf e^{-k (ae + k c2)} / (1 - g12 e^{-2 Lz k}),
+//   Ir = sum w k G J1(k rho),  Iz = sum w k G J0(k rho),  Iu = sum w G J0(k rho)
+// over the nodes k = h (1 + x_n), weights h w_n, h = K / 2 (the forward
+// pass's nodes and integrand), returns S = cr Ir + cz Iz + cu Iu, the value
+// of Ir, and the partials of S with respect to K, ae, pf, g12 and rho, all
+// from one walk over the nodes in scalar FP64.  Writing T = G Phi with
+// Phi = k (cr J1 + cz J0) + cu J0:
+//   dS/dpf = S / pf,  dS/dae = -sum h w k T,  dS/dg12 = sum h w T e / D,
+//   dS/drho = sum h w G dPhi/drho,
+//   dS/dK = (S + sum h w k dT/dk) / K        (the nodes scale with K)
+// with k dPhi/dk = k (J0 (cz + k rho cr) - rho J1 (k cz + cu)),
+//      dPhi/drho = k (cr k (J0 - J1(x)/x) - (k cz + cu) J1),  x = k rho,
+//      k d ln G / dk = -(k ae + 2 k^2 c2) - 2 Lz k g12 e / D,  e = e^{-2 Lz k}.
+struct QAdj {
+    double S, R, dK, dae, dpf, dg12, drho;
+};
+
+__device__ __forceinline__ QAdj quad_adj(const ShortConsts &c, double K, double ae, double c2, double pf,
+                                         double g12, double rho, double cr, double cz, double cu)
 {
-    const T rho2 = dx * dx + dy * dy;
-    const T rho = sqrt(rho2);
-    const T zn = fabs(zi - zj), zp = zi + zj;
-    const double s = jl_sign(dval(zi) - dval(zj));
-    const T g12 = g1 * g2;
-    T zero = rho * 0.0;
-    T Fr = zero, Fzi = zero, Fzj = zero, Uq = zero, Fp2 = zero, Fz2i = zero, Fz2j = zero, Ub = zero;
-    for (int iv = 0; iv < 8; iv++) {
-        const int l = iv >> 1;
-        const bool gauss = (iv & 1) != 0;
-        const T a = (l == 0) ? zn : (l == 1) ? zp : (l == 2) ? c.twoLz - zp : c.twoLz - zn;
-        const T b = (l == 0) ? zero + 1.0 : (l == 1) ? g1 : (l == 2) ? g2 : g12;
-        const double si = (l == 0) ? -s : (l == 1) ? -1.0 : (l == 2) ? 1.0 : s;
-        const double sj = (l == 1 || l == 2) ? si : -si;
-        T K, ae, pf;
-        double c2;
-        if (gauss) {
-            K = gauss_limit_t(c, a);
-            ae = a;
-            c2 = c.inv4alpha;
-            pf = -0.5 * b;
-        } else {
-            K = point_limit_t(c, a);
-            ae = a + c.twoLz;
-            c2 = 0.0;
-            pf = -0.5 * b * g12;
-        }
-        T Ir, Iz, Iu;
-        quad_t<T, true>(c, K, ae, c2, pf, g12, rho, Ir, Iz, Iu);
-        const double sf = gauss ? 1.0 : -1.0;
-        Fr += sf * Ir;
-        Fzi -= (sf * si) * Iz;
-        Fzj -= (sf * sj) * Iz;
-        Uq += sf * Iu;
-        if (!gauss) {
-            const T r2 = a * a + rho2;
-            const T inv15 = 1.0 / (r2 * sqrt(r2));
-            Fp2 += b * rho * inv15;
-            Fz2i += si * (b * a * inv15);
-            Fz2j += sj * (b * a * inv15);
-            Ub += 0.5 * b / sqrt(r2);
-        }
+    const double h = 0.5 * K;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0, bk = 0, r = 0;
+    for (int n = 0; n < c.Nt; n++) {
+        const double k = h * (1.0 + c.xd[n]);
+        const double e = exp(k * (-c.twoLz));
+        const double Di = 1.0 / (1.0 - g12 * e);
+        const double wH = (h * c.wd[n]) * exp(-(k * (ae + k * c2))) * Di;
+        const double x = k * rho;
+        double J0, J1;
+        bessel01(x, J0, J1);
+        const double j1x = x != 0.0 ? J1 / x : 0.5;
+        const double kzu = k * cz + cu;
+        const double Phi = k * (cr * J1 + cz * J0) + cu * J0;
+        const double Phr = k * (cr * k * (J0 - j1x) - kzu * J1);
+        const double kPk = k * (J0 * (cz + x * cr) - rho * J1 * kzu);
+        const double t = e * Di;
+        const double wHP = wH * Phi;
+        a0 += wHP;
+        a1 += wHP * k;
+        a2 += wHP * t;
+        a3 += wH * Phr;
+        bk += wH * (kPk - Phi * (k * (ae + 2.0 * k * c2) + c.twoLz * k * g12 * t));
+        r += wH * k * J1;
     }
-    Fx = zero;
-    Fy = zero;
-    if (dval(rho) != 0.0) {
-        const T Fsr = Fr + 0.5 * Fp2;
-        const bool mi = (c.flags & QEM_DIR_MINIMAGE) != 0;
-        Fx = c.pref * Fsr * (mi ? dx : dxr) / rho;
-        Fy = c.pref * Fsr * (mi ? dy : dyr) / rho;
-    }
-    Fz_i = c.pref * (Fzi - 0.5 * Fz2i);
-    Fz_j = (c.flags & QEM_PAIR_PHYSICAL) ? c.pref * (Fzj - 0.5 * Fz2j) : -Fz_i;
-    U = c.pref * (Uq + Ub);
+    QAdj q;
+    q.S = pf * a0;
+    q.R = pf * r;
+    q.dpf = a0;
+    q.dae = -pf * a1;
+    q.dg12 = pf * a2;
+    q.drho = pf * a3;
+    q.dK = K > 0.0 ? pf * (a0 + bk) / K : 0.0;
+    return q;
 }
 
 __device__ __forceinline__ double3 load_g(const double *gF, int i)
@@ -134,7 +135,16 @@ __device__ __forceinline__ double3 load_g(const double *gF, int i)
 
 // records: RA[2p] = (dL/dx, dL/dy, dL/dz of the owner, dL/dz of the other),
 //          RA[2p+1] = (dL/dq owner, dL/dq other, dL/dgamma_down, dL/dgamma_up)
-__global__ void __launch_bounds__(ADJ_BLOCK) k_short_pair_adj(const int64_t *__restrict__ np, int64_t cap,
+//
+// The unit-charge pair terms (Force_short.jl:25-78, canonical orientation,
+// i the lower index) enter the loss linearly through the interval integrals:
+//   L~ = C Fsr + sum_iv (cz Iz + cu Iu) + closed-form image terms,
+//   Fsr = sum_iv sf Ir + Fp2 / 2,  C = pref (gdx dir_x + gdy dir_y) / rho,
+// gdx = gF_i,x - gF_j,x.  Each interval's cotangents (cr = sf C, cz, cu) are
+// known before its quadrature, so quad_adj returns the interval's share of
+// L~ and its partials; the limits, image distances, closed-form terms and C
+// are carried on Dual<6> numbers in (dx, dy, z_i, z_j, gamma_down, gamma_up).
+__global__ void __launch_bounds__(ADJ_BLOCK, QEM_ADJ_MINB) k_short_pair_adj(const int64_t *__restrict__ np, int64_t cap,
                                                                const int2 *__restrict__ pairs,
                                                                const double4 *__restrict__ pos,
                                                                const double *__restrict__ gF, double gE,
@@ -155,13 +165,68 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_short_pair_adj(const int64_t *__r
         RA[2 * p + 1] = make_double4(0, 0, 0, 0);
         return;
     }
-    // tangents: 0 dx, 1 dy, 2 z_i, 3 z_j, 4 gamma_down, 5 gamma_up
-    const D6 dx = dvar<6>(dxm, 0), dy = dvar<6>(dym, 1), dxr_ = dvar<6>(dxr, 0), dyr_ = dvar<6>(dyr, 1);
-    const D6 zi = dvar<6>(pi.z, 2), zj = dvar<6>(pj.z, 3), g1 = dvar<6>(c.g1, 4), g2 = dvar<6>(c.g2, 5);
-    D6 Fx, Fy, Fzi, Fzj, U;
-    pair_terms<D6>(c, dx, dy, dxr_, dyr_, zi, zj, g1, g2, Fx, Fy, Fzi, Fzj, U);
     const double3 gi = load_g(gF, i), gj = load_g(gF, j);
-    const D6 L = (gi.x - gj.x) * Fx + (gi.y - gj.y) * Fy + gi.z * Fzi + gj.z * Fzj + gE * U;
+    const bool phys = (c.flags & QEM_PAIR_PHYSICAL) != 0, mi = (c.flags & QEM_DIR_MINIMAGE) != 0;
+    const bool python = (c.flags & QEM_CUTOFF_PYTHON) != 0;
+    // tangents: 0 dx, 1 dy, 2 z_i, 3 z_j, 4 gamma_down, 5 gamma_up
+    const D6 dx = dvar<6>(dxm, 0), dy = dvar<6>(dym, 1);
+    const D6 zi = dvar<6>(pi.z, 2), zj = dvar<6>(pj.z, 3), g1 = dvar<6>(c.g1, 4), g2 = dvar<6>(c.g2, 5);
+    const D6 rho2 = dx * dx + dy * dy;
+    const D6 rho = sqrt(rho2);
+    const D6 zn = fabs(zi - zj), zp = zi + zj;
+    const double s = jl_sign(pi.z - pj.z);
+    const D6 g12 = g1 * g2;
+    const D6 zero = dconst<6>(0.0);
+    D6 C = zero;
+    if (rho.v != 0.0) {
+        const D6 ux = mi ? dx : dvar<6>(dxr, 0), uy = mi ? dy : dvar<6>(dyr, 1);
+        C = c.pref * ((gi.x - gj.x) * ux + (gi.y - gj.y) * uy) / rho;
+    }
+    D6 L = zero, Fp2 = zero, Fz2 = zero, Ub = zero;
+    double Fq = 0.0;
+    for (int iv = 0; iv < 8; iv++) {
+        const int l = iv >> 1;
+        const bool gauss = (iv & 1) != 0;
+        const D6 a = (l == 0) ? zn : (l == 1) ? zp : (l == 2) ? c.twoLz - zp : c.twoLz - zn;
+        const D6 b = (l == 0) ? zero + 1.0 : (l == 1) ? g1 : (l == 2) ? g2 : g12;
+        const double si = (l == 0) ? -s : (l == 1) ? -1.0 : (l == 2) ? 1.0 : s;
+        const double sj = (l == 1 || l == 2) ? si : -si;
+        const double sf = gauss ? 1.0 : -1.0;
+        // limit K(a) and dK/da (constant limits in the python cutoff mode)
+        double K, Kp;
+        if (gauss) {
+            K = python ? c.kf_gauss_py : c.neg_lnacc / (a.v + c.twoLz);
+            Kp = python ? 0.0 : -K / (a.v + c.twoLz);
+        } else if (python) {
+            K = c.kf_point_py;
+            Kp = 0.0;
+        } else {
+            const double sq = ::sqrt(4.0 * c.alpha * c.alpha * (a.v * a.v) + 4.0 * c.alpha * c.neg_lnacc);
+            K = sq - 2.0 * c.alpha * a.v;
+            Kp = 4.0 * c.alpha * c.alpha * a.v / sq - 2.0 * c.alpha;
+        }
+        const double ae = gauss ? a.v : a.v + c.twoLz, c2 = gauss ? c.inv4alpha : 0.0;
+        const double pfb = gauss ? -0.5 : -0.5 * g12.v;  // pf = pfb b
+        const double cz = phys ? -sf * c.pref * (si * gi.z + sj * gj.z) : -sf * si * c.pref * (gi.z - gj.z);
+        const QAdj q = quad_adj(c, K, ae, c2, pfb * b.v, g12.v, rho.v, sf * C.v, cz, sf * c.pref * gE);
+        const double dSa = q.dK * Kp + q.dae, dSb = q.dpf * pfb;
+        const double dSg = q.dg12 + (gauss ? 0.0 : -0.5 * b.v * q.dpf);
+        L.v += q.S;
+#pragma unroll
+        for (int t = 0; t < 6; t++) L.d[t] += dSa * a.d[t] + dSb * b.d[t] + dSg * g12.d[t] + q.drho * rho.d[t];
+        Fq += sf * q.R;
+        if (!gauss) {
+            const D6 r2 = a * a + rho2;
+            const D6 inv15 = 1.0 / (r2 * sqrt(r2));
+            Fp2 += b * rho * inv15;
+            Fz2 += (phys ? si * gi.z + sj * gj.z : si * (gi.z - gj.z)) * (b * a * inv15);
+            Ub += 0.5 * b / sqrt(r2);
+        }
+    }
+    // C Fsr: the quadrature part's value and dFq are in L already (cr = sf C.v)
+#pragma unroll
+    for (int t = 0; t < 6; t++) L.d[t] += Fq * C.d[t];
+    L += C * (0.5 * Fp2) + (-0.5 * c.pref) * Fz2 + (gE * c.pref) * Ub;
     const double qq = pi.w * pj.w;
     // dL/d(input) = q_i q_j dL~/d(input); dL/dq_i = q_j L~, dL/dq_j = q_i L~
     const double gdx = qq * L.d[0], gdy = qq * L.d[1], gzi = qq * L.d[2], gzj = qq * L.d[3];

@@ -1,14 +1,24 @@
-// qem_batch.cu -- batches of independent systems: asynchronous batched force
-// evaluation on a pool of streams, a velocity-Verlet step recorded once as a
-// CUDA graph and replayed, and an autotuner for the stream-pool width.
+// qem_batch.cu -- batches of independent systems: batched force evaluation,
+// a velocity-Verlet step recorded once as a CUDA graph and replayed, and an
+// autotuner for the phase tiling.
 //
 // Reference: the MD setups of test/QEM_test.jl:40-60 (Molly VelocityVerlet
 // over QEM_short + QEM_long + Substrate_LJ) run one system at a time; the
 // batch runs many small slabs together.  Each system keeps its own handle
-// (parameters, k-set, neighbour list); the systems' kernels are small (a few
-// thousand particles), so the batch's speed comes from running their
-// pipelines concurrently and from replaying one recorded graph per MD step
-// instead of issuing some forty launches per system from the host.
+// (parameters, k-set, neighbour list, device buffers).
+//
+// Two ways to run a batch evaluation:
+//  * fused phases (every system small enough for the one-block kernels, in
+//    FP32+fix): eight launches for the whole batch.  One block per system
+//    packs, bins, lists pairs and z-sorts; then the pair phase and, on a
+//    second stream, the long-range phases (preparation, chunk totals, their
+//    scan, the k-sliced force pass, the final sum) each run one launch over a
+//    (system, tile) work list; the gather joins them.  The blocks run the
+//    single-system kernels' per-block code on the system's own buffers, so a
+//    system's forces are those of its own qem_forces call.
+//  * per-system pipelines forked over a pool of streams (any batch).
+// The autotuner times the pool widths and the fused tilings (k-slices per
+// system of the force pass, work-list order) and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -102,6 +112,23 @@ struct qem_batch {
     double therm_kT = 0, therm_nu = 0;
     uint64_t therm_seed = 0;
     unsigned long long *therm_step = nullptr;  // device step counter of the random draws
+    // fused phases
+    int mode_req = QEM_BATCH_AUTO;      // requested: auto, fused or pool
+    int mode_cur = QEM_BATCH_FUSED;     // in use when the request is auto (the autotuner's choice)
+    int fks = 0;                        // k-slices per system of the fused force pass (0: each handle's own)
+    int forder = 0;                     // work-list order: 0 batch order, 1 largest system first
+    bool ftab_ok = false;               // device tables built for the current buffers and terms
+    std::string fwhy;                   // why the batch cannot run fused (empty: it can)
+    std::vector<uint64_t> fstate;       // per-handle state the tables were built for
+    uint32_t fterms = 0;
+    int do_lj = 0;
+    BatchSys *d_sys = nullptr;
+    ShortConsts *d_sc = nullptr;
+    BatchWork *d_work = nullptr;
+    size_t work_cap = 0;
+    int nw[5] = {0, 0, 0, 0, 0}, wo[5] = {0, 0, 0, 0, 0};  // pairs, particle tiles, totals, scan, force pass
+    cudaStream_t s_long = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
 };
 
@@ -117,10 +144,121 @@ static qem_status bfail(qem_batch *b, qem_status s, const std::string &m)
         if (e_ != cudaSuccess) return bfail(b, QEM_ERR_CUDA, std::string(#call) + " -> " + cudaGetErrorString(e_)); \
     } while (0)
 
-// enqueue every system's evaluation on the pool, forked from and joined to s
+static bool fused_current(const qem_batch *b, uint32_t terms)
+{
+    if (!b->ftab_ok || b->fterms != terms) return false;
+    for (int i = 0; i < b->B; i++)
+        if (qem_handle_state(b->h[i]) != b->fstate[i]) return false;
+    return true;
+}
+
+static bool use_fused(const qem_batch *b)
+{
+    if (b->mode_req == QEM_BATCH_POOL || !b->fwhy.empty()) return false;
+    return b->mode_req == QEM_BATCH_FUSED || b->mode_cur == QEM_BATCH_FUSED;
+}
+
+// Device tables of the fused phases from the handles' buffers (after their
+// synchronous calls); outside any stream capture.  A system that does not
+// qualify leaves the reason in fwhy and the batch on the stream pool.
+static qem_status build_fused(qem_batch *b, uint32_t terms)
+{
+    b->ftab_ok = false;
+    b->fwhy.clear();
+    if ((terms & (QEM_TERM_SHORT | QEM_TERM_LONG)) != (QEM_TERM_SHORT | QEM_TERM_LONG)) {
+        b->fwhy = "terms without both the short and the long range";
+        return QEM_OK;
+    }
+    std::vector<BatchSys> sys(b->B);
+    std::vector<ShortConsts> sc(b->B);
+    for (int i = 0; i < b->B; i++) {
+        const char *why = nullptr;
+        const qem_status st = qem_handle_batch_sys(b->h[i], b->N[i], b->fks, &sys[i], &sc[i], &why);
+        if (st == QEM_ERR_ARG && why) {
+            b->fwhy = "system " + std::to_string(i) + ": " + why;
+            return QEM_OK;
+        }
+        if (st != QEM_OK) return bfail(b, st, "system " + std::to_string(i) + ": " + qem_handle_error(b->h[i]));
+        sys[i].off = b->off[i];
+    }
+    std::vector<int> order(b->B);
+    for (int i = 0; i < b->B; i++) order[i] = i;
+    if (b->forder == 1)
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->N[x] > b->N[y]; });
+    auto nblk = [](int64_t n, int t) { return (int)((n + t - 1) / t); };
+    std::vector<BatchWork> w;
+    const int tp = qem_batch_pair_tile(), tpart = qem_batch_particle_tile(), tt = qem_batch_ltot_tile();
+    const int ts = qem_batch_lscan_tile(), tf = qem_batch_lforce_tile();
+    for (int ph = 0; ph < 5; ph++) {
+        b->wo[ph] = (int)w.size();
+        for (int s : order) {
+            const BatchSys &d = sys[s];
+            if (ph == 0)
+                for (int t = 0; t < nblk(d.cap, tp); t++) w.push_back({s, t, 0, 0});
+            if (ph == 1)
+                for (int t = 0; t < nblk(d.N, tpart); t++) w.push_back({s, t, 0, 0});
+            if (ph == 2 && d.P > 0)
+                for (int c = 0; c < d.nch; c++)
+                    for (int kb = 0; kb < nblk(d.P, tt); kb++) w.push_back({s, c, kb, 0});
+            if (ph == 3 && d.P > 0)
+                for (int t = 0; t < nblk(d.P, ts); t++) w.push_back({s, t, 0, 0});
+            if (ph == 4)  // also with P = 0: the force pass writes the zero slices the final pass sums
+                for (int c = 0; c < d.nch; c++)
+                    for (int y = 0; y < nblk(d.ks, tf); y++) w.push_back({s, c, y, 0});
+        }
+        b->nw[ph] = (int)w.size() - b->wo[ph];
+    }
+    if (!b->d_sys) {
+        BCU(cudaMalloc(&b->d_sys, sizeof(BatchSys) * b->B));
+        BCU(cudaMalloc(&b->d_sc, sizeof(ShortConsts) * b->B));
+    }
+    if (w.size() > b->work_cap) {
+        if (b->d_work) BCU(cudaFree(b->d_work));
+        b->d_work = nullptr;
+        b->work_cap = w.size() + w.size() / 4;
+        BCU(cudaMalloc(&b->d_work, sizeof(BatchWork) * b->work_cap));
+    }
+    BCU(cudaDeviceSynchronize());  // no recorded evaluation may still read the tables
+    BCU(cudaMemcpy(b->d_sys, sys.data(), sizeof(BatchSys) * b->B, cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_sc, sc.data(), sizeof(ShortConsts) * b->B, cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_work, w.data(), sizeof(BatchWork) * w.size(), cudaMemcpyHostToDevice));
+    b->fstate.resize(b->B);
+    for (int i = 0; i < b->B; i++) b->fstate[i] = qem_handle_state(b->h[i]);
+    b->fterms = terms;
+    b->do_lj = (terms & QEM_TERM_LJ) ? 1 : 0;
+    b->ftab_ok = true;
+    return QEM_OK;
+}
+
+// the fused phases (tables current), forked from and joined to s
+static qem_status enqueue_fused(qem_batch *b, const double *xyz, const double *q, double *F, cudaStream_t s)
+{
+    const BatchWork *w = b->d_work;
+    BCU(qem_launch_batch_setup(b->B, b->d_sys, xyz, q, s));
+    BCU(cudaEventRecord(b->ev_fork, s));
+    BCU(cudaStreamWaitEvent(b->s_long, b->ev_fork, 0));
+    BCU(qem_launch_batch_lprep(b->B, b->d_sys, b->s_long));
+    BCU(qem_launch_batch_ltot(b->nw[2], w + b->wo[2], b->d_sys, b->s_long));
+    BCU(qem_launch_batch_lscan(b->nw[3], w + b->wo[3], b->d_sys, b->s_long));
+    BCU(qem_launch_batch_lforce(b->nw[4], w + b->wo[4], b->d_sys, b->s_long));
+    BCU(qem_launch_batch_lfinal(b->nw[1], w + b->wo[1], b->d_sys, b->s_long));
+    BCU(cudaEventRecord(b->ev_join, b->s_long));
+    BCU(qem_launch_batch_pairs(b->nw[0], w + b->wo[0], b->d_sys, b->d_sc, s));
+    BCU(cudaStreamWaitEvent(s, b->ev_join, 0));
+    BCU(qem_launch_batch_gather(b->nw[1], w + b->wo[1], b->d_sys, b->d_sc, b->do_lj, F, s));
+    return QEM_OK;
+}
+
+// every system's evaluation: the fused phases when their tables are current,
+// else the per-system pipelines on the pool, forked from and joined to s
 static qem_status enqueue_forces(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
                                  cudaStream_t s)
 {
+    if (use_fused(b)) {
+        if (!fused_current(b, terms))
+            return bfail(b, QEM_ERR_ARG, "fused batch tables out of date (a synchronous batch call first)");
+        return enqueue_fused(b, xyz, q, F, s);
+    }
     BCU(cudaEventRecord(b->ev_start, s));
     for (int w = 0; w < b->W; w++) BCU(cudaStreamWaitEvent(b->pool[w], b->ev_start, 0));
     for (int i = 0; i < b->B; i++) {
@@ -179,6 +317,11 @@ qem_status qem_batch_create(int32_t B, qem_handle *const *handles, const int32_t
     const int np = std::min(B, 128);
     bool ok = cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) == cudaSuccess;
+    int prio_lo = 0, prio_hi = 0;
+    ok = ok && cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithPriority(&b->s_long, cudaStreamNonBlocking, prio_hi) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess;
     for (int w = 0; ok && w < np; w++) {
         cudaStream_t s;
         cudaEvent_t e;
@@ -224,6 +367,15 @@ void qem_batch_destroy(qem_batch *b)
     if (b->box) cudaFree(b->box);
     if (b->Fn) cudaFree(b->Fn);
     if (b->therm_step) cudaFree(b->therm_step);
+    if (b->s_long) {
+        cudaStreamSynchronize(b->s_long);
+        cudaStreamDestroy(b->s_long);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->d_sys) cudaFree(b->d_sys);
+    if (b->d_sc) cudaFree(b->d_sc);
+    if (b->d_work) cudaFree(b->d_work);
     delete b;
 }
 
@@ -246,8 +398,14 @@ qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, do
         b->warm = true;
         b->warm_terms = terms;
         drop_md_graph(b);
-        return QEM_OK;
+        return b->mode_req == QEM_BATCH_POOL ? QEM_OK : build_fused(b, terms);
     }
+    if (use_fused(b) && !fused_current(b, terms)) {
+        drop_md_graph(b);
+        const qem_status st = build_fused(b, terms);
+        if (st != QEM_OK) return st;
+    }
+    if (b->mode_req == QEM_BATCH_FUSED && !b->fwhy.empty()) return bfail(b, QEM_ERR_ARG, "fused batch: " + b->fwhy);
     return enqueue_forces(b, xyz, q, F, terms, s);
 }
 
@@ -259,6 +417,11 @@ qem_status qem_batch_check(qem_batch *b, void *stream)
     BCU(cudaStreamSynchronize(s));
     for (int i = 0; i < b->B; i++) {
         const qem_status st = qem_status_check(b->h[i], s);
+        if (st == QEM_ERR_NB_OVERFLOW) {  // the next batch call re-sizes every system synchronously
+            b->warm = false;
+            b->ftab_ok = false;
+            drop_md_graph(b);
+        }
         if (st != QEM_OK) return bfail(b, st, "system " + std::to_string(i) + ": " + qem_handle_error(b->h[i]));
     }
     b->err.clear();
@@ -346,6 +509,37 @@ qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step)
     return QEM_OK;
 }
 
+// one batch evaluation recorded as a graph and replayed reps times on s
+// (after one warm-up replay): milliseconds per evaluation
+static qem_status time_graph(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
+                             cudaStream_t s, cudaEvent_t t0, cudaEvent_t t1, float &ms)
+{
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    BCU(cudaStreamSynchronize(s));
+    BCU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const qem_status st = enqueue_forces(b, xyz, q, F, terms, b->cap);
+    const cudaError_t ec = cudaStreamEndCapture(b->cap, &g);
+    if (st != QEM_OK || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return st != QEM_OK ? st : bfail(b, QEM_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ec));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return bfail(b, QEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    const int reps = 5;
+    cudaError_t e = cudaGraphLaunch(ex, s);
+    e = e == cudaSuccess ? cudaEventRecord(t0, s) : e;
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(ex, s);
+    e = e == cudaSuccess ? cudaEventRecord(t1, s) : e;
+    e = e == cudaSuccess ? cudaEventSynchronize(t1) : e;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+    cudaGraphExecDestroy(ex);
+    if (e != cudaSuccess) return bfail(b, QEM_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(e));
+    ms /= reps;
+    return QEM_OK;
+}
+
 qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
                               void *stream, int32_t *width, double *ms_per_eval)
 {
@@ -354,67 +548,103 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
     cudaStream_t s = (cudaStream_t)stream;
     qem_status st = qem_batch_forces(b, xyz, q, F, terms, s);
     if (st != QEM_OK) return st;
-    const int wmax = (int)b->pool.size();
-    std::vector<int> cand;
-    for (int w = 1; w < wmax; w *= 2) cand.push_back(w);
-    cand.push_back(wmax);
+    // candidates: pool widths 1, 2, 4, ..; fused tilings: k-slices per system
+    // of the force pass (the handle's own count, or at most 1, 2, 4) x
+    // work-list order (batch order, largest system first)
+    struct Cand {
+        int fused, w, ks, order;
+    };
+    std::vector<Cand> cand;
+    if (b->mode_req != QEM_BATCH_FUSED) {
+        const int wmax = (int)b->pool.size();
+        for (int w = 1; w < wmax; w *= 2) cand.push_back({0, w, 0, 0});
+        cand.push_back({0, wmax, 0, 0});
+    }
+    const bool fusable = b->mode_req != QEM_BATCH_POOL && b->fwhy.empty();
+    if (fusable)
+        for (int ks : {0, 1, 2, 4})
+            for (int order : {0, 1}) cand.push_back({1, 0, ks, order});
+    const int mode0 = b->mode_req, W0 = b->W, ks0 = b->fks, order0 = b->forder;
     cudaEvent_t t0, t1;
     BCU(cudaEventCreate(&t0));
     BCU(cudaEventCreate(&t1));
-    int best_w = b->W;
-    float best = 1e30f;
-    const int W0 = b->W;
-    for (int w : cand) {
-        b->W = w;
-        cudaGraph_t g = nullptr;
-        cudaGraphExec_t ex = nullptr;
-        BCU(cudaStreamSynchronize(s));
-        BCU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-        st = enqueue_forces(b, xyz, q, F, terms, b->cap);
-        const cudaError_t ec = cudaStreamEndCapture(b->cap, &g);
-        if (st != QEM_OK || ec != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            b->W = W0;
-            cudaEventDestroy(t0);
-            cudaEventDestroy(t1);
-            return st != QEM_OK ? st : bfail(b, QEM_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ec));
+    int best = -1;
+    float best_ms = 1e30f;
+    for (int c = 0; c < (int)cand.size() && st == QEM_OK; c++) {
+        const Cand &k = cand[c];
+        b->mode_req = k.fused ? QEM_BATCH_FUSED : QEM_BATCH_POOL;
+        if (k.fused) {
+            b->fks = k.ks;
+            b->forder = k.order;
+            st = build_fused(b, terms);
+        } else {
+            b->W = k.w;
         }
-        const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
-        cudaGraphDestroy(g);
-        if (ei != cudaSuccess) {
-            b->W = W0;
-            cudaEventDestroy(t0);
-            cudaEventDestroy(t1);
-            return bfail(b, QEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
-        }
-        const int reps = 5;
-        cudaError_t e = cudaGraphLaunch(ex, s);  // warm-up
-        e = e == cudaSuccess ? cudaEventRecord(t0, s) : e;
-        for (int r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(ex, s);
-        e = e == cudaSuccess ? cudaEventRecord(t1, s) : e;
-        e = e == cudaSuccess ? cudaEventSynchronize(t1) : e;
         float ms = 0;
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
-        cudaGraphExecDestroy(ex);
-        if (e != cudaSuccess) {
-            b->W = W0;
-            cudaEventDestroy(t0);
-            cudaEventDestroy(t1);
-            return bfail(b, QEM_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(e));
-        }
-        ms /= reps;
-        if (ms < best) {
-            best = ms;
-            best_w = w;
+        if (st == QEM_OK) st = time_graph(b, xyz, q, F, terms, s, t0, t1, ms);
+        if (st == QEM_OK && ms < best_ms) {
+            best_ms = ms;
+            best = c;
         }
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    b->W = best_w;
+    b->mode_req = mode0;
+    b->W = W0;
+    b->fks = ks0;
+    b->forder = order0;
+    if (st == QEM_OK && best >= 0) {
+        const Cand &k = cand[best];
+        if (k.fused) {
+            b->fks = k.ks;
+            b->forder = k.order;
+            b->mode_cur = QEM_BATCH_FUSED;
+        } else {
+            b->W = k.w;
+            b->mode_cur = QEM_BATCH_POOL;
+        }
+    }
+    if (fusable) {
+        const qem_status sb = build_fused(b, terms);
+        if (st == QEM_OK) st = sb;
+    }
     drop_md_graph(b);
-    if (width) *width = best_w;
-    if (ms_per_eval) *ms_per_eval = best;
+    if (st != QEM_OK) return st;
+    if (width) *width = b->mode_cur == QEM_BATCH_FUSED ? 0 : b->W;
+    if (ms_per_eval) *ms_per_eval = best_ms;
     return qem_batch_check(b, stream);
+}
+
+qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order)
+{
+    if (!b) return QEM_ERR_ARG;
+    if (mode != QEM_BATCH_AUTO && mode != QEM_BATCH_FUSED && mode != QEM_BATCH_POOL)
+        return bfail(b, QEM_ERR_ARG, "mode must be QEM_BATCH_AUTO, QEM_BATCH_FUSED or QEM_BATCH_POOL");
+    if (ks < 0 || ks > QEM_LONG_MAX_KS || (order != 0 && order != 1))
+        return bfail(b, QEM_ERR_ARG, "ks must be in 0 .. 64 and order 0 or 1");
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaDeviceSynchronize());
+    b->mode_req = mode;
+    b->mode_cur = mode == QEM_BATCH_POOL ? QEM_BATCH_POOL : QEM_BATCH_FUSED;
+    b->fks = ks;
+    b->forder = order;
+    b->ftab_ok = false;  // rebuilt by the next qem_batch_forces
+    drop_md_graph(b);
+    b->err.clear();
+    return QEM_OK;
+}
+
+qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *launches,
+                              const char **why)
+{
+    if (!b) return QEM_ERR_ARG;
+    const bool fused = use_fused(b);
+    if (mode) *mode = fused ? QEM_BATCH_FUSED : QEM_BATCH_POOL;
+    if (ks) *ks = b->fks;
+    if (order) *order = b->forder;
+    if (launches) *launches = fused ? 8 : -1;
+    if (why) *why = b->fwhy.c_str();
+    return QEM_OK;
 }
 
 }  // extern "C"

@@ -19,11 +19,10 @@ constexpr int SCAN_BLOCK = 1024;
 // ---------------------------------------------------------------------------
 // pack: AoS coordinates + charges -> double4, 2-D cell index, finiteness check
 // ---------------------------------------------------------------------------
-__global__ void k_pack(int N, const double *__restrict__ xyz, const double *__restrict__ q, double4 *__restrict__ pos,
-                       int *__restrict__ cell, CellGeom g, unsigned *status)
+__device__ __forceinline__ void pack_one(int i, const double *__restrict__ xyz, const double *__restrict__ q,
+                                         double4 *__restrict__ pos, int *__restrict__ cell, const CellGeom &g,
+                                         unsigned *status)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
     double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2], qq = q[i];
     bool ok = isfinite(x) && isfinite(y) && isfinite(z) && isfinite(qq);
     if (!ok) {
@@ -37,6 +36,13 @@ __global__ void k_pack(int N, const double *__restrict__ xyz, const double *__re
     cx = min(max(cx, 0), g.ncx - 1);
     cy = min(max(cy, 0), g.ncy - 1);
     cell[i] = cx * g.ncy + cy;
+}
+
+__global__ void k_pack(int N, const double *__restrict__ xyz, const double *__restrict__ q, double4 *__restrict__ pos,
+                       int *__restrict__ cell, CellGeom g, unsigned *status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) pack_one(i, xyz, q, pos, cell, g, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -262,10 +268,10 @@ __global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__res
 // build (the order inside a cell does not depend on the scatter).
 constexpr int CELLS_SMALL = 8192;
 
-__global__ void __launch_bounds__(1024) k_cells_small(int N, int ncell, const int *__restrict__ cell,
-                                                      const double4 *__restrict__ pos, int *__restrict__ cstart,
-                                                      int *__restrict__ clist, int *__restrict__ pos_of,
-                                                      double4 *__restrict__ pos_c)
+__device__ __forceinline__ void cells_small_block(int N, int ncell, const int *__restrict__ cell,
+                                                  const double4 *__restrict__ pos, int *__restrict__ cstart,
+                                                  int *__restrict__ clist, int *__restrict__ pos_of,
+                                                  double4 *__restrict__ pos_c)
 {
     __shared__ int cnt[CELLS_SMALL];
     __shared__ int warp_tot[32];
@@ -319,6 +325,14 @@ __global__ void __launch_bounds__(1024) k_cells_small(int N, int ncell, const in
         pos_of[i] = s;
         pos_c[s] = pos[i];
     }
+}
+
+__global__ void __launch_bounds__(1024) k_cells_small(int N, int ncell, const int *__restrict__ cell,
+                                                      const double4 *__restrict__ pos, int *__restrict__ cstart,
+                                                      int *__restrict__ clist, int *__restrict__ pos_of,
+                                                      double4 *__restrict__ pos_c)
+{
+    cells_small_block(N, ncell, cell, pos, cstart, clist, pos_of, pos_c);
 }
 
 // ---------------------------------------------------------------------------
@@ -711,13 +725,13 @@ __device__ void block_scan_small(const TI *in, TO *out, int n, TO *warp_tot)
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__restrict__ pos_c,
-                                                      const int *__restrict__ cell, const int *__restrict__ cstart,
-                                                      const int *__restrict__ clist, CellGeom g, double rc2,
-                                                      int *__restrict__ pcount, int64_t *__restrict__ poff,
-                                                      int2 *__restrict__ pairs, int64_t cap, int *__restrict__ in_cnt,
-                                                      int *__restrict__ in_fill, int64_t *__restrict__ in_off,
-                                                      int *__restrict__ in_list, unsigned *status)
+__device__ __forceinline__ void pairs_small_block(int N, const double4 *__restrict__ pos_c,
+                                                  const int *__restrict__ cell, const int *__restrict__ cstart,
+                                                  const int *__restrict__ clist, const CellGeom &g, double rc2,
+                                                  int *__restrict__ pcount, int64_t *__restrict__ poff,
+                                                  int2 *__restrict__ pairs, int64_t cap, int *__restrict__ in_cnt,
+                                                  int *__restrict__ in_fill, int64_t *__restrict__ in_off,
+                                                  int *__restrict__ in_list, unsigned *status)
 {
     __shared__ int64_t warp_tot[32];
     const int tid = threadIdx.x;
@@ -739,6 +753,18 @@ __global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__re
     }
     __syncthreads();
     for (int i = tid; i < N; i += 1024) sort_incoming(i, in_off, in_list);
+}
+
+__global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__restrict__ pos_c,
+                                                      const int *__restrict__ cell, const int *__restrict__ cstart,
+                                                      const int *__restrict__ clist, CellGeom g, double rc2,
+                                                      int *__restrict__ pcount, int64_t *__restrict__ poff,
+                                                      int2 *__restrict__ pairs, int64_t cap, int *__restrict__ in_cnt,
+                                                      int *__restrict__ in_fill, int64_t *__restrict__ in_off,
+                                                      int *__restrict__ in_list, unsigned *status)
+{
+    pairs_small_block(N, pos_c, cell, cstart, clist, g, rc2, pcount, poff, pairs, cap, in_cnt, in_fill, in_off,
+                      in_list, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -787,11 +813,10 @@ __global__ void __launch_bounds__(ZTILE) k_ztile(int N, const double4 *__restric
 }
 
 template <bool REV>
-__global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
-                         double *__restrict__ key_out, int *__restrict__ idx_out)
+__device__ __forceinline__ void zmerge_one(int p, int N, int width, const double *__restrict__ key,
+                                           const int *__restrict__ idx, double *__restrict__ key_out,
+                                           int *__restrict__ idx_out)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= N) return;
     const int run = p / width;
     const int gstart = (run - run % ZWAY) * width;  // first key of this group of ZWAY runs
     const double kz = key[p];
@@ -812,6 +837,74 @@ __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const
     }
     key_out[pos] = kz;
     idx_out[pos] = ki;
+}
+
+template <bool REV>
+__global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
+                         double *__restrict__ key_out, int *__restrict__ idx_out)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < N) zmerge_one<REV>(p, N, width, key, idx, key_out, idx_out);
+}
+
+// The z order of one small system by the calling block of 1024 threads:
+// the rank-sorted tiles of ZTILE keys (1024 / ZTILE tiles at a time) and the
+// ZWAY-way merges of k_ztile / k_zmerge, with block barriers between the
+// passes, ending in (zkey, zperm).  (z, index) is a total order, so the
+// permutation is the one the multi-kernel sort gives.
+__device__ __forceinline__ void zsort_block(int N, const double4 *__restrict__ pos, int *zperm, int *ztmp,
+                                            double *zkey, double *zkey2)
+{
+    __shared__ double sk[1024];
+    __shared__ int si[1024];
+    int passes = 0;
+    for (int64_t w = ZTILE; w < N; w *= ZWAY) passes++;
+    double *ka = (passes & 1) ? zkey2 : zkey, *kb = (passes & 1) ? zkey : zkey2;
+    int *ia = (passes & 1) ? ztmp : zperm, *ib = (passes & 1) ? zperm : ztmp;
+    const int tid = threadIdx.x, t0 = (tid / ZTILE) * ZTILE;
+    for (int base = 0; base < N; base += 1024) {
+        const int i = base + tid;
+        double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
+        int me = 0x7fffffff;
+        if (i < N) {
+            z = pos[i].z;
+            me = i;
+        }
+        sk[tid] = z;
+        si[tid] = me;
+        __syncthreads();
+        int rank = 0;
+#pragma unroll 8
+        for (int j = 0; j < ZTILE; j++) rank += zless<false>(sk[t0 + j], si[t0 + j], z, me) ? 1 : 0;
+        if (i < N) {
+            ka[base + t0 + rank] = z;
+            ia[base + t0 + rank] = me;
+        }
+        __syncthreads();
+    }
+    for (int64_t w = ZTILE; w < N; w *= ZWAY) {
+        for (int p = tid; p < N; p += 1024) zmerge_one<false>(p, N, (int)w, ka, ia, kb, ib);
+        __syncthreads();
+        double *tk = ka; ka = kb; kb = tk;
+        int *ti = ia; ia = ib; ib = ti;
+    }
+}
+
+// Fused batches: pack, cells, pair list and z order of one small system per
+// block (the small-system kernels' code, in their order)
+__global__ void __launch_bounds__(1024) k_batch_setup(const BatchSys *__restrict__ ds, const double *__restrict__ xyz,
+                                                      const double *__restrict__ q)
+{
+    QEM_SHARED_COPY(BatchSys, d, ds + blockIdx.x);
+    for (int i = threadIdx.x; i < d.N; i += 1024)
+        pack_one(i, xyz + 3 * d.off, q + d.off, d.pos, d.cell, d.geom, d.status);
+    __syncthreads();
+    cells_small_block(d.N, d.ncell, d.cell, d.pos, d.cstart, d.clist, d.pos_of, d.pos_c);
+    __syncthreads();
+    pairs_small_block(d.N, d.pos_c, d.cell, d.cstart, d.clist, d.geom, d.rc2, d.pcount, d.poff, d.pairs, d.cap,
+                      d.in_cnt, d.in_fill, d.in_off, d.in_list, d.status);
+    __syncthreads();
+    zsort_block(d.N, d.pos, d.zperm, d.ztmp, d.zkey, d.zkey2);
 }
 
 inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
@@ -879,6 +972,13 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
 }
 
 bool qem_cells_small(int N, int ncell) { return N <= CELLS_SMALL && ncell <= CELLS_SMALL; }
+
+cudaError_t qem_launch_batch_setup(int B, const BatchSys *d, const double *xyz, const double *q, cudaStream_t s)
+{
+    if (B <= 0) return cudaSuccess;
+    k_batch_setup<<<B, 1024, 0, s>>>(d, xyz, q);
+    return cudaGetLastError();
+}
 
 cudaError_t qem_launch_cells(int N, int ncell, const int *cell, const double4 *pos, int *cell_cnt, int *cell_start,
                              int *cell_fill, int *cell_list, int *pos_of, double4 *pos_c, void *scan_tmp,

@@ -138,7 +138,7 @@ struct qem_handle {
     std::vector<double> ktab_host;
     KSampler ksamp{};
     double sampler_sumK = 0;
-    double kmax_lattice = 0;  // largest |k| the sampler can draw
+    double kmax_lattice = 0;  // bound on the |k| the sampler can draw
     DevBuf ktab, kctr;
     bool ktab_on_dev = false;
     bool kctr_reset = true;   // the device counter must be set to 0 before the next draw
@@ -314,8 +314,11 @@ static void make_sampler(const qem_params &p, KSampler &S, std::vector<double> &
     cdf(My, p.Ly, true, S.Sy);
     S.tab = tab.data();
     sumK = S.Sx + S.Sy + S.Sx * S.Sy;
+    // drawable: Float32(exp(-k^2 / 4 alpha) / sum_K) > 0, i.e. the probability
+    // above 2^-150 (K_set_generator.jl:43 keeps the probabilities as Float32)
+    S.k2max = 4.0 * p.alpha * (150.0 * log(2.0) - log(sumK));
     const double kxm = 2.0 * QEM_PI * Mx / p.Lx, kym = 2.0 * QEM_PI * My / p.Ly;
-    kmax = sqrt(kxm * kxm + kym * kym);
+    kmax = sqrt(std::min(S.k2max, kxm * kxm + kym * kym));
 }
 
 static void build_consts(qem_handle *h)
@@ -648,8 +651,6 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         }
         const int Pall = h->has_kset ? h->P : 0;
         const double kmax = draw ? h->kmax_lattice : h->kmax;
-        if (prec == QEM_FP32_FIX && Pall > 0 && kmax * h->p.Lz > 120.0)
-            return fail(h, QEM_ERR_RANGE, "max(k) * L_z > 120: use QEM_FP64 for this system");
         if (prec == QEM_FP32_FIX && Pall > 0 && !draw && !h->kset_lattice)
             return fail(h, QEM_ERR_ARG, "the FP32 k-space path takes lattice k-vectors 2 pi (m / Lx, n / Ly) only "
                                         "(K_set_generator.jl:19-25); use QEM_FP64 for other rows");
@@ -1682,6 +1683,107 @@ qem_status qem_status_check(qem_handle *h, cudaStream_t s)
 
 const qem_params *qem_handle_params(const qem_handle *h) { return &h->p; }
 const char *qem_handle_error(const qem_handle *h) { return h->err.c_str(); }
+
+uint64_t qem_handle_state(const qem_handle *h)
+{
+    uint64_t v = mix64(g_alloc_epoch.load() + 0x51ULL);
+    v = mix64(v ^ h->cfg_version);
+    v = mix64(v ^ (uint64_t)h->pair_cap);
+    v = mix64(v ^ ((uint64_t)h->P << 1) ^ (h->has_kset ? 1u : 0u));
+    return mix64(v ^ (h->kset_dirty ? 3u : 5u) ^ ((uint64_t)h->pairs_N << 8));
+}
+
+// The arguments run_once gives the small-system kernels, collected for one
+// system of a fused batch: the same buffers, the same k-slice count (unless
+// ks > 0 picks fewer) and the same per-k constants.
+qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, ShortConsts *sc, const char **why)
+{
+    auto no = [&](const char *m) {
+        if (why) *why = m;
+        return QEM_ERR_ARG;
+    };
+    if (h->p.precision != QEM_FP32_FIX) return no("precision is not QEM_FP32_FIX");
+    if (N <= 0 || N > 8192 || !qem_cells_small(N, h->ncell)) return no("more than 8192 particles or cells");
+    if (h->geom.ncx >= 3 && h->geom.ncy >= 3 && (int64_t)N >= 2 * (int64_t)h->ncell)
+        return no("two or more particles per cell (warp-per-cell pair list)");
+    if (h->p.mode_flags & QEM_EQUAL_Z_TIES) return no("equal-z tie mode");
+    if (h->shard_world != 1) return no("sharded handle");
+    if (h->sc.norm) return no("gamma_up * gamma_down > 1");
+    if (!h->pairs_valid || h->pairs_N != N || !h->status.p || !h->Epart.p)
+        return no("no synchronous call of this size yet");
+    const bool draw = resampling(h);
+    if ((h->p.rbe_p > 0 && !h->has_kset) || h->kset_dirty || (draw && (!h->ktab_on_dev || h->kctr_reset)))
+        return no("the k-set is not on the device (synchronous call first)");
+    const int P = h->has_kset ? h->P : 0;
+    const double kmax = draw ? h->kmax_lattice : h->kmax;
+    if (P > 0 && !draw && !h->kset_lattice) return no("k-set rows off the lattice");
+    if (P > 0 && (h->kin_lo != 0 || h->kin_hi != P)) return no("the k rows on the device are not the whole set");
+    const int LCH = qem_long_chunk();
+    const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = nbS;
+    const int ks_own = qem_long_ksplit(nch, std::max(P > 0 ? P : h->p.rbe_p, 1), h->long_max_ks, h->p.precision);
+    LongBuffers b;
+    const qem_status ls = long_buffers(h, N, P, nch, ks_own, ptr<double>(h->Epart), nbS, nb0, b);
+    if (ls != QEM_OK) return ls;
+    b.ks = ks > 0 ? std::min(ks, ks_own) : ks_own;
+    b.zlim = P > 0 ? qem_fp32_zlim(kmax) : 0.0;
+    if (draw && P > 0) {
+        b.draw_ctr = ptr<unsigned long long>(h->kctr);
+        b.sampler = h->ksamp;
+        b.sampler.tab = ptr<double>(h->ktab);
+        b.sampler.seed = h->kseed;
+        b.sampler.row0 = 0;
+        b.kwt = nullptr;
+    }
+    BatchSys &e = *d;
+    e = BatchSys{};
+    e.N = N;
+    e.ncell = h->ncell;
+    e.P = P;
+    e.nch = nch;
+    e.ks = b.ks;
+    e.cap = h->pair_cap;
+    e.Flong = ptr<double>(h->Flong);
+    e.pos = ptr<double4>(h->pos);
+    e.pos_c = ptr<double4>(h->pos_c);
+    e.cell = ptr<int>(h->cell);
+    e.cstart = ptr<int>(h->cell_start);
+    e.clist = ptr<int>(h->cell_list);
+    e.pos_of = ptr<int>(h->pos_of);
+    e.pcount = ptr<int>(h->pcount);
+    e.in_cnt = ptr<int>(h->in_cnt);
+    e.in_fill = ptr<int>(h->in_fill);
+    e.in_list = ptr<int>(h->in_list);
+    e.poff = ptr<int64_t>(h->poff);
+    e.in_off = ptr<int64_t>(h->in_off);
+    e.pairs = ptr<int2>(h->pairs);
+    e.R = ptr<double4>(h->R);
+    e.status = ptr<unsigned>(h->status);
+    e.geom = h->geom;
+    e.rc2 = h->sc.rc2;
+    e.zperm = ptr<int>(h->zperm);
+    e.ztmp = ptr<int>(h->ztmp);
+    e.zkey = ptr<double>(h->zkey);
+    e.zkey2 = ptr<double>(h->zkey2);
+    e.b = b;
+    const double Lx = h->p.Lx, Ly = h->p.Ly, Lz = h->p.Lz, eps0 = h->p.eps_0;
+    const double sumK = P > 0 ? h->sum_K * P / P : 0.0;  // run_once's sum_K * Pk / Pall, bit for bit
+    e.h = 0.5 * Lz;
+    e.fscale = 1.0 / (2.0 * Lx * Ly * eps0);
+    e.Lz = Lz;
+    e.g1 = h->p.gamma_down;
+    e.g2 = h->p.gamma_up;
+    e.g12 = e.g1 * e.g2;
+    e.wk = P > 0 ? (sumK / P) / (Lx * Ly * eps0) : 0.0;
+    e.esc = P > 0 ? -(sumK / P) / (2.0 * eps0 * Lx * Ly) : 0.0;
+    e.wden = Lx * Ly * eps0;
+    e.eden = 2.0 * eps0 * Lx * Ly;
+    e.invLx = 1.0 / Lx;
+    e.invLy = 1.0 / Ly;
+    e.Lx_2pi = Lx / (2.0 * QEM_PI);
+    e.Ly_2pi = Ly / (2.0 * QEM_PI);
+    *sc = h->sc;
+    return QEM_OK;
+}
 
 extern "C" qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world)
 {

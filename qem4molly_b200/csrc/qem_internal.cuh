@@ -124,14 +124,21 @@ __host__ __device__ inline double unit53_lo(uint64_t r) { return (double)(r >> 1
 // uniform picks the part, two more pick m_x and m_y by inverse CDF.
 // tab holds four cumulative weight tables, m ascending: x over all m
 // (2 Mx + 1), x over m != 0 (2 Mx), y over all m (2 My + 1), y over m != 0 (2 My).
+// The reference stores the probabilities exp(-k^2 / 4 alpha) / sum_K as
+// Float32 (K_set_generator.jl:34, 43), so lattice points whose probability
+// rounds to zero there (|k|^2 >= k2max) are never drawn; a separable draw
+// that lands on one (probability below 2^-150 per row) is drawn again from
+// the next counter words.
 struct KSampler {
     const double *tab;   // device (or host) address of the tables
     int Mx, My;
     double Lx, Ly;
     double Sx, Tx, Sy, Ty;  // sums over m != 0 (S) and over all m (T) per axis
+    double k2max;           // |k|^2 bound of the drawable points
     uint64_t seed;
     int64_t row0;           // first row of this rank's share (the device k rows start there)
 };
+constexpr int QEM_KSAMPLE_TRIES = 16;
 
 // smallest i in [0, n) with c[i] > u (n - 1 if none): inverse CDF of an
 // ascending cumulative table
@@ -146,25 +153,42 @@ __host__ __device__ inline int cdf_pick(const double *c, int n, double u)
     return lo;
 }
 
-// row `row` of batch n: (kx, ky, |k|)
+// row `row` of batch n: (kx, ky, |k|).  Try t takes the words 3 t .. 3 t + 2
+// of (seed, n, row); after QEM_KSAMPLE_TRIES off-support draws (probability
+// below 2^-2400) the row is the lattice point (0, 1) (or (1, 0) if My = 0).
 __host__ __device__ inline void ksample_row(const KSampler &S, uint64_t n, int64_t row, double &kx, double &ky,
                                             double &k)
 {
     const double *cx_all = S.tab, *cx_nz = cx_all + 2 * S.Mx + 1;
     const double *cy_all = cx_nz + 2 * S.Mx, *cy_nz = cy_all + 2 * S.My + 1;
-    const double u0 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 0));
-    const double u1 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 1));
-    const double u2 = unit53_lo(draw64(S.seed, n, (uint64_t)row, 2));
     const double A = S.Sx * S.Ty;  // weight of m_x != 0
-    int mx, my;
-    if (S.Mx > 0 && u0 * (A + S.Sy) < A) {
-        const int i = cdf_pick(cx_nz, 2 * S.Mx, u1 * S.Sx);
-        mx = i < S.Mx ? i - S.Mx : i - S.Mx + 1;
-        my = cdf_pick(cy_all, 2 * S.My + 1, u2 * S.Ty) - S.My;
-    } else {
-        mx = 0;
-        const int i = cdf_pick(cy_nz, 2 * S.My, u2 * S.Sy);
-        my = i < S.My ? i - S.My : i - S.My + 1;
+    int mx = S.My > 0 ? 0 : 1, my = S.My > 0 ? 1 : 0;
+    for (int t = 0; t < QEM_KSAMPLE_TRIES; t++) {
+        const uint64_t c = 3 * (uint64_t)t;
+        const double u0 = unit53_lo(draw64(S.seed, n, (uint64_t)row, c));
+        const double u1 = unit53_lo(draw64(S.seed, n, (uint64_t)row, c + 1));
+        const double u2 = unit53_lo(draw64(S.seed, n, (uint64_t)row, c + 2));
+        int ax, ay;
+        if (S.Mx > 0 && u0 * (A + S.Sy) < A) {
+            const int i = cdf_pick(cx_nz, 2 * S.Mx, u1 * S.Sx);
+            ax = i < S.Mx ? i - S.Mx : i - S.Mx + 1;
+            ay = cdf_pick(cy_all, 2 * S.My + 1, u2 * S.Ty) - S.My;
+        } else {
+            ax = 0;
+            const int i = cdf_pick(cy_nz, 2 * S.My, u2 * S.Sy);
+            ay = i < S.My ? i - S.My : i - S.My + 1;
+        }
+        const double fx = (2.0 * QEM_PI) * (double)ax / S.Lx, fy = (2.0 * QEM_PI) * (double)ay / S.Ly;
+#ifdef __CUDA_ARCH__
+        const double k2 = __dadd_rn(__dmul_rn(fx, fx), __dmul_rn(fy, fy));  // the host's rounding
+#else
+        const double k2 = fx * fx + fy * fy;
+#endif
+        if (k2 < S.k2max) {
+            mx = ax;
+            my = ay;
+            break;
+        }
     }
     kx = 2.0 * QEM_PI * (double)mx / S.Lx;
     ky = 2.0 * QEM_PI * (double)my / S.Ly;
@@ -334,6 +358,81 @@ const qem_params *qem_handle_params(const qem_handle *h);
 // caps the k-slices of the handle's long-range force pass (1 .. QEM_LONG_MAX_KS)
 void qem_handle_set_long_max_ks(qem_handle *h, int max_ks);
 const char *qem_handle_error(const qem_handle *h);
+
+// ---- fused batches: one launch per phase over all systems -------------------
+// BatchSys is one system of a batch: its slice of the batch arrays, its
+// handle's device buffers and its per-call constants, i.e. the arguments the
+// single-system launches of the small-system path take.  A phase's blocks
+// read (system, x, y) from a work list built on the host and run the same
+// per-block code as the single-system kernels; the one-block kernels of a
+// small system (pack + cells + pair list + z order, and the long-range
+// preparation) run as one block per system.
+struct BatchSys {
+    int N, ncell, P, nch, ks;
+    int64_t cap;              // pair capacity
+    int64_t off;              // first particle of the system in the batch arrays
+    double *Flong;            // long-range forces (handle buffer), added by the gather
+    double4 *pos, *pos_c;
+    int *cell, *cstart, *clist, *pos_of, *pcount, *in_cnt, *in_fill, *in_list;
+    int64_t *poff, *in_off;
+    int2 *pairs;
+    double4 *R;
+    unsigned *status;
+    CellGeom geom;
+    double rc2;
+    int *zperm, *ztmp;
+    double *zkey, *zkey2;
+    LongBuffers b;
+    // k-space constants of the preparation (as qem_launch_long derives them)
+    double h, fscale, Lz, g1, g2, g12, wk, esc, wden, eden, invLx, invLy, Lx_2pi, Ly_2pi;
+};
+struct BatchWork {
+    int s, x, y, pad;
+};
+// the block's shared copy of a system's struct (BatchSys, ShortConsts):
+// every thread copies words, then a block barrier
+template <class T>
+__device__ __forceinline__ void block_copy(T *dst, const T *src)
+{
+    static_assert(sizeof(T) % 4 == 0, "word copy");
+    const unsigned *a = reinterpret_cast<const unsigned *>(src);
+    unsigned *b = reinterpret_cast<unsigned *>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) b[i] = a[i];
+    __syncthreads();
+}
+// declares `T &name` in shared memory holding *src (the types have default
+// member initialisers, which a __shared__ declaration of the type cannot take)
+#define QEM_SHARED_COPY(T, name, src)                              \
+    __shared__ __align__(16) unsigned char name##_raw[sizeof(T)]; \
+    T &name = *reinterpret_cast<T *>(name##_raw);                  \
+    block_copy(&name, (src))
+// blocks per system of each phase: pairs per pair block, particles per
+// gather / final block, k-vectors per totals / scan block, k-slices per
+// force-pass block
+int qem_batch_pair_tile(void);
+int qem_batch_particle_tile(void);
+int qem_batch_ltot_tile(void);
+int qem_batch_lscan_tile(void);
+int qem_batch_lforce_tile(void);
+cudaError_t qem_launch_batch_setup(int B, const BatchSys *d, const double *xyz, const double *q, cudaStream_t s);
+cudaError_t qem_launch_batch_lprep(int B, const BatchSys *d, cudaStream_t s);
+cudaError_t qem_launch_batch_ltot(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
+cudaError_t qem_launch_batch_lscan(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
+cudaError_t qem_launch_batch_lforce(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
+cudaError_t qem_launch_batch_lfinal(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
+cudaError_t qem_launch_batch_pairs(int nw, const BatchWork *w, const BatchSys *d, const ShortConsts *sc,
+                                   cudaStream_t s);
+cudaError_t qem_launch_batch_gather(int nw, const BatchWork *w, const BatchSys *d, const ShortConsts *sc, int do_lj,
+                                    double *F, cudaStream_t s);
+// fills one system's entry (qem_capi.cu; off is left 0) after a synchronous
+// call of the same size; ks <= 0 keeps the handle's own k-slice count.
+// Returns QEM_ERR_ARG with the reason in *why when the system does not take
+// the small-system kernels in FP32+fix (the batch then keeps per-system
+// pipelines).
+qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, ShortConsts *sc, const char **why);
+// changes whenever a buffer of any handle is reallocated or this handle's
+// k-set, shard or pair capacity changes
+uint64_t qem_handle_state(const qem_handle *h);
 
 // ---- adjoint (FP64) --------------------------------------------------------
 // pair records RA (2 double4 per pair) and the per-particle pass writing

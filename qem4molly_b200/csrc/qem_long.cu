@@ -163,19 +163,16 @@ __global__ void k_zgather(int N, const double4 *__restrict__ pos, const int *__r
 // and k_kconst.
 constexpr int LONG_PREP_SMALL = 8192;
 
-__global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *__restrict__ pos,
-                                                          const int *__restrict__ zperm, double h,
-                                                          double *__restrict__ zx, double *__restrict__ zy,
-                                                          double *__restrict__ zhd, double *__restrict__ qd,
-                                                          double *__restrict__ qscan, double fscale,
-                                                          double *__restrict__ k0, int P,
-                                                          double *__restrict__ kin, KConst *__restrict__ kc,
-                                                          double Lz, double g12, double wk, double esc,
-                                                          const double *__restrict__ kwt, double wden, double eden,
-                                                          double zlim, unsigned *status, const KSampler S,
-                                                          const unsigned long long *__restrict__ ctr,
-                                                          uint4 *__restrict__ zP, double invLx, double invLy,
-                                                          double Lx_2pi, double Ly_2pi)
+__device__ __forceinline__ void long_prep_block(int N, const double4 *__restrict__ pos,
+                                                const int *__restrict__ zperm, double h, double *__restrict__ zx,
+                                                double *__restrict__ zy, double *__restrict__ zhd,
+                                                double *__restrict__ qd, double *__restrict__ qscan, double fscale,
+                                                double *__restrict__ k0, int P, double *__restrict__ kin,
+                                                KConst *__restrict__ kc, double Lz, double g12, double wk,
+                                                double esc, const double *__restrict__ kwt, double wden,
+                                                double eden, double zlim, unsigned *status, const KSampler &S,
+                                                const unsigned long long *__restrict__ ctr, uint4 *__restrict__ zP,
+                                                double invLx, double invLy, double Lx_2pi, double Ly_2pi)
 {
     __shared__ double warp_tot[32];
     for (int m = threadIdx.x; m < P; m += 1024)
@@ -198,6 +195,24 @@ __global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *
         const double above = (tot - below) - q;
         k0[m] = q * (below - above) * fscale;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_long_prep_small(int N, const double4 *__restrict__ pos,
+                                                          const int *__restrict__ zperm, double h,
+                                                          double *__restrict__ zx, double *__restrict__ zy,
+                                                          double *__restrict__ zhd, double *__restrict__ qd,
+                                                          double *__restrict__ qscan, double fscale,
+                                                          double *__restrict__ k0, int P,
+                                                          double *__restrict__ kin, KConst *__restrict__ kc,
+                                                          double Lz, double g12, double wk, double esc,
+                                                          const double *__restrict__ kwt, double wden, double eden,
+                                                          double zlim, unsigned *status, const KSampler S,
+                                                          const unsigned long long *__restrict__ ctr,
+                                                          uint4 *__restrict__ zP, double invLx, double invLy,
+                                                          double Lx_2pi, double Ly_2pi)
+{
+    long_prep_block(N, pos, zperm, h, zx, zy, zhd, qd, qscan, fscale, k0, P, kin, kc, Lz, g12, wk, esc, kwt, wden,
+                    eden, zlim, status, S, ctr, zP, invLx, invLy, Lx_2pi, Ly_2pi);
 }
 
 // k = 0 term (Force_long.jl:130-161, Energy_long_range_njit.py:25-44)
@@ -295,12 +310,13 @@ __global__ void __launch_bounds__(LT) k_ltot(int N, int P, int nch, const double
 // one warp per k: exclusive scans of the chunk totals (FP64), written in the
 // force pass's precision, and the per-k force constants
 template <typename Real>
-__global__ void k_lscan(int P, int nch, const double *__restrict__ tot, Real *__restrict__ off,
-                        double *__restrict__ Utot, const KConst *__restrict__ kc, double g1, double g2,
-                        double *__restrict__ Eks, KForce<Real> *__restrict__ kf)
+__device__ __forceinline__ void lscan_tile(int bx, int P, int nch, const double *__restrict__ tot,
+                                           Real *__restrict__ off, double *__restrict__ Utot,
+                                           const KConst *__restrict__ kc, double g1, double g2,
+                                           double *__restrict__ Eks, KForce<Real> *__restrict__ kf)
 {
     const int lane = threadIdx.x & 31;
-    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int m = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (m >= P) return;
     const double *T = tot + (int64_t)m * nch * 4;
     Real *O = off + (int64_t)m * nch * 4;
@@ -358,6 +374,14 @@ __global__ void k_lscan(int P, int nch, const double *__restrict__ tot, Real *__
         F.s2i = (Real)(gW * (g12W * ci + g1 * di));
         kf[m] = F;
     }
+}
+
+template <typename Real>
+__global__ void k_lscan(int P, int nch, const double *__restrict__ tot, Real *__restrict__ off,
+                        double *__restrict__ Utot, const KConst *__restrict__ kc, double g1, double g2,
+                        double *__restrict__ Eks, KForce<Real> *__restrict__ kf)
+{
+    lscan_tile<Real>(blockIdx.x, P, nch, tot, off, Utot, kc, g1, g2, Eks, kf);
 }
 
 // Force pass.  For particle j with phase e^{i theta} = c + i s, ep = e^{k(z-h)},
@@ -516,12 +540,12 @@ constexpr float THIN = 1.0f;    // largest k * (chunk z extent) of the one-walk 
 
 // chunk totals: lane k sums u = q e^{k (z-h)} e^{i k.rho} and v = q e^{-k (z-h)}
 // e^{i k.rho} over the chunk, in FP32 over 16 particles at a time, in FP64 across
-__global__ void __launch_bounds__(KTT) k_ltot_lk(int N, int P, int nch, const uint4 *__restrict__ zp,
-                                                 const KConst *__restrict__ kc, double *__restrict__ tot)
+__device__ __forceinline__ void ltot_lk_tile(int c, int kb, int N, int P, int nch, const uint4 *__restrict__ zp,
+                                             const KConst *__restrict__ kc, double *__restrict__ tot)
 {
     constexpr float LOG2E = 1.4426950408889634f;
-    const int c = blockIdx.x, m0 = c * LCH, n = min(LCH, N - m0);
-    const int k = blockIdx.y * KTT + threadIdx.x;
+    const int m0 = c * LCH, n = min(LCH, N - m0);
+    const int k = kb * KTT + threadIdx.x;
     if (k >= P) return;
     const int mx = kc[k].mx, my = kc[k].my;
     const float kl = (float)kc[k].k * LOG2E;
@@ -557,6 +581,12 @@ __global__ void __launch_bounds__(KTT) k_ltot_lk(int N, int P, int nch, const ui
     T[1] = U1;
     T[2] = U2;
     T[3] = U3;
+}
+
+__global__ void __launch_bounds__(KTT) k_ltot_lk(int N, int P, int nch, const uint4 *__restrict__ zp,
+                                                 const KConst *__restrict__ kc, double *__restrict__ tot)
+{
+    ltot_lk_tile(blockIdx.x, blockIdx.y, N, P, nch, zp, kc, tot);
 }
 
 // one lane's k-vector for the force pass (zeros for lanes past P: no force)
@@ -685,18 +715,18 @@ __device__ __forceinline__ float lk_walk(const uint4 *__restrict__ pp, int n, co
 // k-groups of 32 vectors g = t, t + ks_n, ... and writes slice t of Fpart
 // (z order, the particle's q applied) and of the energy partials
 template <bool ENERGY>
-__global__ void __launch_bounds__(32 * KFW) k_lforce_lk(int N, int P, int nch, int ks_n,
-                                                        const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
-                                                        const KForce<float> *__restrict__ kf,
-                                                        const float *__restrict__ off, const double *__restrict__ tot,
-                                                        double *__restrict__ Fpart, double *__restrict__ Epart)
+__device__ __forceinline__ void lforce_lk_tile(int c, int by, int N, int P, int nch, int ks_n,
+                                               const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
+                                               const KForce<float> *__restrict__ kf, const float *__restrict__ off,
+                                               const double *__restrict__ tot, double *__restrict__ Fpart,
+                                               double *__restrict__ Epart)
 {
     constexpr float LOG2E = 1.4426950408889634f;
     __shared__ float tr[KFW][32][3 * KG + 1];  // +1: column reads on distinct banks
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int t = blockIdx.y * KFW + w;
+    const int t = by * KFW + w;
     if (t >= ks_n) return;  // whole warp; the kernel has no block barrier
-    const int c = blockIdx.x, m0 = c * LCH, n = min(LCH, N - m0);
+    const int m0 = c * LCH, n = min(LCH, N - m0);
     const uint4 *pp = zp + m0;
     const float dz = __uint_as_float(pp[n - 1].z) - __uint_as_float(pp[0].z);
     double *Fo = Fpart + ((int64_t)t * N + m0) * 3;
@@ -752,13 +782,23 @@ __global__ void __launch_bounds__(32 * KFW) k_lforce_lk(int N, int P, int nch, i
     }
 }
 
+template <bool ENERGY>
+__global__ void __launch_bounds__(32 * KFW) k_lforce_lk(int N, int P, int nch, int ks_n,
+                                                        const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
+                                                        const KForce<float> *__restrict__ kf,
+                                                        const float *__restrict__ off, const double *__restrict__ tot,
+                                                        double *__restrict__ Fpart, double *__restrict__ Epart)
+{
+    lforce_lk_tile<ENERGY>(blockIdx.x, blockIdx.y, N, P, nch, ks_n, zp, kc, kf, off, tot, Fpart, Epart);
+}
+
 // F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term; ctr: the batch
 // counter of a per-call random batch, advanced once here, after every read of
 // it (the per-k constants kernel ran earlier on the same stream)
-__global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, const double *__restrict__ k0,
-                         const int *__restrict__ zperm, double *__restrict__ F3, unsigned long long *ctr)
+__device__ __forceinline__ void lfinal_one(int m, int N, int ks_n, const double *__restrict__ Fpart,
+                                           const double *__restrict__ k0, const int *__restrict__ zperm,
+                                           double *__restrict__ F3, unsigned long long *ctr)
 {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctr && m == 0) *ctr += 1;
     if (m >= N) return;
     double fx = 0, fy = 0, fz = 0;
@@ -772,6 +812,60 @@ __global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, cons
     F3[3 * i] += fx;
     F3[3 * i + 1] += fy;
     F3[3 * i + 2] += fz + k0[m];
+}
+
+__global__ void k_lfinal(int N, int ks_n, const double *__restrict__ Fpart, const double *__restrict__ k0,
+                         const int *__restrict__ zperm, double *__restrict__ F3, unsigned long long *ctr)
+{
+    lfinal_one(blockIdx.x * blockDim.x + threadIdx.x, N, ks_n, Fpart, k0, zperm, F3, ctr);
+}
+
+// ---------------------------------------------------------------------------
+// fused batches: the small-system long-range phases over all systems
+// ---------------------------------------------------------------------------
+constexpr int BATCH_PTILE = 256;  // particles per block of the final pass
+
+// one block per system: clears the long-range force buffer (the final pass
+// adds into it) and runs the one-block preparation of k_long_prep_small
+__global__ void __launch_bounds__(1024) k_batch_lprep(const BatchSys *__restrict__ ds)
+{
+    QEM_SHARED_COPY(BatchSys, d, ds + blockIdx.x);
+    for (int i = threadIdx.x; i < 3 * d.N; i += 1024) d.Flong[i] = 0.0;
+    long_prep_block(d.N, d.pos, d.zperm, d.h, d.b.zx, d.b.zy, d.b.zhd, d.b.qd, d.b.qscan, d.fscale, d.b.k0, d.P,
+                    d.b.kin, d.b.kc, d.Lz, d.g12, d.wk, d.esc, d.b.kwt, d.wden, d.eden, d.b.zlim, d.status,
+                    d.b.sampler, d.b.draw_ctr, d.b.zP, d.invLx, d.invLy, d.Lx_2pi, d.Ly_2pi);
+}
+
+__global__ void __launch_bounds__(KTT) k_batch_ltot(const BatchWork *__restrict__ wl, const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    ltot_lk_tile(t.x, t.y, d.N, d.P, d.nch, d.b.zP, d.b.kc, d.b.tot);
+}
+
+__global__ void __launch_bounds__(128) k_batch_lscan(const BatchWork *__restrict__ wl, const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    lscan_tile<float>(t.x, d.P, d.nch, d.b.tot, (float *)d.b.off, d.b.Utot, d.b.kc, d.g1, d.g2, d.b.Eks,
+                      (KForce<float> *)d.b.kf);
+}
+
+__global__ void __launch_bounds__(32 * KFW) k_batch_lforce(const BatchWork *__restrict__ wl,
+                                                           const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    lforce_lk_tile<false>(t.x, t.y, d.N, d.P, d.nch, d.ks, d.b.zP, d.b.kc, (const KForce<float> *)d.b.kf,
+                          (const float *)d.b.off, d.b.tot, d.b.Fpart, d.b.Epart);
+}
+
+__global__ void __launch_bounds__(BATCH_PTILE) k_batch_lfinal(const BatchWork *__restrict__ wl,
+                                                              const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    lfinal_one(t.x * BATCH_PTILE + threadIdx.x, d.N, d.ks, d.b.Fpart, d.b.k0, d.zperm, d.Flong, d.b.draw_ctr);
 }
 
 __global__ void k_reduce_sum(const double *__restrict__ in, int n, double *__restrict__ out)
@@ -1305,6 +1399,42 @@ __global__ void k_scale_vec(int n, double a, const double *x, double *y)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] = a * x[i];
+}
+
+int qem_batch_particle_tile(void) { return BATCH_PTILE; }
+int qem_batch_ltot_tile(void) { return KTT; }
+int qem_batch_lscan_tile(void) { return 4; }
+int qem_batch_lforce_tile(void) { return KFW; }
+
+cudaError_t qem_launch_batch_lprep(int B, const BatchSys *d, cudaStream_t s)
+{
+    if (B <= 0) return cudaSuccess;
+    k_batch_lprep<<<B, 1024, 0, s>>>(d);
+    return cudaGetLastError();
+}
+cudaError_t qem_launch_batch_ltot(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_ltot<<<nw, KTT, 0, s>>>(w, d);
+    return cudaGetLastError();
+}
+cudaError_t qem_launch_batch_lscan(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_lscan<<<nw, 128, 0, s>>>(w, d);
+    return cudaGetLastError();
+}
+cudaError_t qem_launch_batch_lforce(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_lforce<<<nw, 32 * KFW, 0, s>>>(w, d);
+    return cudaGetLastError();
+}
+cudaError_t qem_launch_batch_lfinal(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_lfinal<<<nw, BATCH_PTILE, 0, s>>>(w, d);
+    return cudaGetLastError();
 }
 
 cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s)

@@ -108,7 +108,6 @@ extern "C" qem_status qem_long_forces_noalloc(const qem_params *p, int32_t N, co
             return reject("k-set rows must be (kx, ky, |k|) with |k| > 0");
         kmax = std::max(kmax, k);
     }
-    if (p->precision == QEM_FP32_FIX && P > 0 && kmax * p->Lz > 120.0) return QEM_ERR_RANGE;
     if (p->precision == QEM_FP32_FIX) {  // the FP32 phases are fixed-point lattice phases
         for (int i = 0; i < P; i++) {
             const double m = k3[3 * i] * p->Lx / (2.0 * QEM_PI), n = k3[3 * i + 1] * p->Ly / (2.0 * QEM_PI);

@@ -267,19 +267,17 @@ __device__ __forceinline__ void quad(const ShortConsts &c, const Interval &v, do
 // np: device pointer to the pair count; the grid covers the capacity cap and
 // blocks past the count return (a count above cap, which the host treats as
 // an overflow and re-evaluates, is clamped so every access stays in bounds)
+// bx: the block's tile of PAIR_BLOCK pairs
 template <int PREC, bool ENERGY>
-__global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const int64_t *__restrict__ np,
-                                                                           int64_t cap,
-                                                                           const int2 *__restrict__ pairs,
-                                                                           const double4 *__restrict__ pos,
-                                                                           double4 *__restrict__ R,
-                                                                           double *__restrict__ Upair,
-                                                                           const ShortConsts c)
+__device__ __forceinline__ void short_pair_tile(const ShortConsts &c, int64_t bx, const int64_t *__restrict__ np,
+                                                int64_t cap, const int2 *__restrict__ pairs,
+                                                const double4 *__restrict__ pos, double4 *__restrict__ R,
+                                                double *__restrict__ Upair)
 {
     __shared__ int hist[RHO_BINS];
     __shared__ int sidx[PAIR_BLOCK];
     const int64_t Np = min(*np, cap);
-    if ((int64_t)blockIdx.x * PAIR_BLOCK >= Np) return;  // whole block: before any barrier
+    if (bx * PAIR_BLOCK >= Np) return;  // whole block: before any barrier
     // this rank's block of the pair list (all of it unless sharded)
     const int64_t lo = Np * c.shard_rank / c.shard_world, hi = Np * (c.shard_rank + 1) / c.shard_world;
     // 1. every thread loads one pair and its rho^2; the block's pairs are
@@ -291,7 +289,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
     {
         if (threadIdx.x < RHO_BINS) hist[threadIdx.x] = 0;
         __syncthreads();
-        const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + threadIdx.x;
+        const int64_t p = bx * PAIR_BLOCK + threadIdx.x;
         int bin = RHO_BINS - 1;
         if (p >= lo && p < hi) {
             const int2 ij = pairs[p];
@@ -323,7 +321,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
         sidx[hist[bin] + slot] = threadIdx.x;
         __syncthreads();
     }
-    const int64_t p = (int64_t)blockIdx.x * PAIR_BLOCK + sidx[threadIdx.x];
+    const int64_t p = bx * PAIR_BLOCK + sidx[threadIdx.x];
     if (p >= Np) return;
     if (p < lo || p >= hi) {  // another rank's pair
         R[p] = make_double4(0, 0, 0, 0);
@@ -390,6 +388,18 @@ __global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const 
     if (ENERGY) Upair[p] = pref * (U + Ub);
 }
 
+template <int PREC, bool ENERGY>
+__global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_short_pair(const int64_t *__restrict__ np,
+                                                                           int64_t cap,
+                                                                           const int2 *__restrict__ pairs,
+                                                                           const double4 *__restrict__ pos,
+                                                                           double4 *__restrict__ R,
+                                                                           double *__restrict__ Upair,
+                                                                           const ShortConsts c)
+{
+    short_pair_tile<PREC, ENERGY>(c, blockIdx.x, np, cap, pairs, pos, R, Upair);
+}
+
 // ---------------------------------------------------------------------------
 // self image z-force (Force_short.jl:82-107) and self energy
 // (Energy_short_range_njit.py:64-81), rho = 0 so J0 = 1
@@ -427,20 +437,17 @@ __device__ void self_terms(const ShortConsts &c, double z, double q, double &Fz,
 // ---------------------------------------------------------------------------
 // per-particle pass: own + incoming pair records, self term, walls
 // ---------------------------------------------------------------------------
+// particle i: writes F3[i], returns its energy share
 template <int PREC, bool ENERGY>
-__global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__restrict__ pos,
-                                                       const int *__restrict__ pos_of, const int64_t *__restrict__ poff,
-                                                       const double4 *__restrict__ R, const double *__restrict__ Upair,
-                                                       const int64_t *__restrict__ in_off,
-                                                       const int *__restrict__ in_list, int64_t cap,
-                                                       const ShortConsts c, double *__restrict__ F3,
-                                                       double *__restrict__ Epart, unsigned *status, int do_short,
-                                                       int do_lj, const double *__restrict__ Fadd)
+__device__ __forceinline__ double gather_one(const ShortConsts &c, int i, const double4 *__restrict__ pos,
+                                             const int *__restrict__ pos_of, const int64_t *__restrict__ poff,
+                                             const double4 *__restrict__ R, const double *__restrict__ Upair,
+                                             const int64_t *__restrict__ in_off, const int *__restrict__ in_list,
+                                             int64_t cap, double *__restrict__ F3, unsigned *status, int do_short,
+                                             int do_lj, const double *__restrict__ Fadd)
 {
-    __shared__ double red[256 / 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double Fx = 0, Fy = 0, Fz = 0, E = 0;
-    if (i < N) {
+    {
         const double4 pi = pos[i];
         if (do_short) {
             const int t = pos_of[i];
@@ -484,6 +491,25 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
         F3[3 * i + 1] = Fy;
         F3[3 * i + 2] = Fz;
     }
+    return E;
+}
+
+template <int PREC, bool ENERGY>
+__global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__restrict__ pos,
+                                                       const int *__restrict__ pos_of, const int64_t *__restrict__ poff,
+                                                       const double4 *__restrict__ R, const double *__restrict__ Upair,
+                                                       const int64_t *__restrict__ in_off,
+                                                       const int *__restrict__ in_list, int64_t cap,
+                                                       const ShortConsts c, double *__restrict__ F3,
+                                                       double *__restrict__ Epart, unsigned *status, int do_short,
+                                                       int do_lj, const double *__restrict__ Fadd)
+{
+    __shared__ double red[256 / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double E = 0;
+    if (i < N)
+        E = gather_one<PREC, ENERGY>(c, i, pos, pos_of, poff, R, Upair, in_off, in_list, cap, F3, status, do_short,
+                                     do_lj, Fadd);
     if (ENERGY) {
         // deterministic block reduction of the per-particle energies
         for (int d = 16; d > 0; d >>= 1) E += __shfl_down_sync(0xffffffffu, E, d);
@@ -497,9 +523,58 @@ __global__ void __launch_bounds__(256) k_short_gather(int N, const double4 *__re
     }
 }
 
+// ---------------------------------------------------------------------------
+// fused batches: the pair and gather phases over (system, tile) work lists;
+// each block works on its system's ShortConsts copied to shared memory
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PAIR_BLOCK, QEM_PAIR_MINB) k_batch_pairs(const BatchWork *__restrict__ wl,
+                                                                            const BatchSys *__restrict__ ds,
+                                                                            const ShortConsts *__restrict__ scs)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    QEM_SHARED_COPY(ShortConsts, c, scs + t.s);
+    short_pair_tile<QEM_FP32_FIX, false>(c, t.x, d.poff + d.N, d.cap, d.pairs, d.pos, d.R, nullptr);
+}
+
+constexpr int GATHER_TILE = 256;
+
+__global__ void __launch_bounds__(GATHER_TILE) k_batch_gather(const BatchWork *__restrict__ wl,
+                                                              const BatchSys *__restrict__ ds,
+                                                              const ShortConsts *__restrict__ scs, int do_lj,
+                                                              double *__restrict__ F)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    QEM_SHARED_COPY(ShortConsts, c, scs + t.s);
+    const int i = t.x * GATHER_TILE + threadIdx.x;
+    if (i < d.N)
+        gather_one<QEM_FP32_FIX, false>(c, i, d.pos, d.pos_of, d.poff, d.R, nullptr, d.in_off, d.in_list, d.cap,
+                                        F + 3 * d.off, d.status, 1, do_lj, d.Flong);
+}
+
 inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
 
 }  // namespace
+
+int qem_batch_pair_tile(void) { return PAIR_BLOCK; }
+
+cudaError_t qem_launch_batch_pairs(int nw, const BatchWork *w, const BatchSys *d, const ShortConsts *sc,
+                                   cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_pairs<<<nw, PAIR_BLOCK, 0, s>>>(w, d, sc);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_batch_gather(int nw, const BatchWork *w, const BatchSys *d, const ShortConsts *sc, int do_lj,
+                                    double *F, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    static_assert(GATHER_TILE == 256, "the gather tile is the particle tile of the final pass");
+    k_batch_gather<<<nw, GATHER_TILE, 0, s>>>(w, d, sc, do_lj, F);
+    return cudaGetLastError();
+}
 
 cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np, int64_t cap, const int2 *pairs,
                                    const double4 *pos, double4 *R, double *Upair, const ShortConsts &c,

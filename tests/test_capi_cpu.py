@@ -159,7 +159,14 @@ def sampler_rows(Lx, Ly, alpha, accuracy, seed, n, row0, P):
     my = np.where(partx, iy_all, np.where(iyn < M[1], iyn - M[1], iyn - M[1] + 1))
     kx = 2.0 * np.pi * mx.astype(np.float64) / Lx
     ky = 2.0 * np.pi * my.astype(np.float64) / Ly
-    return np.stack([kx, ky, np.sqrt(kx * kx + ky * ky)], 1), Sx + Sy + Sx * Sy
+    sum_K = Sx + Sy + Sx * Sy
+    # support: Float32(exp(-k^2 / 4 alpha) / sum_K) > 0 (K_set_generator.jl:43);
+    # the library draws an off-support row again from the next counter words,
+    # which these parameters never need (such a row has probability < 2^-150)
+    k2max = 4.0 * alpha * (150.0 * math.log(2.0) - math.log(sum_K))
+    fx, fy = 2.0 * np.pi * mx / Lx, 2.0 * np.pi * my / Ly
+    assert np.all(fx * fx + fy * fy < k2max)
+    return np.stack([kx, ky, np.sqrt(kx * kx + ky * ky)], 1), sum_K
 
 
 def _draw(lib, Lx, Ly, alpha, seed, n, row0, P, accuracy=1e-6):
