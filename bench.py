@@ -487,7 +487,7 @@ def run_batch(args, quiet=False):
                           "kset": "a fresh seeded random batch of P k-vectors per system on every step",
                           "l2": "working set (< 100 MB) stays in L2 between steps; not flushed"},
                "batch_mode": {"mode": mode["mode"], "pool_width": width, "ks_per_system": mode["ks"],
-                              "order": ["batch", "largest first"][mode["order"]],
+                              "order": ["batch", "largest first"][mode["order"]], "chunk": mode["chunk"],
                               "launches_per_evaluation": mode["launches"], "why_not_fused": mode["why"]},
                "batch_forces_graph_ms": ms_eval, "eager_per_system_forces_ms": eager_ms,
                "particle_steps_per_s": args.steps * sum(N) * world * 1000.0 / ms,

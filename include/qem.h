@@ -317,11 +317,13 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  * exclusive prefix sum of N.  The handles stay owned by the caller.
  *
  * A batch evaluation runs one of two ways (qem_batch_set_mode):
- *   QEM_BATCH_FUSED: eight launches for the whole batch -- one block per
- *     system for pack, cells, pair list and z order; one launch per phase
- *     (pair forces; long-range preparation, chunk totals, their scan, the
- *     k-sliced force pass and the final sum; the gather) over a (system,
- *     tile) work list.  Every system must take the small-system kernels in
+ *   QEM_BATCH_FUSED: 17 or 18 launches for the whole batch, each over all
+ *     systems -- pack and z order over (system, particle tile) work lists (a
+ *     tile pass and one or two merge passes); cells and pair list in eight
+ *     phases over cell, particle and pair tiles (their scans one block per
+ *     system); then one launch per phase (pair forces; long-range
+ *     preparation, chunk totals, their scan, the k-sliced force pass and the
+ *     final sum; the gather) over a (system, tile) work list.  Every system must take the small-system kernels in
  *     FP32+fix: N <= 8192, fewer than two particles per cell on average (or
  *     fewer than 3 cells along x or y), no equal-z tie mode, no shard, and
  *     terms with both QEM_TERM_SHORT and QEM_TERM_LONG.  Each system's forces
@@ -351,17 +353,23 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  *   k-set for the whole run.
  * qem_batch_autotune: times the graph-replayed force evaluation for stream
  *   pool widths 1, 2, 4, ... up to min(B, 128) and, when the batch can run
- *   fused, for the fused tilings (k-slices per system of the force pass: the
- *   handle's own count or at most 1, 2, 4; work lists in batch order or
- *   largest system first), and keeps the fastest; returns the pool width (0
- *   when the fused phases won) and the time per batch evaluation (ms).
+ *   fused, for the fused tilings (chunk length 512, 256, 128 or 64; k-slices
+ *   per system of the force pass: the handle's own count or at most 2, 4;
+ *   work lists in batch order or largest system first), and keeps the
+ *   fastest; returns the pool width (0 when the fused phases won) and the
+ *   time per batch evaluation (ms).
  * qem_batch_set_mode: mode (QEM_BATCH_AUTO, _FUSED or _POOL), ks (k-slices
- *   per system of the fused force pass, 0 = each handle's own) and order (0
- *   batch order, 1 largest system first) of the fused work lists.  A fused
- *   request for a batch that does not qualify fails at qem_batch_forces.
+ *   per system of the fused force pass, 0 = each handle's own), order (0
+ *   batch order, 1 largest system first) of the fused work lists and chunk
+ *   (particles per z-ordered chunk of the fused k-space passes: 0 = 512, or
+ *   a divisor of 512 of at least 32; shorter chunks keep sparse slabs on the
+ *   force pass's one-walk path, which needs max(k) x the chunk's z extent
+ *   <= 1).  A fused request for a batch that does not qualify fails at
+ *   qem_batch_forces.
  * qem_batch_get_mode: the way evaluations run now (QEM_BATCH_FUSED or
- *   QEM_BATCH_POOL), ks, order, the kernel launches per fused evaluation
- *   (-1 on the pool) and, when the batch cannot run fused, why (else "").
+ *   QEM_BATCH_POOL), ks, order, chunk, the kernel launches per fused
+ *   evaluation (-1 on the pool) and, when the batch cannot run fused, why
+ *   (else "").
  * qem_batch_set_thermostat: the Andersen thermostat of the MD steps (Molly's
  *   AndersenThermostat(temp, coupling_const) in test/QEM_test.jl:53-56;
  *   python_lib Andersen.py:8-22): after each step every particle, with
@@ -388,9 +396,9 @@ qem_status qem_batch_thermostat_step(const qem_batch *b, uint64_t *step);
 #define QEM_BATCH_AUTO 0
 #define QEM_BATCH_FUSED 1
 #define QEM_BATCH_POOL 2
-qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order);
-qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *launches,
-                              const char **why);
+qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order, int32_t chunk);
+qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *chunk,
+                              int32_t *launches, const char **why);
 
 /* Library identity (version string and the compiled CUDA architecture). */
 const char *qem_version(void);

@@ -116,8 +116,8 @@ def load(build: bool = False):
         "qem_batch_md": (C.c_int32, [vp, C.c_int32, C.c_double, vp, vp, vp, vp, C.c_uint32, vp]),
         "qem_batch_autotune": (C.c_int32, [vp, vp, vp, vp, C.c_uint32, vp, ip, dp]),
         "qem_batch_set_thermostat": (C.c_int32, [vp, C.c_double, C.c_double, C.c_uint64]),
-        "qem_batch_set_mode": (C.c_int32, [vp, C.c_int32, C.c_int32, C.c_int32]),
-        "qem_batch_get_mode": (C.c_int32, [vp, ip, ip, ip, ip, C.POINTER(C.c_char_p)]),
+        "qem_batch_set_mode": (C.c_int32, [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "qem_batch_get_mode": (C.c_int32, [vp, ip, ip, ip, ip, ip, C.POINTER(C.c_char_p)]),
         "qem_batch_thermostat_step": (C.c_int32, [vp, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():

@@ -421,19 +421,20 @@ class Batch:
                                                  self._stream(xyz, stream), C.byref(w), C.byref(ms)))
         return w.value, ms.value
 
-    def set_mode(self, mode=L.QEM_BATCH_AUTO, ks=0, order=0):
+    def set_mode(self, mode=L.QEM_BATCH_AUTO, ks=0, order=0, chunk=0):
         """QEM_BATCH_AUTO / _FUSED / _POOL; ks: k-slices per system of the fused force
-        pass (0: each engine's own); order: 0 batch order, 1 largest system first."""
-        self._check(self._lib.qem_batch_set_mode(self._b, int(mode), int(ks), int(order)))
+        pass (0: each engine's own); order: 0 batch order, 1 largest system first;
+        chunk: particles per chunk of the fused k-space passes (0: 512)."""
+        self._check(self._lib.qem_batch_set_mode(self._b, int(mode), int(ks), int(order), int(chunk)))
 
     def mode(self):
-        """dict(mode, ks, order, launches, why) of the way evaluations run now."""
-        m, ks, order, n = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        """dict(mode, ks, order, chunk, launches, why) of the way evaluations run now."""
+        m, ks, order, ch, n = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         why = C.c_char_p()
-        self._check(self._lib.qem_batch_get_mode(self._b, C.byref(m), C.byref(ks), C.byref(order), C.byref(n),
-                                                 C.byref(why)))
+        self._check(self._lib.qem_batch_get_mode(self._b, C.byref(m), C.byref(ks), C.byref(order), C.byref(ch),
+                                                 C.byref(n), C.byref(why)))
         name = {L.QEM_BATCH_FUSED: "fused", L.QEM_BATCH_POOL: "pool"}.get(m.value, m.value)
-        return dict(mode=name, ks=ks.value, order=order.value, launches=n.value,
+        return dict(mode=name, ks=ks.value, order=order.value, chunk=ch.value, launches=n.value,
                     why=(why.value or b"").decode())
 
 

@@ -9,13 +9,15 @@
 //
 // Two ways to run a batch evaluation:
 //  * fused phases (every system small enough for the one-block kernels, in
-//    FP32+fix): eight launches for the whole batch.  One block per system
-//    packs, bins, lists pairs and z-sorts; then the pair phase and, on a
-//    second stream, the long-range phases (preparation, chunk totals, their
-//    scan, the k-sliced force pass, the final sum) each run one launch over a
-//    (system, tile) work list; the gather joins them.  The blocks run the
-//    single-system kernels' per-block code on the system's own buffers, so a
-//    system's forces are those of its own qem_forces call.
+//    FP32+fix): 17 or 18 launches for the whole batch.  Pack and the
+//    rank-sorted z tiles run over (system, particle tile) work lists; then,
+//    on a second stream, the z merge passes and the long-range phases
+//    (preparation one block per system, chunk totals, their scan, the
+//    k-sliced force pass, the final sum), and on the first stream the cells
+//    and the pair list (eight phases over cell, particle and pair tiles, the
+//    scans one block per system) and the pair forces; the gather joins them.  The blocks run the single-system kernels' per-block code on the
+//    system's own buffers, so a system's forces are those of its own
+//    qem_forces call.
 //  * per-system pipelines forked over a pool of streams (any batch).
 // The autotuner times the pool widths and the fused tilings (k-slices per
 // system of the force pass, work-list order) and keeps the fastest.
@@ -117,6 +119,7 @@ struct qem_batch {
     int mode_cur = QEM_BATCH_FUSED;     // in use when the request is auto (the autotuner's choice)
     int fks = 0;                        // k-slices per system of the fused force pass (0: each handle's own)
     int forder = 0;                     // work-list order: 0 batch order, 1 largest system first
+    int flch = 0;                       // chunk length of the fused k-space passes (0: qem_long_chunk())
     bool ftab_ok = false;               // device tables built for the current buffers and terms
     std::string fwhy;                   // why the batch cannot run fused (empty: it can)
     std::vector<uint64_t> fstate;       // per-handle state the tables were built for
@@ -126,7 +129,9 @@ struct qem_batch {
     ShortConsts *d_sc = nullptr;
     BatchWork *d_work = nullptr;
     size_t work_cap = 0;
-    int nw[5] = {0, 0, 0, 0, 0}, wo[5] = {0, 0, 0, 0, 0};  // pairs, particle tiles, totals, scan, force pass
+    // work lists: pairs, particle tiles, totals, scan, force pass, merge passes 0 and 1, cell tiles
+    int nw[8] = {0, 0, 0, 0, 0, 0, 0, 0}, wo[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int launches = 0;                   // kernels per fused evaluation
     cudaStream_t s_long = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
@@ -173,7 +178,7 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
     std::vector<ShortConsts> sc(b->B);
     for (int i = 0; i < b->B; i++) {
         const char *why = nullptr;
-        const qem_status st = qem_handle_batch_sys(b->h[i], b->N[i], b->fks, &sys[i], &sc[i], &why);
+        const qem_status st = qem_handle_batch_sys(b->h[i], b->N[i], b->fks, b->flch, &sys[i], &sc[i], &why);
         if (st == QEM_ERR_ARG && why) {
             b->fwhy = "system " + std::to_string(i) + ": " + why;
             return QEM_OK;
@@ -189,7 +194,9 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
     std::vector<BatchWork> w;
     const int tp = qem_batch_pair_tile(), tpart = qem_batch_particle_tile(), tt = qem_batch_ltot_tile();
     const int ts = qem_batch_lscan_tile(), tf = qem_batch_lforce_tile();
-    for (int ph = 0; ph < 5; ph++) {
+    if (tp != 256 || tpart != 256)
+        return bfail(b, QEM_ERR_ARG, "the list phases take pair and particle tiles of 256");
+    for (int ph = 0; ph < 8; ph++) {
         b->wo[ph] = (int)w.size();
         for (int s : order) {
             const BatchSys &d = sys[s];
@@ -205,9 +212,16 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
             if (ph == 4)  // also with P = 0: the force pass writes the zero slices the final pass sums
                 for (int c = 0; c < d.nch; c++)
                     for (int y = 0; y < nblk(d.ks, tf); y++) w.push_back({s, c, y, 0});
+            if ((ph == 5 || ph == 6) && qem_batch_zsort_passes(d.N) > ph - 5)
+                for (int t = 0; t < nblk(d.N, 256); t++) w.push_back({s, t, 0, 0});
+            if (ph == 7)
+                for (int t = 0; t < nblk(d.ncell, 256); t++) w.push_back({s, t, 0, 0});
         }
         b->nw[ph] = (int)w.size() - b->wo[ph];
     }
+    for (int i = 0; i < b->B; i++)
+        if (qem_batch_zsort_passes(b->N[i]) > 2) return bfail(b, QEM_ERR_ARG, "more z-merge passes than two");
+    b->launches = 16 + (b->nw[5] > 0) + (b->nw[6] > 0);
     if (!b->d_sys) {
         BCU(cudaMalloc(&b->d_sys, sizeof(BatchSys) * b->B));
         BCU(cudaMalloc(&b->d_sc, sizeof(ShortConsts) * b->B));
@@ -234,15 +248,19 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
 static qem_status enqueue_fused(qem_batch *b, const double *xyz, const double *q, double *F, cudaStream_t s)
 {
     const BatchWork *w = b->d_work;
-    BCU(qem_launch_batch_setup(b->B, b->d_sys, xyz, q, s));
+    BCU(qem_launch_batch_pack_ztile(b->nw[1], w + b->wo[1], b->d_sys, xyz, q, s));
     BCU(cudaEventRecord(b->ev_fork, s));
     BCU(cudaStreamWaitEvent(b->s_long, b->ev_fork, 0));
+    for (int pass = 0; pass < 2; pass++)
+        BCU(qem_launch_batch_zmerge(b->nw[5 + pass], w + b->wo[5 + pass], b->d_sys, pass, b->s_long));
     BCU(qem_launch_batch_lprep(b->B, b->d_sys, b->s_long));
     BCU(qem_launch_batch_ltot(b->nw[2], w + b->wo[2], b->d_sys, b->s_long));
     BCU(qem_launch_batch_lscan(b->nw[3], w + b->wo[3], b->d_sys, b->s_long));
     BCU(qem_launch_batch_lforce(b->nw[4], w + b->wo[4], b->d_sys, b->s_long));
     BCU(qem_launch_batch_lfinal(b->nw[1], w + b->wo[1], b->d_sys, b->s_long));
     BCU(cudaEventRecord(b->ev_join, b->s_long));
+    BCU(qem_launch_batch_lists(b->B, w + b->wo[7], b->nw[7], w + b->wo[1], b->nw[1], w + b->wo[0], b->nw[0],
+                               b->d_sys, s));
     BCU(qem_launch_batch_pairs(b->nw[0], w + b->wo[0], b->d_sys, b->d_sc, s));
     BCU(cudaStreamWaitEvent(s, b->ev_join, 0));
     BCU(qem_launch_batch_gather(b->nw[1], w + b->wo[1], b->d_sys, b->d_sc, b->do_lj, F, s));
@@ -552,19 +570,20 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
     // of the force pass (the handle's own count, or at most 1, 2, 4) x
     // work-list order (batch order, largest system first)
     struct Cand {
-        int fused, w, ks, order;
+        int fused, w, ks, order, lch;
     };
     std::vector<Cand> cand;
     if (b->mode_req != QEM_BATCH_FUSED) {
         const int wmax = (int)b->pool.size();
-        for (int w = 1; w < wmax; w *= 2) cand.push_back({0, w, 0, 0});
-        cand.push_back({0, wmax, 0, 0});
+        for (int w = 1; w < wmax; w *= 2) cand.push_back({0, w, 0, 0, 0});
+        cand.push_back({0, wmax, 0, 0, 0});
     }
     const bool fusable = b->mode_req != QEM_BATCH_POOL && b->fwhy.empty();
     if (fusable)
-        for (int ks : {0, 1, 2, 4})
-            for (int order : {0, 1}) cand.push_back({1, 0, ks, order});
-    const int mode0 = b->mode_req, W0 = b->W, ks0 = b->fks, order0 = b->forder;
+        for (int lch : {0, 256, 128, 64})
+            for (int ks : {0, 2, 4})
+                for (int order : {0, 1}) cand.push_back({1, 0, ks, order, lch});
+    const int mode0 = b->mode_req, W0 = b->W, ks0 = b->fks, order0 = b->forder, lch0 = b->flch;
     cudaEvent_t t0, t1;
     BCU(cudaEventCreate(&t0));
     BCU(cudaEventCreate(&t1));
@@ -576,6 +595,7 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
         if (k.fused) {
             b->fks = k.ks;
             b->forder = k.order;
+            b->flch = k.lch;
             st = build_fused(b, terms);
         } else {
             b->W = k.w;
@@ -593,11 +613,13 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
     b->W = W0;
     b->fks = ks0;
     b->forder = order0;
+    b->flch = lch0;
     if (st == QEM_OK && best >= 0) {
         const Cand &k = cand[best];
         if (k.fused) {
             b->fks = k.ks;
             b->forder = k.order;
+            b->flch = k.lch;
             b->mode_cur = QEM_BATCH_FUSED;
         } else {
             b->W = k.w;
@@ -615,34 +637,38 @@ qem_status qem_batch_autotune(qem_batch *b, const double *xyz, const double *q, 
     return qem_batch_check(b, stream);
 }
 
-qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order)
+qem_status qem_batch_set_mode(qem_batch *b, int32_t mode, int32_t ks, int32_t order, int32_t chunk)
 {
     if (!b) return QEM_ERR_ARG;
     if (mode != QEM_BATCH_AUTO && mode != QEM_BATCH_FUSED && mode != QEM_BATCH_POOL)
         return bfail(b, QEM_ERR_ARG, "mode must be QEM_BATCH_AUTO, QEM_BATCH_FUSED or QEM_BATCH_POOL");
     if (ks < 0 || ks > QEM_LONG_MAX_KS || (order != 0 && order != 1))
         return bfail(b, QEM_ERR_ARG, "ks must be in 0 .. 64 and order 0 or 1");
+    if (chunk != 0 && (chunk < 32 || qem_long_chunk() % chunk != 0))
+        return bfail(b, QEM_ERR_ARG, "chunk must be 0 or a divisor of 512 of at least 32");
     BCU(cudaSetDevice(b->device));
     BCU(cudaDeviceSynchronize());
     b->mode_req = mode;
     b->mode_cur = mode == QEM_BATCH_POOL ? QEM_BATCH_POOL : QEM_BATCH_FUSED;
     b->fks = ks;
     b->forder = order;
+    b->flch = chunk;
     b->ftab_ok = false;  // rebuilt by the next qem_batch_forces
     drop_md_graph(b);
     b->err.clear();
     return QEM_OK;
 }
 
-qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *launches,
-                              const char **why)
+qem_status qem_batch_get_mode(const qem_batch *b, int32_t *mode, int32_t *ks, int32_t *order, int32_t *chunk,
+                              int32_t *launches, const char **why)
 {
     if (!b) return QEM_ERR_ARG;
     const bool fused = use_fused(b);
     if (mode) *mode = fused ? QEM_BATCH_FUSED : QEM_BATCH_POOL;
     if (ks) *ks = b->fks;
     if (order) *order = b->forder;
-    if (launches) *launches = fused ? 8 : -1;
+    if (chunk) *chunk = b->flch > 0 ? b->flch : qem_long_chunk();
+    if (launches) *launches = fused ? b->launches : -1;
     if (why) *why = b->fwhy.c_str();
     return QEM_OK;
 }

@@ -19,9 +19,10 @@ constexpr int SCAN_BLOCK = 1024;
 // ---------------------------------------------------------------------------
 // pack: AoS coordinates + charges -> double4, 2-D cell index, finiteness check
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void pack_one(int i, const double *__restrict__ xyz, const double *__restrict__ q,
-                                         double4 *__restrict__ pos, int *__restrict__ cell, const CellGeom &g,
-                                         unsigned *status)
+// returns the z it stored (0 for non-finite input)
+__device__ __forceinline__ double pack_one(int i, const double *__restrict__ xyz, const double *__restrict__ q,
+                                           double4 *__restrict__ pos, int *__restrict__ cell, const CellGeom &g,
+                                           unsigned *status)
 {
     double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2], qq = q[i];
     bool ok = isfinite(x) && isfinite(y) && isfinite(z) && isfinite(qq);
@@ -36,6 +37,7 @@ __device__ __forceinline__ void pack_one(int i, const double *__restrict__ xyz, 
     cx = min(max(cx, 0), g.ncx - 1);
     cy = min(max(cy, 0), g.ncy - 1);
     cell[i] = cx * g.ncy + cy;
+    return z;
 }
 
 __global__ void k_pack(int N, const double *__restrict__ xyz, const double *__restrict__ q, double4 *__restrict__ pos,
@@ -268,6 +270,8 @@ __global__ void k_cell_sort(int ncell, const int *__restrict__ start, int *__res
 // build (the order inside a cell does not depend on the scatter).
 constexpr int CELLS_SMALL = 8192;
 
+// SORT = false stops after the scatter (cstart and the unsorted cell lists)
+template <bool SORT = true>
 __device__ __forceinline__ void cells_small_block(int N, int ncell, const int *__restrict__ cell,
                                                   const double4 *__restrict__ pos, int *__restrict__ cstart,
                                                   int *__restrict__ clist, int *__restrict__ pos_of,
@@ -315,6 +319,7 @@ __device__ __forceinline__ void cells_small_block(int N, int ncell, const int *_
     __syncthreads();
     for (int i = tid; i < N; i += 1024) clist[atomicAdd(&cnt[cell[i]], 1)] = i;
     __syncthreads();
+    if (!SORT) return;
     for (int c = w; c < ncell; c += 32) {
         const int cb = cstart[c], ce = cstart[c + 1];
         warp_sort_segment<int>(clist, cb, ce, lane, 0x7fffffff);
@@ -847,64 +852,165 @@ __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const
     if (p < N) zmerge_one<REV>(p, N, width, key, idx, key_out, idx_out);
 }
 
-// The z order of one small system by the calling block of 1024 threads:
-// the rank-sorted tiles of ZTILE keys (1024 / ZTILE tiles at a time) and the
-// ZWAY-way merges of k_ztile / k_zmerge, with block barriers between the
-// passes, ending in (zkey, zperm).  (z, index) is a total order, so the
-// permutation is the one the multi-kernel sort gives.
-__device__ __forceinline__ void zsort_block(int N, const double4 *__restrict__ pos, int *zperm, int *ztmp,
-                                            double *zkey, double *zkey2)
+// number of ZWAY-way merge passes after the tile pass for N keys
+__host__ __device__ inline int zsort_pass_count(int N)
 {
-    __shared__ double sk[1024];
-    __shared__ int si[1024];
     int passes = 0;
     for (int64_t w = ZTILE; w < N; w *= ZWAY) passes++;
-    double *ka = (passes & 1) ? zkey2 : zkey, *kb = (passes & 1) ? zkey : zkey2;
-    int *ia = (passes & 1) ? ztmp : zperm, *ib = (passes & 1) ? zperm : ztmp;
-    const int tid = threadIdx.x, t0 = (tid / ZTILE) * ZTILE;
-    for (int base = 0; base < N; base += 1024) {
-        const int i = base + tid;
-        double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
-        int me = 0x7fffffff;
-        if (i < N) {
-            z = pos[i].z;
-            me = i;
-        }
-        sk[tid] = z;
-        si[tid] = me;
-        __syncthreads();
-        int rank = 0;
-#pragma unroll 8
-        for (int j = 0; j < ZTILE; j++) rank += zless<false>(sk[t0 + j], si[t0 + j], z, me) ? 1 : 0;
-        if (i < N) {
-            ka[base + t0 + rank] = z;
-            ia[base + t0 + rank] = me;
-        }
-        __syncthreads();
+    return passes;
+}
+
+// ---------------------------------------------------------------------------
+// fused batches: the small-system binning and z order over all systems
+// ---------------------------------------------------------------------------
+// (system, particle tile of ZTILE): pack the tile's particles and rank-sort
+// its (z, index) keys -- k_pack and k_ztile -- into the buffer the system's
+// first pass reads (so that its last pass ends in zkey, zperm)
+__global__ void __launch_bounds__(ZTILE) k_batch_pack_ztile(const BatchWork *__restrict__ wl,
+                                                            const BatchSys *__restrict__ ds,
+                                                            const double *__restrict__ xyz,
+                                                            const double *__restrict__ q)
+{
+    __shared__ double sk[ZTILE];
+    __shared__ int si[ZTILE];
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int N = d.N, base = t.x * ZTILE, i = base + threadIdx.x;
+    double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
+    int me = 0x7fffffff;
+    if (i < N) {
+        z = pack_one(i, xyz + 3 * d.off, q + d.off, d.pos, d.cell, d.geom, d.status);
+        me = i;
     }
-    for (int64_t w = ZTILE; w < N; w *= ZWAY) {
-        for (int p = tid; p < N; p += 1024) zmerge_one<false>(p, N, (int)w, ka, ia, kb, ib);
-        __syncthreads();
-        double *tk = ka; ka = kb; kb = tk;
-        int *ti = ia; ia = ib; ib = ti;
+    sk[threadIdx.x] = z;
+    si[threadIdx.x] = me;
+    __syncthreads();
+    int rank = 0;
+#pragma unroll 8
+    for (int j = 0; j < ZTILE; j++) rank += zless<false>(sk[j], si[j], z, me) ? 1 : 0;
+    if (i < N) {
+        const bool odd = zsort_pass_count(N) & 1;
+        (odd ? d.zkey2 : d.zkey)[base + rank] = z;
+        (odd ? d.ztmp : d.zperm)[base + rank] = me;
     }
 }
 
-// Fused batches: pack, cells, pair list and z order of one small system per
-// block (the small-system kernels' code, in their order)
-__global__ void __launch_bounds__(1024) k_batch_setup(const BatchSys *__restrict__ ds, const double *__restrict__ xyz,
-                                                      const double *__restrict__ q)
+// (system, particle tile of 256): merge pass `pass` of the system's z order
+__global__ void __launch_bounds__(256) k_batch_zmerge(const BatchWork *__restrict__ wl,
+                                                      const BatchSys *__restrict__ ds, int pass)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int N = d.N, p = t.x * 256 + threadIdx.x;
+    const bool odd = ((zsort_pass_count(N) + pass) & 1) != 0;  // pass j reads what pass j - 1 wrote
+    int width = ZTILE;
+    for (int j = 0; j < pass; j++) width *= ZWAY;
+    if (p < N)
+        zmerge_one<false>(p, N, width, odd ? d.zkey2 : d.zkey, odd ? d.ztmp : d.zperm, odd ? d.zkey : d.zkey2,
+                          odd ? d.zperm : d.ztmp);
+}
+
+// The cells and the pair list of the small systems, as separate phases over
+// all systems (the steps of k_cells_small and k_pairs_small, so the lists
+// are the same): one block per system for the counting scatter into cells
+// and for the two scans; thread-per-cell and thread-per-owner tiles for the
+// rest, which keeps every thread's chain of dependent loads short.
+
+// one block per system: cell counts, their scan (cstart) and the scatter
+__global__ void __launch_bounds__(1024) k_batch_cells(const BatchSys *__restrict__ ds)
 {
     QEM_SHARED_COPY(BatchSys, d, ds + blockIdx.x);
-    for (int i = threadIdx.x; i < d.N; i += 1024)
-        pack_one(i, xyz + 3 * d.off, q + d.off, d.pos, d.cell, d.geom, d.status);
-    __syncthreads();
-    cells_small_block(d.N, d.ncell, d.cell, d.pos, d.cstart, d.clist, d.pos_of, d.pos_c);
-    __syncthreads();
-    pairs_small_block(d.N, d.pos_c, d.cell, d.cstart, d.clist, d.geom, d.rc2, d.pcount, d.poff, d.pairs, d.cap,
-                      d.in_cnt, d.in_fill, d.in_off, d.in_list, d.status);
-    __syncthreads();
-    zsort_block(d.N, d.pos, d.zperm, d.ztmp, d.zkey, d.zkey2);
+    cells_small_block<false>(d.N, d.ncell, d.cell, d.pos, d.cstart, d.clist, d.pos_of, d.pos_c);
+}
+
+// (system, tile of 256 cells): ascending index inside each cell (the cells
+// of these systems hold a few particles: insertion sort by one thread), the
+// inverse map and the positions in cell order
+__global__ void __launch_bounds__(256) k_batch_cell_sort(const BatchWork *__restrict__ wl,
+                                                         const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int c = t.x * 256 + threadIdx.x;
+    if (c >= d.ncell) return;
+    const int b = d.cstart[c], e = d.cstart[c + 1];
+    int *list = d.clist;
+    for (int s = b + 1; s < e; s++) {
+        const int v = list[s];
+        int u = s - 1;
+        while (u >= b && list[u] > v) {
+            list[u + 1] = list[u];
+            u--;
+        }
+        list[u + 1] = v;
+    }
+    for (int s = b; s < e; s++) {
+        const int i = list[s];
+        d.pos_of[i] = s;
+        d.pos_c[s] = d.pos[i];
+    }
+}
+
+// (system, tile of 256 cell-order slots): pair count of each owner (and the
+// incoming counters cleared)
+__global__ void __launch_bounds__(256) k_batch_pair_count(const BatchWork *__restrict__ wl,
+                                                          const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int s = t.x * 256 + threadIdx.x;
+    if (s >= d.N) return;
+    const CellGeom g = d.geom;
+    pairs_of_owner<false>(s, d.pos_c, d.cell, d.cstart, d.clist, g, d.rc2, d.pcount, nullptr, nullptr, 0, nullptr,
+                          nullptr);
+    d.in_cnt[s] = 0;
+    d.in_fill[s] = 0;
+}
+
+// one block per system: exclusive scan, pcount -> poff (WHICH = 0) or
+// in_cnt -> in_off (WHICH = 1); out[N] = total
+template <int WHICH>
+__global__ void __launch_bounds__(1024) k_batch_scan(const BatchSys *__restrict__ ds)
+{
+    __shared__ int64_t warp_tot[32];
+    const BatchSys &d = ds[blockIdx.x];
+    block_scan_small<int, int64_t>(WHICH == 0 ? d.pcount : d.in_cnt, WHICH == 0 ? d.poff : d.in_off, d.N, warp_tot);
+}
+
+// (system, tile of 256 slots): the owners' pairs into their poff ranges
+__global__ void __launch_bounds__(256) k_batch_pair_fill(const BatchWork *__restrict__ wl,
+                                                         const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int s = t.x * 256 + threadIdx.x;
+    if (s >= d.N) return;
+    const CellGeom g = d.geom;
+    pairs_of_owner<true>(s, d.pos_c, d.cell, d.cstart, d.clist, g, d.rc2, nullptr, d.poff, d.pairs, d.cap, d.in_cnt,
+                         d.status);
+}
+
+// (system, tile of 256 pairs): each pair's entry in its second particle's
+// incoming list (any slot order; the lists are sorted next)
+__global__ void __launch_bounds__(256) k_batch_in_scatter(const BatchWork *__restrict__ wl,
+                                                          const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int64_t p = (int64_t)t.x * 256 + threadIdx.x;
+    if (p >= min(d.poff[d.N], d.cap)) return;
+    const int j = d.pairs[p].y;
+    d.in_list[d.in_off[j] + atomicAdd(&d.in_fill[j], 1)] = (int)p;
+}
+
+// (system, tile of 256 particles): incoming lists in ascending pair order
+__global__ void __launch_bounds__(256) k_batch_in_sort(const BatchWork *__restrict__ wl,
+                                                       const BatchSys *__restrict__ ds)
+{
+    const BatchWork t = wl[blockIdx.x];
+    const BatchSys &d = ds[t.s];
+    const int i = t.x * 256 + threadIdx.x;
+    if (i < d.N) sort_incoming(i, d.in_off, d.in_list);
 }
 
 inline int nblk(int64_t n, int b) { return (int)((n + b - 1) / b); }
@@ -933,12 +1039,7 @@ size_t qem_scan_tmp_bytes(int n) { return sizeof(double) * (size_t)(nblk(n, SCAN
 int qem_scan_launches(int n) { return n <= SCAN_SMALL_MAX_INT ? 1 : 3; }
 int qem_scan_f64_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
 
-static int zsort_passes(int N)
-{
-    int passes = 0;
-    for (int64_t w = ZTILE; w < N; w *= ZWAY) passes++;
-    return passes;
-}
+static int zsort_passes(int N) { return zsort_pass_count(N); }
 
 int qem_zsort_launches(int N) { return N <= 0 ? 0 : 1 + zsort_passes(N); }
 
@@ -973,10 +1074,36 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
 
 bool qem_cells_small(int N, int ncell) { return N <= CELLS_SMALL && ncell <= CELLS_SMALL; }
 
-cudaError_t qem_launch_batch_setup(int B, const BatchSys *d, const double *xyz, const double *q, cudaStream_t s)
+int qem_batch_zsort_passes(int N) { return zsort_pass_count(N); }
+
+cudaError_t qem_launch_batch_pack_ztile(int nw, const BatchWork *w, const BatchSys *d, const double *xyz,
+                                        const double *q, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    static_assert(ZTILE == 256, "particle tiles of the fused phases are ZTILE long");
+    k_batch_pack_ztile<<<nw, ZTILE, 0, s>>>(w, d, xyz, q);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_batch_zmerge(int nw, const BatchWork *w, const BatchSys *d, int pass, cudaStream_t s)
+{
+    if (nw <= 0) return cudaSuccess;
+    k_batch_zmerge<<<nw, 256, 0, s>>>(w, d, pass);
+    return cudaGetLastError();
+}
+
+cudaError_t qem_launch_batch_lists(int B, const BatchWork *cells, int ncells, const BatchWork *parts, int nparts,
+                                   const BatchWork *pairs, int npairs, const BatchSys *d, cudaStream_t s)
 {
     if (B <= 0) return cudaSuccess;
-    k_batch_setup<<<B, 1024, 0, s>>>(d, xyz, q);
+    k_batch_cells<<<B, 1024, 0, s>>>(d);
+    if (ncells > 0) k_batch_cell_sort<<<ncells, 256, 0, s>>>(cells, d);
+    if (nparts > 0) k_batch_pair_count<<<nparts, 256, 0, s>>>(parts, d);
+    k_batch_scan<0><<<B, 1024, 0, s>>>(d);
+    if (nparts > 0) k_batch_pair_fill<<<nparts, 256, 0, s>>>(parts, d);
+    k_batch_scan<1><<<B, 1024, 0, s>>>(d);
+    if (npairs > 0) k_batch_in_scatter<<<npairs, 256, 0, s>>>(pairs, d);
+    if (nparts > 0) k_batch_in_sort<<<nparts, 256, 0, s>>>(parts, d);
     return cudaGetLastError();
 }
 

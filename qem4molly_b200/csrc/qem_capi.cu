@@ -1696,7 +1696,8 @@ uint64_t qem_handle_state(const qem_handle *h)
 // The arguments run_once gives the small-system kernels, collected for one
 // system of a fused batch: the same buffers, the same k-slice count (unless
 // ks > 0 picks fewer) and the same per-k constants.
-qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, ShortConsts *sc, const char **why)
+qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys *d, ShortConsts *sc,
+                                const char **why)
 {
     auto no = [&](const char *m) {
         if (why) *why = m;
@@ -1719,8 +1720,12 @@ qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, Short
     if (P > 0 && !draw && !h->kset_lattice) return no("k-set rows off the lattice");
     if (P > 0 && (h->kin_lo != 0 || h->kin_hi != P)) return no("the k rows on the device are not the whole set");
     const int LCH = qem_long_chunk();
-    const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = nbS;
+    if (lch <= 0) lch = LCH;
+    if (lch < 32 || LCH % lch != 0) return no("chunk length must divide qem_long_chunk() and be >= 32");
+    const int nch = (N + lch - 1) / lch, nbS = (N + 255) / 256, nb0 = nbS;
     const int ks_own = qem_long_ksplit(nch, std::max(P > 0 ? P : h->p.rbe_p, 1), h->long_max_ks, h->p.precision);
+    // energy partials (the scan writes its per-k split terms there) for this chunking
+    CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks_own * nch + nb0 + std::max(P, h->p.rbe_p) + 8)));
     LongBuffers b;
     const qem_status ls = long_buffers(h, N, P, nch, ks_own, ptr<double>(h->Epart), nbS, nb0, b);
     if (ls != QEM_OK) return ls;
@@ -1740,6 +1745,7 @@ qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, Short
     e.ncell = h->ncell;
     e.P = P;
     e.nch = nch;
+    e.lch = lch;
     e.ks = b.ks;
     e.cap = h->pair_cap;
     e.Flong = ptr<double>(h->Flong);

@@ -365,10 +365,11 @@ const char *qem_handle_error(const qem_handle *h);
 // single-system launches of the small-system path take.  A phase's blocks
 // read (system, x, y) from a work list built on the host and run the same
 // per-block code as the single-system kernels; the one-block kernels of a
-// small system (pack + cells + pair list + z order, and the long-range
-// preparation) run as one block per system.
+// small system (cells + pair list, and the long-range preparation) run as
+// one block per system.
 struct BatchSys {
     int N, ncell, P, nch, ks;
+    int lch;                  // particles per chunk of the k-space passes
     int64_t cap;              // pair capacity
     int64_t off;              // first particle of the system in the batch arrays
     double *Flong;            // long-range forces (handle buffer), added by the gather
@@ -414,7 +415,18 @@ int qem_batch_particle_tile(void);
 int qem_batch_ltot_tile(void);
 int qem_batch_lscan_tile(void);
 int qem_batch_lforce_tile(void);
-cudaError_t qem_launch_batch_setup(int B, const BatchSys *d, const double *xyz, const double *q, cudaStream_t s);
+// z order: pack + rank-sorted tiles over particle tiles, then merge passes
+// 0, 1, .. over the particle tiles of the systems with that many passes
+int qem_batch_zsort_passes(int N);
+cudaError_t qem_launch_batch_pack_ztile(int nw, const BatchWork *w, const BatchSys *d, const double *xyz,
+                                        const double *q, cudaStream_t s);
+cudaError_t qem_launch_batch_zmerge(int nw, const BatchWork *w, const BatchSys *d, int pass, cudaStream_t s);
+// cells and pair list: eight launches (counting scatter into cells and the
+// two scans one block per system; the in-cell sort over tiles of 256 cells,
+// the owners' count and fill passes and the incoming sort over particle
+// tiles, the incoming scatter over pair tiles of 256)
+cudaError_t qem_launch_batch_lists(int B, const BatchWork *cells, int ncells, const BatchWork *parts, int nparts,
+                                   const BatchWork *pairs, int npairs, const BatchSys *d, cudaStream_t s);
 cudaError_t qem_launch_batch_lprep(int B, const BatchSys *d, cudaStream_t s);
 cudaError_t qem_launch_batch_ltot(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
 cudaError_t qem_launch_batch_lscan(int nw, const BatchWork *w, const BatchSys *d, cudaStream_t s);
@@ -425,11 +437,14 @@ cudaError_t qem_launch_batch_pairs(int nw, const BatchWork *w, const BatchSys *d
 cudaError_t qem_launch_batch_gather(int nw, const BatchWork *w, const BatchSys *d, const ShortConsts *sc, int do_lj,
                                     double *F, cudaStream_t s);
 // fills one system's entry (qem_capi.cu; off is left 0) after a synchronous
-// call of the same size; ks <= 0 keeps the handle's own k-slice count.
+// call of the same size; ks <= 0 keeps the handle's own k-slice count, lch
+// (a divisor of qem_long_chunk(), 32 or more; 0: qem_long_chunk()) is the
+// chunk length of the k-space passes.
 // Returns QEM_ERR_ARG with the reason in *why when the system does not take
 // the small-system kernels in FP32+fix (the batch then keeps per-system
 // pipelines).
-qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, BatchSys *d, ShortConsts *sc, const char **why);
+qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys *d, ShortConsts *sc,
+                                const char **why);
 // changes whenever a buffer of any handle is reallocated or this handle's
 // k-set, shard or pair capacity changes
 uint64_t qem_handle_state(const qem_handle *h);

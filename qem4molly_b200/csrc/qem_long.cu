@@ -540,11 +540,13 @@ constexpr float THIN = 1.0f;    // largest k * (chunk z extent) of the one-walk 
 
 // chunk totals: lane k sums u = q e^{k (z-h)} e^{i k.rho} and v = q e^{-k (z-h)}
 // e^{i k.rho} over the chunk, in FP32 over 16 particles at a time, in FP64 across
-__device__ __forceinline__ void ltot_lk_tile(int c, int kb, int N, int P, int nch, const uint4 *__restrict__ zp,
-                                             const KConst *__restrict__ kc, double *__restrict__ tot)
+// lch: particles per chunk (LCH, or a shorter chunk of a fused batch)
+__device__ __forceinline__ void ltot_lk_tile(int c, int kb, int lch, int N, int P, int nch,
+                                             const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
+                                             double *__restrict__ tot)
 {
     constexpr float LOG2E = 1.4426950408889634f;
-    const int m0 = c * LCH, n = min(LCH, N - m0);
+    const int m0 = c * lch, n = min(lch, N - m0);
     const int k = kb * KTT + threadIdx.x;
     if (k >= P) return;
     const int mx = kc[k].mx, my = kc[k].my;
@@ -586,7 +588,7 @@ __device__ __forceinline__ void ltot_lk_tile(int c, int kb, int N, int P, int nc
 __global__ void __launch_bounds__(KTT) k_ltot_lk(int N, int P, int nch, const uint4 *__restrict__ zp,
                                                  const KConst *__restrict__ kc, double *__restrict__ tot)
 {
-    ltot_lk_tile(blockIdx.x, blockIdx.y, N, P, nch, zp, kc, tot);
+    ltot_lk_tile(blockIdx.x, blockIdx.y, LCH, N, P, nch, zp, kc, tot);
 }
 
 // one lane's k-vector for the force pass (zeros for lanes past P: no force)
@@ -715,7 +717,7 @@ __device__ __forceinline__ float lk_walk(const uint4 *__restrict__ pp, int n, co
 // k-groups of 32 vectors g = t, t + ks_n, ... and writes slice t of Fpart
 // (z order, the particle's q applied) and of the energy partials
 template <bool ENERGY>
-__device__ __forceinline__ void lforce_lk_tile(int c, int by, int N, int P, int nch, int ks_n,
+__device__ __forceinline__ void lforce_lk_tile(int c, int by, int lch, int N, int P, int nch, int ks_n,
                                                const uint4 *__restrict__ zp, const KConst *__restrict__ kc,
                                                const KForce<float> *__restrict__ kf, const float *__restrict__ off,
                                                const double *__restrict__ tot, double *__restrict__ Fpart,
@@ -726,7 +728,7 @@ __device__ __forceinline__ void lforce_lk_tile(int c, int by, int N, int P, int 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int t = by * KFW + w;
     if (t >= ks_n) return;  // whole warp; the kernel has no block barrier
-    const int m0 = c * LCH, n = min(LCH, N - m0);
+    const int m0 = c * lch, n = min(lch, N - m0);
     const uint4 *pp = zp + m0;
     const float dz = __uint_as_float(pp[n - 1].z) - __uint_as_float(pp[0].z);
     double *Fo = Fpart + ((int64_t)t * N + m0) * 3;
@@ -789,7 +791,7 @@ __global__ void __launch_bounds__(32 * KFW) k_lforce_lk(int N, int P, int nch, i
                                                         const float *__restrict__ off, const double *__restrict__ tot,
                                                         double *__restrict__ Fpart, double *__restrict__ Epart)
 {
-    lforce_lk_tile<ENERGY>(blockIdx.x, blockIdx.y, N, P, nch, ks_n, zp, kc, kf, off, tot, Fpart, Epart);
+    lforce_lk_tile<ENERGY>(blockIdx.x, blockIdx.y, LCH, N, P, nch, ks_n, zp, kc, kf, off, tot, Fpart, Epart);
 }
 
 // F[zperm[m]] += sum over k-slices (fixed order) + k = 0 term; ctr: the batch
@@ -840,7 +842,7 @@ __global__ void __launch_bounds__(KTT) k_batch_ltot(const BatchWork *__restrict_
 {
     const BatchWork t = wl[blockIdx.x];
     const BatchSys &d = ds[t.s];
-    ltot_lk_tile(t.x, t.y, d.N, d.P, d.nch, d.b.zP, d.b.kc, d.b.tot);
+    ltot_lk_tile(t.x, t.y, d.lch, d.N, d.P, d.nch, d.b.zP, d.b.kc, d.b.tot);
 }
 
 __global__ void __launch_bounds__(128) k_batch_lscan(const BatchWork *__restrict__ wl, const BatchSys *__restrict__ ds)
@@ -856,7 +858,7 @@ __global__ void __launch_bounds__(32 * KFW) k_batch_lforce(const BatchWork *__re
 {
     const BatchWork t = wl[blockIdx.x];
     const BatchSys &d = ds[t.s];
-    lforce_lk_tile<false>(t.x, t.y, d.N, d.P, d.nch, d.ks, d.b.zP, d.b.kc, (const KForce<float> *)d.b.kf,
+    lforce_lk_tile<false>(t.x, t.y, d.lch, d.N, d.P, d.nch, d.ks, d.b.zP, d.b.kc, (const KForce<float> *)d.b.kf,
                           (const float *)d.b.off, d.b.tot, d.b.Fpart, d.b.Epart);
 }
 

@@ -145,7 +145,8 @@ def main(argv=None):
     import torch
 
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--config", type=int, default=2, choices=(1, 2, 3, 5))
+    ap.add_argument("--config", type=int, default=2, choices=(1, 2, 3, 4, 5),
+                    help="4: the 256-slab batch in fused phases (FP32+fix, a fresh k batch per evaluation)")
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--precision", default="fp32", choices=("fp32", "fp64"))
     ap.add_argument("--N", type=int, default=None, help="particle count (configs 2, 3, 5)")
@@ -155,8 +156,28 @@ def main(argv=None):
                     help="gamma_1 = gamma_2 = e with Lz = 2 (regularised quadrature, python mode, FP64)")
     ap.add_argument("--backward", action="store_true",
                     help="time qem_backward (FP64) for loss = E + sum_i w_i . F_i, w ~ N(0, 1), instead")
+    ap.add_argument("--tiling", type=int, nargs=3, default=(4, 0, 64), metavar=("KS", "ORDER", "CHUNK"),
+                    help="config 4: fused tiling (k-slices per system, work-list order, chunk length)")
     a = ap.parse_args(argv)
     from . import _lib as L
+
+    if a.config == 4:
+        from .api import Batch
+
+        cfgs = config4()
+        engines = [engine_for(c, "fp32", mode_flags=L.QEM_RESAMPLE_KSET, seed=100 + i) for i, c in enumerate(cfgs)]
+        dev = torch.device("cuda", 0)
+        x = torch.tensor(np.concatenate([c["xyz"] for c in cfgs]), device=dev)
+        q = torch.tensor(np.concatenate([c["q"] for c in cfgs]), device=dev)
+        F = torch.empty_like(x)
+        b = Batch(engines, [c["N"] for c in cfgs])
+        b.set_mode(L.QEM_BATCH_FUSED, *a.tiling)
+        b.forces(x, q, F)  # synchronous sizing pass
+        for _ in range(a.evals):
+            b.forces(x, q, F)
+        b.check()
+        print(f"config 4: {len(cfgs)} slabs, {x.shape[0]} particles, {a.evals} fused evaluations, {b.mode()}")
+        return
 
     make = {1: config1, 2: config2, 3: config3, 5: config5}[a.config]
     cfg = make(N=a.N) if (a.N and a.config != 1) else make()

@@ -110,13 +110,13 @@ def _batch_F(b, x, q):
 
 def test_fused_batch_runs_fused_and_pool_agrees():
     """FP32+fix systems of the many-slab workload qualify for the fused phases
-    (eight launches per evaluation); forcing the stream pool gives the same
+    (17 or 18 launches per evaluation); forcing the stream pool gives the same
     forces (same per-block code, same k-slices) to FUSED_TOL."""
     cfgs, engines, N, x, q = _setup(16, "fp32")
     b = Batch(engines, N)
     Ff = _batch_F(b, x, q)
     m = b.mode()
-    assert m["mode"] == "fused" and m["launches"] == 8 and m["why"] == "", m
+    assert m["mode"] == "fused" and m["launches"] in (17, 18) and m["why"] == "", m
     b.set_mode(L.QEM_BATCH_POOL)
     Fp = _batch_F(b, x, q)
     assert b.mode()["mode"] == "pool"
@@ -125,15 +125,18 @@ def test_fused_batch_runs_fused_and_pool_agrees():
 
 def test_fused_batch_tilings_agree():
     """Other fused tilings (at most 1 or 2 k-slices per system, largest
-    system first) change only the order of the k-slice sums."""
+    system first) change only the order of the k-slice sums; shorter chunks
+    regroup the FP32 structure sums as well."""
     cfgs, engines, N, x, q = _setup(10, "fp32", seed=77)
     b = Batch(engines, N)
     ref = _batch_F(b, x, q)
-    for ks, order in ((1, 0), (2, 1), (0, 1)):
-        b.set_mode(L.QEM_BATCH_FUSED, ks, order)
+    for ks, order, chunk in ((1, 0, 0), (2, 1, 0), (0, 1, 0), (0, 0, 128), (2, 1, 64)):
+        b.set_mode(L.QEM_BATCH_FUSED, ks, order, chunk)
         F = _batch_F(b, x, q)
-        assert W.rel_err(F, ref)[0] <= 1e-12, (ks, order)
-        if ks == 0:
+        assert b.mode()["chunk"] == (chunk or 512)
+        # other chunks regroup the FP32 structure sums (FP32 rounding, ~1e-7)
+        assert W.rel_err(F, ref)[0] <= (1e-12 if chunk == 0 else 1e-6), (ks, order, chunk)
+        if ks == 0 and chunk == 0:
             assert np.array_equal(F, ref)
 
 
@@ -243,4 +246,4 @@ def test_fused_batch_autotune_keeps_results():
     assert ms > 0 and 0 <= w <= 16
     assert (b.mode()["mode"] == "fused") == (w == 0)
     F = _batch_F(b, x, q)
-    assert W.rel_err(F, ref)[0] <= 1e-12
+    assert W.rel_err(F, ref)[0] <= (1e-12 if b.mode()["chunk"] == 512 else 1e-6)
