@@ -151,8 +151,23 @@ __global__ void __launch_bounds__(ADJ_BLOCK, QEM_ADJ_MINB) k_short_pair_adj(cons
                                                                double4 *__restrict__ RA, const ShortConsts c)
 {
     typedef Dual<6> D6;
+    __shared__ int hist[QEM_RHO_BINS];
+    __shared__ int sidx[ADJ_BLOCK];
     const int64_t Np = min(*np, cap);
-    const int64_t p = (int64_t)blockIdx.x * ADJ_BLOCK + threadIdx.x;
+    if ((int64_t)blockIdx.x * ADJ_BLOCK >= Np) return;  // whole block: before any barrier
+    // the block's pairs grouped by rho^2, as in the forward pair kernel, so
+    // that a warp's lanes take the same branches of the Bessel functions
+    int bin = QEM_RHO_BINS - 1;
+    {
+        const int64_t p0 = (int64_t)blockIdx.x * ADJ_BLOCK + threadIdx.x;
+        if (p0 < Np) {
+            const int2 ij = pairs[p0];
+            const double4 a = pos[ij.x], b = pos[ij.y];
+            const double dx = min_image(a.x - b.x, c.Lx, c.invLx), dy = min_image(a.y - b.y, c.Ly, c.invLy);
+            bin = min(QEM_RHO_BINS - 1, (int)((dx * dx + dy * dy) * c.bins_per_rc2));
+        }
+    }
+    const int64_t p = (int64_t)blockIdx.x * ADJ_BLOCK + group_by_bin<QEM_RHO_BINS>(bin, hist, sidx);
     if (p >= Np) return;
     const int2 oo = pairs[p];
     const bool owner_is_i = oo.x < oo.y;

@@ -2,6 +2,7 @@
 // validation, device scratch, k-set sampling and the per-call orchestration of
 // the binning, short-range and long-range kernels.
 #include <algorithm>
+#include <functional>
 #include <cstddef>
 #include <atomic>
 #include <cmath>
@@ -378,7 +379,7 @@ static void build_consts(qem_handle *h)
     c.f_2Lz = (float)c.twoLz;
     c.f_g12 = (float)c.g12;
     c.f_omg12 = (float)c.one_minus_g12;
-    c.bins_per_rc2 = 64.0 / c.rc2;  // RHO_BINS of k_short_pair
+    c.bins_per_rc2 = QEM_RHO_BINS / c.rc2;
     c.Nt2 = (p.N_t + 1) / 2;
     for (int m = 0; m < c.Nt2; m++) {
         // node pair (2m, 2m + 1); an odd N_t ends with a node at t = 0 of weight 0
@@ -1495,6 +1496,108 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
     double *gout = ptr<double>(h->gout);  // [0, 2): short gamma, [2, 4): long gamma
     CU(grow(h->scan_tmp, qem_scan_tmp_bytes(std::max(std::max(N, h->ncell), 1)) + 64));
 
+    std::function<cudaError_t()> long_final;  // the side stream's last step, on s after the short range
+    auto long_range = [&]() -> qem_status {
+        if (do_long) {
+            if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
+            uint64_t nb = 0;
+            if (resampling(h) && h->has_kset) {  // the batch of the latest forward call
+                if (!read_batch_counter(h, &nb)) return fail(h, QEM_ERR_CUDA, "reading the k batch counter");
+                if (nb > 0) {
+                    batch_rows(h, nb - 1, h->P, h->kset);
+                    h->kwt.clear();
+                    h->sum_K = h->sampler_sumK;
+                    h->kset_dirty = true;
+                }
+            }
+            const int Pk = h->has_kset ? h->P : 0;
+            const int LCH = qem_long_chunk();
+            const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;
+            const int ks = qem_long_ksplit(nch, std::max(Pk, 1), h->long_max_ks, QEM_FP64);
+            CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks * nch + nb0 + std::max(Pk, 1) + 8)));
+            LongBuffers b;
+            {
+                const qem_status ls = long_buffers(h, N, Pk, nch, ks, ptr<double>(h->Epart), nbS, nb0, b);
+                if (ls != QEM_OK) return ls;
+            }
+            if ((h->kset_dirty || h->kin_lo != 0 || h->kin_hi != Pk) && Pk > 0) {
+                CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
+                if (!h->kwt.empty())
+                    CU(cudaMemcpyAsync(h->kw.p, h->kwt.data(), sizeof(double) * Pk, cudaMemcpyHostToDevice, s));
+                h->kset_dirty = false;
+                h->kin_lo = 0;
+                h->kin_hi = Pk;
+            }
+            // the long range runs on the side stream beside the short range
+            // (its final pass, which adds into the gradients, after the join);
+            // with equal-z ties it stays on s after the short range
+            const bool side = !(h->p.mode_flags & QEM_EQUAL_Z_TIES);
+            cudaStream_t sl = side ? h->s2 : s;
+            if (side) {
+                CU(cudaEventRecord(h->ev_fork, s));
+                CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
+            }
+            CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
+                                ptr<double>(h->zkey2), sl));
+            CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
+                               h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch, st, sl, 0));
+            const size_t P1 = std::max(Pk, 1);
+            CU(grow(h->zgx, sizeof(double) * N));
+            CU(grow(h->zgy, sizeof(double) * N));
+            CU(grow(h->zgz, sizeof(double) * N));
+            CU(grow(h->w1, sizeof(double) * N));
+            CU(grow(h->w2, sizeof(double) * N));
+            CU(grow(h->ws1, sizeof(double) * (N + 1)));
+            CU(grow(h->ws2, sizeof(double) * (N + 1)));
+            CU(grow(h->atot, sizeof(double) * 8 * P1 * nch));
+            CU(grow(h->aoff, sizeof(double) * 4 * P1 * nch));
+            CU(grow(h->lam, sizeof(double) * 4 * P1));
+            CU(grow(h->ggk, sizeof(double) * 2 * P1));
+            CU(grow(h->Gpart, sizeof(double) * 4 * (size_t)ks * N));
+            LongAdjBuffers a;
+            a.zgx = ptr<double>(h->zgx); a.zgy = ptr<double>(h->zgy); a.zgz = ptr<double>(h->zgz);
+            a.w1 = ptr<double>(h->w1); a.w2 = ptr<double>(h->w2); a.s1 = ptr<double>(h->ws1); a.s2 = ptr<double>(h->ws2);
+            a.atot = ptr<double>(h->atot); a.aoff = ptr<double>(h->aoff); a.lam = ptr<double>(h->lam);
+            a.ggk = ptr<double>(h->ggk); a.Gpart = ptr<double>(h->Gpart); a.gam = gout + 2;
+            if (side) {
+                CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                       h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch, ks, sl, 0));
+                CU(cudaEventRecord(h->ev_join, sl));
+                long_final = [=]() -> cudaError_t {
+                    cudaError_t e = cudaStreamWaitEvent(s, h->ev_join, 0);
+                    if (e != cudaSuccess) return e;
+                    return qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz,
+                                               h->p.gamma_down, h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch,
+                                               ks, s, 1);
+                };
+            } else {
+                // the forward force is the mean over the two tie orders, so the
+                // adjoint is the sum of both orders' adjoints of (gF / 2, gE / 2);
+                // the second order's gamma gradient goes to gout[4 .. 6)
+                CU(grow(h->gFh, sizeof(double) * 3 * N));
+                double *gFh = ptr<double>(h->gFh);
+                if (gF_d) CU(qem_launch_scale(3 * N, 0.5, gF_d, gFh, s));
+                else CU(cudaMemsetAsync(gFh, 0, sizeof(double) * 3 * N, s));
+                CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                       h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
+                CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
+                                    ptr<double>(h->zkey), ptr<double>(h->zkey2), s, true));
+                CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
+                                   h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch,
+                                   st, s, 0));
+                a.gam = gout + 4;
+                CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
+                                       h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
+                ties_adj = true;
+            }
+        }
+        return QEM_OK;
+    };
+    const bool long_first = do_long && !(h->p.mode_flags & QEM_EQUAL_Z_TIES);
+    if (long_first) {
+        const qem_status ls_ = long_range();
+        if (ls_ != QEM_OK) return ls_;
+    }
     if (do_short || do_lj) {
         if (do_short) {
             const bool stale = (h->p.mode_flags & QEM_STALE_NEIGHBORS) != 0;
@@ -1519,82 +1622,11 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
         if (gq_d) CU(cudaMemsetAsync(gq_d, 0, sizeof(double) * N, s));
     }
 
-    if (do_long) {
-        if (!h->has_kset && h->p.rbe_p > 0) sample_kset(h, h->p.rbe_p);
-        uint64_t nb = 0;
-        if (resampling(h) && h->has_kset) {  // the batch of the latest forward call
-            if (!read_batch_counter(h, &nb)) return fail(h, QEM_ERR_CUDA, "reading the k batch counter");
-            if (nb > 0) {
-                batch_rows(h, nb - 1, h->P, h->kset);
-                h->kwt.clear();
-                h->sum_K = h->sampler_sumK;
-                h->kset_dirty = true;
-            }
-        }
-        const int Pk = h->has_kset ? h->P : 0;
-        const int LCH = qem_long_chunk();
-        const int nch = (N + LCH - 1) / LCH, nbS = (N + 255) / 256, nb0 = (N + 255) / 256;
-        const int ks = qem_long_ksplit(nch, std::max(Pk, 1), h->long_max_ks, QEM_FP64);
-        CU(grow(h->Epart, sizeof(double) * ((size_t)nbS + (size_t)ks * nch + nb0 + std::max(Pk, 1) + 8)));
-        LongBuffers b;
-        {
-            const qem_status ls = long_buffers(h, N, Pk, nch, ks, ptr<double>(h->Epart), nbS, nb0, b);
-            if (ls != QEM_OK) return ls;
-        }
-        if ((h->kset_dirty || h->kin_lo != 0 || h->kin_hi != Pk) && Pk > 0) {
-            CU(cudaMemcpyAsync(h->kin.p, h->kset.data(), sizeof(double) * 3 * Pk, cudaMemcpyHostToDevice, s));
-            if (!h->kwt.empty())
-                CU(cudaMemcpyAsync(h->kw.p, h->kwt.data(), sizeof(double) * Pk, cudaMemcpyHostToDevice, s));
-            h->kset_dirty = false;
-            h->kin_lo = 0;
-            h->kin_hi = Pk;
-        }
-        CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
-                            ptr<double>(h->zkey2), s));
-        CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
-                           h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch, st, s, 0));
-        const size_t P1 = std::max(Pk, 1);
-        CU(grow(h->zgx, sizeof(double) * N));
-        CU(grow(h->zgy, sizeof(double) * N));
-        CU(grow(h->zgz, sizeof(double) * N));
-        CU(grow(h->w1, sizeof(double) * N));
-        CU(grow(h->w2, sizeof(double) * N));
-        CU(grow(h->ws1, sizeof(double) * (N + 1)));
-        CU(grow(h->ws2, sizeof(double) * (N + 1)));
-        CU(grow(h->atot, sizeof(double) * 8 * P1 * nch));
-        CU(grow(h->aoff, sizeof(double) * 4 * P1 * nch));
-        CU(grow(h->lam, sizeof(double) * 4 * P1));
-        CU(grow(h->ggk, sizeof(double) * 2 * P1));
-        CU(grow(h->Gpart, sizeof(double) * 4 * (size_t)ks * N));
-        LongAdjBuffers a;
-        a.zgx = ptr<double>(h->zgx); a.zgy = ptr<double>(h->zgy); a.zgz = ptr<double>(h->zgz);
-        a.w1 = ptr<double>(h->w1); a.w2 = ptr<double>(h->w2); a.s1 = ptr<double>(h->ws1); a.s2 = ptr<double>(h->ws2);
-        a.atot = ptr<double>(h->atot); a.aoff = ptr<double>(h->aoff); a.lam = ptr<double>(h->lam);
-        a.ggk = ptr<double>(h->ggk); a.Gpart = ptr<double>(h->Gpart); a.gam = gout + 2;
-        if (!(h->p.mode_flags & QEM_EQUAL_Z_TIES)) {
-            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
-                                   h->p.gamma_up, h->p.eps_0, gF_d, gE, gx_d, gq_d, nch, ks, s));
-        } else {
-            // the forward force is the mean over the two tie orders, so the
-            // adjoint is the sum of both orders' adjoints of (gF / 2, gE / 2);
-            // the second order's gamma gradient goes to gout[4 .. 6)
-            CU(grow(h->gFh, sizeof(double) * 3 * N));
-            double *gFh = ptr<double>(h->gFh);
-            if (gF_d) CU(qem_launch_scale(3 * N, 0.5, gF_d, gFh, s));
-            else CU(cudaMemsetAsync(gFh, 0, sizeof(double) * 3 * N, s));
-            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
-                                   h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
-            CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
-                                ptr<double>(h->zkey), ptr<double>(h->zkey2), s, true));
-            CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
-                               h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch,
-                               st, s, 0));
-            a.gam = gout + 4;
-            CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
-                                   h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
-            ties_adj = true;
-        }
+    if (!long_first) {
+        const qem_status ls_ = long_range();
+        if (ls_ != QEM_OK) return ls_;
     }
+    if (long_final) CU(long_final());
     double hg[6] = {0, 0, 0, 0, 0, 0};
     CU(cudaMemcpyAsync(hg, gout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
     if (mem == QEM_MEM_HOST) {

@@ -55,6 +55,48 @@ struct ShortConsts {
     const double *norm_xw;
 };
 
+// rho^2 bins of the pair grouping (bins_per_rc2 = QEM_RHO_BINS / r_c^2)
+constexpr int QEM_RHO_BINS = 64;
+
+// Counting sort of a block's items into NBINS bins (NBINS a multiple of 32;
+// every thread passes its item's bin, NBINS - 1 for no item): returns the
+// thread whose item this thread takes, so that the items of a bin sit on
+// consecutive threads, bins ascending.  hist (NBINS ints) and sidx (one int
+// per thread) are shared memory.  The order inside a bin depends on the
+// atomics; callers evaluate and write each item under its own index, so
+// their results do not.  Every thread of the block must call it.
+template <int NBINS>
+__device__ __forceinline__ int group_by_bin(int bin, int *hist, int *sidx)
+{
+    static_assert(NBINS % 32 == 0, "bins per lane");
+    if (threadIdx.x < NBINS) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int slot = atomicAdd(&hist[bin], 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the bin counts (NBINS / 32 per lane)
+        constexpr int PER = NBINS / 32;
+        int v[PER], tot = 0;
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            v[j] = tot;
+            tot += hist[threadIdx.x * PER + j];
+        }
+        int x = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, x, d);
+            if ((int)threadIdx.x >= d) x += t;
+        }
+        const int base = x - tot;
+#pragma unroll
+        for (int j = 0; j < PER; j++) hist[threadIdx.x * PER + j] = base + v[j];
+    }
+    __syncthreads();
+    sidx[hist[bin] + slot] = threadIdx.x;
+    __syncthreads();
+    return sidx[threadIdx.x];
+}
+
 // 2-D cell grid of the in-plane binning
 struct CellGeom {
     double Lx, Ly, invLx, invLy;
@@ -472,9 +514,13 @@ struct LongAdjBuffers {
 };
 // after stage 0 of qem_launch_long in FP64: adds the long-range dL/dr, dL/dq
 // into gxyz, gq (particle order)
+// stage 0: everything up to the per-slice partials and the gamma sums (reads
+// only the forward quantities and gF); stage 1: the final pass, which adds
+// into gxyz and gq; -1: both
 cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffers &b, const LongAdjBuffers &a,
                                 double Lx, double Ly, double Lz, double g1, double g2, double eps0, const double *gF,
-                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s);
+                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s,
+                                int stage = -1);
 
 // ---------------------------------------------------------------------------
 // device helpers

@@ -1454,10 +1454,16 @@ cudaError_t qem_launch_reduce_sum(const double *in, int n, double *out, cudaStre
 
 cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffers &b, const LongAdjBuffers &a,
                                 double Lx, double Ly, double Lz, double g1, double g2, double eps0, const double *gF,
-                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s)
+                                double gE, double *gxyz, double *gq, int nch, int ks, cudaStream_t s, int stage)
 {
     if (N <= 0) return cudaSuccess;
     const double h = 0.5 * Lz;
+    if (stage == 1) {
+        const double fs = 1.0 / (2.0 * Lx * Ly * eps0), es = -1.0 / (4.0 * eps0 * Lx * Ly);
+        k_ladj_final<<<nblk(N, 256), 256, 0, s>>>(N, ks, a.Gpart, zperm, b.qd, b.zhd, h, b.qscan, a.zgz, a.w1,
+                                                  a.s1, a.w2, a.s2, fs, es, gE, gxyz, gq);
+        return cudaGetLastError();
+    }
     k_ladj_prep<<<nblk(N, 256), 256, 0, s>>>(N, gF, zperm, b.qd, b.zhd, h, a.zgx, a.zgy, a.zgz, a.w1, a.w2);
     cudaError_t e = qem_scan_f64_excl(a.w1, a.s1, N, b.stmp, b.stmp_bytes, s);
     if (e == cudaSuccess) e = qem_scan_f64_excl(a.w2, a.s2, N, b.stmp, b.stmp_bytes, s);
@@ -1470,9 +1476,10 @@ cudaError_t qem_launch_long_adj(int N, int P, const int *zperm, const LongBuffer
     }
     k_ladj<<<dim3(nch, ks), LT, 0, s>>>(N, P, nch, ks, b.zx, b.zy, b.zhd, b.qd, b.kc, b.kin,
                                         (const KForce<double> *)b.kf, b.off, a.aoff, a.lam, in, a.Gpart);
+    k_ladj_gsum<<<1, 256, 0, s>>>(P, a.ggk, a.gam);
+    if (stage == 0) return cudaGetLastError();
     const double fs = 1.0 / (2.0 * Lx * Ly * eps0), es = -1.0 / (4.0 * eps0 * Lx * Ly);
     k_ladj_final<<<nblk(N, 256), 256, 0, s>>>(N, ks, a.Gpart, zperm, b.qd, b.zhd, h, b.qscan, a.zgz, a.w1, a.s1,
                                               a.w2, a.s2, fs, es, gE, gxyz, gq);
-    k_ladj_gsum<<<1, 256, 0, s>>>(P, a.ggk, a.gam);
     return cudaGetLastError();
 }

@@ -45,7 +45,7 @@ namespace {
 #define QEM_PAIR_BLOCK 256
 #endif
 constexpr int PAIR_BLOCK = QEM_PAIR_BLOCK;  // pairs per block, grouped by rho in shared memory
-constexpr int RHO_BINS = 64;                // rho^2 bins of the grouping (a multiple of 32)
+constexpr int RHO_BINS = QEM_RHO_BINS;      // rho^2 bins of the grouping (a multiple of 32)
 // resident pair blocks per SM requested from the register allocator, and the
 // unroll factor of the FP32 node loop (tuning knobs; measured defaults)
 #ifndef QEM_PAIR_MINB
@@ -286,42 +286,17 @@ __device__ __forceinline__ void short_pair_tile(const ShortConsts &c, int64_t bx
     // a warp cross the Bessel branch point at nearly the same node.  The order
     // inside a bin depends on the atomics, but every thread evaluates and
     // writes its own pair, so the results do not.
+    int bin = RHO_BINS - 1;
     {
-        if (threadIdx.x < RHO_BINS) hist[threadIdx.x] = 0;
-        __syncthreads();
         const int64_t p = bx * PAIR_BLOCK + threadIdx.x;
-        int bin = RHO_BINS - 1;
         if (p >= lo && p < hi) {
             const int2 ij = pairs[p];
             const double4 pi = pos[ij.x], pj = pos[ij.y];
             const double dx = min_image(pi.x - pj.x, c.Lx, c.invLx), dy = min_image(pi.y - pj.y, c.Ly, c.invLy);
             bin = min(RHO_BINS - 1, (int)((dx * dx + dy * dy) * c.bins_per_rc2));
         }
-        const int slot = atomicAdd(&hist[bin], 1);
-        __syncthreads();
-        if (threadIdx.x < 32) {  // exclusive scan of the bin counts (RHO_BINS / 32 per lane)
-            constexpr int PER = RHO_BINS / 32;
-            int v[PER], tot = 0;
-#pragma unroll
-            for (int j = 0; j < PER; j++) {
-                v[j] = tot;
-                tot += hist[threadIdx.x * PER + j];
-            }
-            int x = tot;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, x, d);
-                if ((int)threadIdx.x >= d) x += t;
-            }
-            const int base = x - tot;
-#pragma unroll
-            for (int j = 0; j < PER; j++) hist[threadIdx.x * PER + j] = base + v[j];
-        }
-        __syncthreads();
-        sidx[hist[bin] + slot] = threadIdx.x;
-        __syncthreads();
     }
-    const int64_t p = bx * PAIR_BLOCK + sidx[threadIdx.x];
+    const int64_t p = bx * PAIR_BLOCK + group_by_bin<RHO_BINS>(bin, hist, sidx);
     if (p >= Np) return;
     if (p < lo || p >= hi) {  // another rank's pair
         R[p] = make_double4(0, 0, 0, 0);
