@@ -1736,7 +1736,8 @@ qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys 
         return QEM_ERR_ARG;
     };
     if (h->p.precision != QEM_FP32_FIX) return no("precision is not QEM_FP32_FIX");
-    if (N <= 0 || N > 8192 || !qem_cells_small(N, h->ncell)) return no("more than 8192 particles or cells");
+    if (N <= 0) return no("no particles");
+    if (N > 8192 || !qem_cells_small(N, h->ncell)) return no("more than 8192 particles or cells");
     if (h->geom.ncx >= 3 && h->geom.ncy >= 3 && (int64_t)N >= 2 * (int64_t)h->ncell)
         return no("two or more particles per cell (warp-per-cell pair list)");
     if (h->p.mode_flags & QEM_EQUAL_Z_TIES) return no("equal-z tie mode");
