@@ -317,9 +317,9 @@ qem_status qem_set_shard(qem_handle *h, int32_t rank, int32_t world);
  * exclusive prefix sum of N.  The handles stay owned by the caller.
  *
  * A batch evaluation runs one of two ways (qem_batch_set_mode):
- *   QEM_BATCH_FUSED: 17 or 18 launches for the whole batch, each over all
+ *   QEM_BATCH_FUSED: 16 or 17 launches for the whole batch, each over all
  *     systems -- pack and z order over (system, particle tile) work lists (a
- *     tile pass and one or two merge passes); cells and pair list in eight
+ *     tile pass of 2048-key tiles and, above 2048 particles, one merge pass); cells and pair list in eight
  *     phases over cell, particle and pair tiles (their scans one block per
  *     system); then one launch per phase (pair forces; long-range
  *     preparation, chunk totals, their scan, the k-sliced force pass and the

@@ -9,8 +9,8 @@
 //
 // Two ways to run a batch evaluation:
 //  * fused phases (every system small enough for the one-block kernels, in
-//    FP32+fix): 17 or 18 launches for the whole batch.  Pack and the
-//    rank-sorted z tiles run over (system, particle tile) work lists; then,
+//    FP32+fix): 16 or 17 launches for the whole batch.  Pack and the
+//    sorted 2048-key z tiles run over (system, tile) work lists; then,
 //    on a second stream, the z merge passes and the long-range phases
 //    (preparation one block per system, chunk totals, their scan, the
 //    k-sliced force pass, the final sum), and on the first stream the cells
@@ -129,8 +129,9 @@ struct qem_batch {
     ShortConsts *d_sc = nullptr;
     BatchWork *d_work = nullptr;
     size_t work_cap = 0;
-    // work lists: pairs, particle tiles, totals, scan, force pass, merge passes 0 and 1, cell tiles
-    int nw[8] = {0, 0, 0, 0, 0, 0, 0, 0}, wo[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // work lists: pairs, particle tiles, totals, scan, force pass, merge passes 0 and 1, cell tiles,
+    // z-order tiles
+    int nw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, wo[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int launches = 0;                   // kernels per fused evaluation
     cudaStream_t s_long = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -196,7 +197,8 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
     const int ts = qem_batch_lscan_tile(), tf = qem_batch_lforce_tile();
     if (tp != 256 || tpart != 256)
         return bfail(b, QEM_ERR_ARG, "the list phases take pair and particle tiles of 256");
-    for (int ph = 0; ph < 8; ph++) {
+    const int tz = qem_batch_ztile();
+    for (int ph = 0; ph < 9; ph++) {
         b->wo[ph] = (int)w.size();
         for (int s : order) {
             const BatchSys &d = sys[s];
@@ -216,6 +218,8 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
                 for (int t = 0; t < nblk(d.N, 256); t++) w.push_back({s, t, 0, 0});
             if (ph == 7)
                 for (int t = 0; t < nblk(d.ncell, 256); t++) w.push_back({s, t, 0, 0});
+            if (ph == 8)
+                for (int t = 0; t < nblk(d.N, tz); t++) w.push_back({s, t, 0, 0});
         }
         b->nw[ph] = (int)w.size() - b->wo[ph];
     }
@@ -248,7 +252,7 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
 static qem_status enqueue_fused(qem_batch *b, const double *xyz, const double *q, double *F, cudaStream_t s)
 {
     const BatchWork *w = b->d_work;
-    BCU(qem_launch_batch_pack_ztile(b->nw[1], w + b->wo[1], b->d_sys, xyz, q, s));
+    BCU(qem_launch_batch_pack_ztile(b->nw[8], w + b->wo[8], b->d_sys, xyz, q, s));
     BCU(cudaEventRecord(b->ev_fork, s));
     BCU(cudaStreamWaitEvent(b->s_long, b->ev_fork, 0));
     for (int pass = 0; pass < 2; pass++)

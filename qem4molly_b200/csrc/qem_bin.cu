@@ -776,13 +776,14 @@ __global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__re
 // z order.  Keys are (z, index): a total order, so the result is the stable
 // ascending order of z (sortperm, QEM_long.jl:39-40); non-finite z was zeroed
 // by k_pack.  REV orders equal z by descending index instead (the second
-// order of the equal-z tie mode).  Tiles of ZTILE keys are sorted by rank
-// (each thread counts the keys of its tile that precede its own), then runs
+// order of the equal-z tie mode).  Tiles of ZTILE keys are sorted in shared
+// memory by a bitonic network (ZTILE / 2 threads, two keys each), then runs
 // are merged ZWAY at a time: every key counts, by binary search, the keys
-// that precede it in the other runs of its group.  With distinct keys both
-// steps place every key exactly.
+// that precede it in the other runs of its group.  With distinct keys every
+// step places every key exactly.
 // ---------------------------------------------------------------------------
-constexpr int ZTILE = 256;
+constexpr int ZTILE = 2048;
+constexpr int ZT_THREADS = ZTILE / 2;
 constexpr int ZWAY = 8;
 
 template <bool REV>
@@ -791,29 +792,56 @@ __device__ __forceinline__ bool zless(double za, int ia, double zb, int ib)
     return (za < zb) || (za == zb && (REV ? ia > ib : ia < ib));
 }
 
+// ascending (zless) order of the ZTILE keys (sk, si) of the calling block of
+// ZT_THREADS threads: the bitonic network, thread t comparing the pair
+// (i, i + stride) with i = 2 t - t mod stride at every stage
 template <bool REV>
-__global__ void __launch_bounds__(ZTILE) k_ztile(int N, const double4 *__restrict__ pos, double *__restrict__ key,
-                                                 int *__restrict__ idx)
+__device__ __forceinline__ void bitonic_tile(double *sk, int *si)
+{
+    const int t = threadIdx.x;
+#pragma unroll 1
+    for (int size = 2; size <= ZTILE; size <<= 1) {
+#pragma unroll 1
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+            const double zi = sk[i], zj = sk[j];
+            const int ii = si[i], ij = si[j];
+            const bool up = (i & size) == 0;
+            if (up ? zless<REV>(zj, ij, zi, ii) : zless<REV>(zi, ii, zj, ij)) {
+                sk[i] = zj;
+                sk[j] = zi;
+                si[i] = ij;
+                si[j] = ii;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// tile blockIdx.x of the keys (pos[i].z, i), sorted into key / idx at the
+// tile's place (padding, +inf, ranks last and is not written)
+template <bool REV>
+__global__ void __launch_bounds__(ZT_THREADS) k_ztile(int N, const double4 *__restrict__ pos,
+                                                      double *__restrict__ key, int *__restrict__ idx)
 {
     __shared__ double sk[ZTILE];
     __shared__ int si[ZTILE];
     const int base = blockIdx.x * ZTILE;
-    const int i = base + threadIdx.x;
-    double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
-    int me = 0x7fffffff;
-    if (i < N) {
-        z = pos[i].z;
-        me = i;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int l = threadIdx.x + h * ZT_THREADS, i = base + l;
+        sk[l] = i < N ? pos[i].z : __longlong_as_double(0x7ff0000000000000LL);
+        si[l] = i < N ? i : 0x7fffffff;
     }
-    sk[threadIdx.x] = z;
-    si[threadIdx.x] = me;
-    __syncthreads();
-    int rank = 0;
-#pragma unroll 8
-    for (int j = 0; j < ZTILE; j++) rank += zless<REV>(sk[j], si[j], z, me) ? 1 : 0;
-    if (i < N) {
-        key[base + rank] = z;
-        idx[base + rank] = me;
+    bitonic_tile<REV>(sk, si);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int l = threadIdx.x + h * ZT_THREADS;
+        if (base + l < N) {
+            key[base + l] = sk[l];
+            idx[base + l] = si[l];
+        }
     }
 }
 
@@ -863,35 +891,35 @@ __host__ __device__ inline int zsort_pass_count(int N)
 // ---------------------------------------------------------------------------
 // fused batches: the small-system binning and z order over all systems
 // ---------------------------------------------------------------------------
-// (system, particle tile of ZTILE): pack the tile's particles and rank-sort
-// its (z, index) keys -- k_pack and k_ztile -- into the buffer the system's
-// first pass reads (so that its last pass ends in zkey, zperm)
-__global__ void __launch_bounds__(ZTILE) k_batch_pack_ztile(const BatchWork *__restrict__ wl,
-                                                            const BatchSys *__restrict__ ds,
-                                                            const double *__restrict__ xyz,
-                                                            const double *__restrict__ q)
+// (system, particle tile of ZTILE): pack the tile's particles and sort its
+// (z, index) keys -- k_pack and k_ztile -- into the buffer the system's
+// first merge pass reads (so that its last pass ends in zkey, zperm)
+__global__ void __launch_bounds__(ZT_THREADS) k_batch_pack_ztile(const BatchWork *__restrict__ wl,
+                                                                 const BatchSys *__restrict__ ds,
+                                                                 const double *__restrict__ xyz,
+                                                                 const double *__restrict__ q)
 {
     __shared__ double sk[ZTILE];
     __shared__ int si[ZTILE];
     const BatchWork t = wl[blockIdx.x];
     const BatchSys &d = ds[t.s];
-    const int N = d.N, base = t.x * ZTILE, i = base + threadIdx.x;
-    double z = __longlong_as_double(0x7ff0000000000000LL);  // +inf: padding ranks last
-    int me = 0x7fffffff;
-    if (i < N) {
-        z = pack_one(i, xyz + 3 * d.off, q + d.off, d.pos, d.cell, d.geom, d.status);
-        me = i;
+    const int N = d.N, base = t.x * ZTILE;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int l = threadIdx.x + h * ZT_THREADS, i = base + l;
+        sk[l] = i < N ? pack_one(i, xyz + 3 * d.off, q + d.off, d.pos, d.cell, d.geom, d.status)
+                      : __longlong_as_double(0x7ff0000000000000LL);
+        si[l] = i < N ? i : 0x7fffffff;
     }
-    sk[threadIdx.x] = z;
-    si[threadIdx.x] = me;
-    __syncthreads();
-    int rank = 0;
-#pragma unroll 8
-    for (int j = 0; j < ZTILE; j++) rank += zless<false>(sk[j], si[j], z, me) ? 1 : 0;
-    if (i < N) {
-        const bool odd = zsort_pass_count(N) & 1;
-        (odd ? d.zkey2 : d.zkey)[base + rank] = z;
-        (odd ? d.ztmp : d.zperm)[base + rank] = me;
+    bitonic_tile<false>(sk, si);
+    const bool odd = zsort_pass_count(N) & 1;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int l = threadIdx.x + h * ZT_THREADS;
+        if (base + l < N) {
+            (odd ? d.zkey2 : d.zkey)[base + l] = sk[l];
+            (odd ? d.ztmp : d.zperm)[base + l] = si[l];
+        }
     }
 }
 
@@ -1075,13 +1103,13 @@ cudaError_t qem_launch_pack(int N, const double *xyz, const double *q, double4 *
 bool qem_cells_small(int N, int ncell) { return N <= CELLS_SMALL && ncell <= CELLS_SMALL; }
 
 int qem_batch_zsort_passes(int N) { return zsort_pass_count(N); }
+int qem_batch_ztile(void) { return ZTILE; }
 
 cudaError_t qem_launch_batch_pack_ztile(int nw, const BatchWork *w, const BatchSys *d, const double *xyz,
                                         const double *q, cudaStream_t s)
 {
     if (nw <= 0) return cudaSuccess;
-    static_assert(ZTILE == 256, "particle tiles of the fused phases are ZTILE long");
-    k_batch_pack_ztile<<<nw, ZTILE, 0, s>>>(w, d, xyz, q);
+    k_batch_pack_ztile<<<nw, ZT_THREADS, 0, s>>>(w, d, xyz, q);
     return cudaGetLastError();
 }
 
@@ -1177,8 +1205,8 @@ cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, d
     const int passes = zsort_passes(N);
     double *ka = (passes & 1) ? zkey_tmp : zkey, *kb = (passes & 1) ? zkey : zkey_tmp;
     int *ia = (passes & 1) ? ztmp : zperm, *ib = (passes & 1) ? zperm : ztmp;
-    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), ZTILE, 0, s>>>(N, pos, ka, ia);
-    else k_ztile<false><<<nblk(N, ZTILE), ZTILE, 0, s>>>(N, pos, ka, ia);
+    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia);
+    else k_ztile<false><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia);
     for (int64_t w = ZTILE; w < N; w *= ZWAY) {
         if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);
         else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);

@@ -460,6 +460,7 @@ int qem_batch_lforce_tile(void);
 // z order: pack + rank-sorted tiles over particle tiles, then merge passes
 // 0, 1, .. over the particle tiles of the systems with that many passes
 int qem_batch_zsort_passes(int N);
+int qem_batch_ztile(void);  // particles per tile of the z-order tile pass
 cudaError_t qem_launch_batch_pack_ztile(int nw, const BatchWork *w, const BatchSys *d, const double *xyz,
                                         const double *q, cudaStream_t s);
 cudaError_t qem_launch_batch_zmerge(int nw, const BatchWork *w, const BatchSys *d, int pass, cudaStream_t s);
