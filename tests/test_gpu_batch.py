@@ -247,3 +247,64 @@ def test_fused_batch_autotune_keeps_results():
     assert (b.mode()["mode"] == "fused") == (w == 0)
     F = _batch_F(b, x, q)
     assert W.rel_err(F, ref)[0] <= (1e-12 if b.mode()["chunk"] == 512 else 1e-6)
+
+
+def test_fused_batch_with_walls():
+    """Substrate_LJ walls are fused into the gather of the fused phases as in
+    the systems' own calls (config-1-like slabs with walls at z = 0 and L_z)."""
+    import torch
+
+    from qem4molly_b200.api import Engine, Substrate_LJ
+
+    rng = np.random.default_rng(23)
+    cfgs, engines = [], []
+    for i, n in enumerate((150, 400, 900)):
+        Lxy = float(np.sqrt(n / 0.01))
+        xyz = np.stack([rng.random(n) * Lxy, rng.random(n) * Lxy, 0.5 + 9.0 * rng.random(n)], 1)
+        q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+        walls = [Substrate_LJ(cutoff=1.0, sigma=1.0, eps=1.0, sub_pos=0.0, direction=1),
+                 Substrate_LJ(cutoff=1.0, sigma=1.0, eps=1.0, sub_pos=10.0, direction=-1)]
+        e = Engine(L_box=(Lxy, Lxy, 10.0), alpha=0.1, r_cutoff=10.0, gamma_1=0.6, gamma_2=-0.8, rbe_p=60,
+                   walls=walls, precision=L.QEM_FP32_FIX)
+        e.sample_kset(70 + i, 60)
+        cfgs.append(dict(xyz=xyz, q=q, N=n))
+        engines.append(e)
+    x = torch.tensor(np.concatenate([c["xyz"] for c in cfgs]), device="cuda")
+    q = torch.tensor(np.concatenate([c["q"] for c in cfgs]), device="cuda")
+    b = Batch(engines, [c["N"] for c in cfgs])
+    Fb = _batch_F(b, x, q)
+    assert b.mode()["mode"] == "fused"
+    for c, e, o in zip(cfgs, engines, b.off):
+        own = e.forces(c["xyz"], c["q"])
+        assert _close(Fb[o:o + c["N"]], own)
+        no_walls = e.forces(c["xyz"], c["q"], terms=L.QEM_TERM_SHORT | L.QEM_TERM_LONG)
+        assert np.abs(own - no_walls).max() > 0  # the walls act on these slabs
+
+
+def test_fused_batch_recovers_from_a_pair_list_overflow():
+    """Positions whose pair list outgrows the capacity sized on the first call:
+    check() reports QEM_ERR_NB_OVERFLOW, and the next batch call sizes every
+    system again and equals the systems' own calls."""
+    import torch
+
+    cfgs, engines, N, x, q = _setup(6, "fp32", seed=41)
+    b = Batch(engines, N)
+    F = torch.empty_like(x)
+    b.forces(x, q, F)
+    assert b.mode()["mode"] == "fused"
+    # squeeze system 2 into a quarter of its box in x and y: ~16x the pairs
+    o, n = b.off[2], N[2]
+    xs = x.clone()
+    xs[o:o + n, :2] *= 0.25
+    b.forces(xs, q, F)
+    with pytest.raises(L.QemError) as err:
+        b.check()
+    assert err.value.status == 4  # QEM_ERR_NB_OVERFLOW
+    b.forces(xs, q, F)  # sizes every system again (synchronously)
+    b.forces(xs, q, F)
+    b.check()
+    assert b.mode()["mode"] == "fused"
+    Fb = F.cpu().numpy()
+    xh = xs.cpu().numpy()
+    for c, e, oo, nn in zip(cfgs, engines, b.off, N):
+        assert _close(Fb[oo:oo + nn], e.forces(xh[oo:oo + nn], c["q"]))
