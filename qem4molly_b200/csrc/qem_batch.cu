@@ -122,6 +122,8 @@ struct qem_batch {
     int flch = 0;                       // chunk length of the fused k-space passes (0: qem_long_chunk())
     bool ftab_ok = false;               // device tables built for the current buffers and terms
     std::string fwhy;                   // why the batch cannot run fused (empty: it can)
+    bool fneed_warm = false;            // a system needs a synchronous call before the tables can be built
+    bool rewarming = false;             // inside the one re-sizing pass of a batch call
     std::vector<uint64_t> fstate;       // per-handle state the tables were built for
     uint32_t fterms = 0;
     int do_lj = 0;
@@ -170,6 +172,7 @@ static bool use_fused(const qem_batch *b)
 static qem_status build_fused(qem_batch *b, uint32_t terms)
 {
     b->ftab_ok = false;
+    b->fneed_warm = false;
     b->fwhy.clear();
     if ((terms & (QEM_TERM_SHORT | QEM_TERM_LONG)) != (QEM_TERM_SHORT | QEM_TERM_LONG)) {
         b->fwhy = "terms without both the short and the long range";
@@ -180,6 +183,11 @@ static qem_status build_fused(qem_batch *b, uint32_t terms)
     for (int i = 0; i < b->B; i++) {
         const char *why = nullptr;
         const qem_status st = qem_handle_batch_sys(b->h[i], b->N[i], b->fks, b->flch, &sys[i], &sc[i], &why);
+        if (st == QEM_ERR_NO_KSET && why) {  // the caller changed the handle: size every system again
+            b->fneed_warm = true;
+            b->fwhy = "system " + std::to_string(i) + ": " + why;
+            return QEM_OK;
+        }
         if (st == QEM_ERR_ARG && why) {
             b->fwhy = "system " + std::to_string(i) + ": " + why;
             return QEM_OK;
@@ -403,6 +411,18 @@ void qem_batch_destroy(qem_batch *b)
 
 const char *qem_batch_last_error(const qem_batch *b) { return b ? b->err.c_str() : "NULL batch"; }
 
+// A handle changed since the last sizing pass (its k-set or size): wait for
+// any work already enqueued, then size every system again, once.
+static qem_status rewarm(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms, void *stream)
+{
+    BCU(cudaDeviceSynchronize());
+    b->warm = false;
+    b->rewarming = true;
+    const qem_status st = qem_batch_forces(b, xyz, q, F, terms, stream);
+    b->rewarming = false;
+    return st;
+}
+
 qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, double *F, uint32_t terms,
                             void *stream)
 {
@@ -426,9 +446,12 @@ qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, do
         drop_md_graph(b);
         const qem_status st = build_fused(b, terms);
         if (st != QEM_OK) return st;
+        if (b->fneed_warm && !b->rewarming) return rewarm(b, xyz, q, F, terms, stream);
     }
     if (b->mode_req == QEM_BATCH_FUSED && !b->fwhy.empty()) return bfail(b, QEM_ERR_ARG, "fused batch: " + b->fwhy);
-    return enqueue_forces(b, xyz, q, F, terms, s);
+    const qem_status st = enqueue_forces(b, xyz, q, F, terms, s);
+    if (st == QEM_ERR_NO_KSET && !b->rewarming) return rewarm(b, xyz, q, F, terms, stream);
+    return st;
 }
 
 qem_status qem_batch_check(qem_batch *b, void *stream)

@@ -1735,6 +1735,10 @@ qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys 
         if (why) *why = m;
         return QEM_ERR_ARG;
     };
+    auto not_ready = [&](const char *m) {  // a synchronous call of the system sizes it
+        if (why) *why = m;
+        return QEM_ERR_NO_KSET;
+    };
     if (h->p.precision != QEM_FP32_FIX) return no("precision is not QEM_FP32_FIX");
     if (N <= 0) return no("no particles");
     if (N > 8192 || !qem_cells_small(N, h->ncell)) return no("more than 8192 particles or cells");
@@ -1744,14 +1748,14 @@ qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys 
     if (h->shard_world != 1) return no("sharded handle");
     if (h->sc.norm) return no("gamma_up * gamma_down > 1");
     if (!h->pairs_valid || h->pairs_N != N || !h->status.p || !h->Epart.p)
-        return no("no synchronous call of this size yet");
+        return not_ready("no synchronous call of this size yet");
     const bool draw = resampling(h);
     if ((h->p.rbe_p > 0 && !h->has_kset) || h->kset_dirty || (draw && (!h->ktab_on_dev || h->kctr_reset)))
-        return no("the k-set is not on the device (synchronous call first)");
+        return not_ready("the k-set is not on the device (synchronous call first)");
     const int P = h->has_kset ? h->P : 0;
     const double kmax = draw ? h->kmax_lattice : h->kmax;
     if (P > 0 && !draw && !h->kset_lattice) return no("k-set rows off the lattice");
-    if (P > 0 && (h->kin_lo != 0 || h->kin_hi != P)) return no("the k rows on the device are not the whole set");
+    if (P > 0 && (h->kin_lo != 0 || h->kin_hi != P)) return not_ready("the k rows on the device are not the whole set");
     const int LCH = qem_long_chunk();
     if (lch <= 0) lch = LCH;
     if (lch < 32 || LCH % lch != 0) return no("chunk length must divide qem_long_chunk() and be >= 32");

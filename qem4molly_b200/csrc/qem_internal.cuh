@@ -485,7 +485,8 @@ cudaError_t qem_launch_batch_gather(int nw, const BatchWork *w, const BatchSys *
 // chunk length of the k-space passes.
 // Returns QEM_ERR_ARG with the reason in *why when the system does not take
 // the small-system kernels in FP32+fix (the batch then keeps per-system
-// pipelines).
+// pipelines), QEM_ERR_NO_KSET when it needs a synchronous call first (its
+// size, buffers or k-set changed since the last one).
 qem_status qem_handle_batch_sys(qem_handle *h, int N, int ks, int lch, BatchSys *d, ShortConsts *sc,
                                 const char **why);
 // changes whenever a buffer of any handle is reallocated or this handle's

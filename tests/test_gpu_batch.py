@@ -308,3 +308,25 @@ def test_fused_batch_recovers_from_a_pair_list_overflow():
     xh = xs.cpu().numpy()
     for c, e, oo, nn in zip(cfgs, engines, b.off, N):
         assert _close(Fb[oo:oo + nn], e.forces(xh[oo:oo + nn], c["q"]))
+
+
+@pytest.mark.parametrize("mode", [L.QEM_BATCH_FUSED, L.QEM_BATCH_POOL])
+def test_batch_follows_a_changed_kset(mode):
+    """A new k-set fed to one handle between batch calls is sized and uploaded
+    by the next batch call (fused phases and stream pool alike), whose forces
+    then equal the systems' own calls with their current k-sets."""
+    import torch
+
+    cfgs, engines, N, x, q = _setup(5, "fp32", seed=43)
+    b = Batch(engines, N)
+    b.set_mode(mode)
+    _batch_F(b, x, q)
+    other = W.engine_for(cfgs[3], "fp32", seed=999)
+    k3, sK = other.get_kset()
+    engines[3].set_kset(k3, sK)
+    Fb = _batch_F(b, x, q)
+    assert b.mode()["mode"] == ("fused" if mode == L.QEM_BATCH_FUSED else "pool")
+    assert np.array_equal(engines[3].get_kset()[0], k3)
+    for c, e, o, n in zip(cfgs, engines, b.off, N):
+        own = e.forces(c["xyz"], c["q"])
+        assert _close(Fb[o:o + n], own) if mode == L.QEM_BATCH_FUSED else np.array_equal(Fb[o:o + n], own)
