@@ -27,7 +27,7 @@ namespace {
 constexpr int ADJ_BLOCK = 128;
 // resident blocks per SM the pair adjoint is compiled for (register cap)
 #ifndef QEM_ADJ_MINB
-#define QEM_ADJ_MINB 4
+#define QEM_ADJ_MINB 8
 #endif
 
 template <class T>
