@@ -440,7 +440,11 @@ qem_status qem_batch_forces(qem_batch *b, const double *xyz, const double *q, do
         b->warm = true;
         b->warm_terms = terms;
         drop_md_graph(b);
-        return b->mode_req == QEM_BATCH_POOL ? QEM_OK : build_fused(b, terms);
+        if (b->mode_req == QEM_BATCH_POOL) return QEM_OK;
+        const qem_status st = build_fused(b, terms);
+        if (st == QEM_OK && b->mode_req == QEM_BATCH_FUSED && !b->fwhy.empty())
+            return bfail(b, QEM_ERR_ARG, "fused batch: " + b->fwhy);
+        return st;
     }
     if (use_fused(b) && !fused_current(b, terms)) {
         drop_md_graph(b);

@@ -330,3 +330,29 @@ def test_batch_follows_a_changed_kset(mode):
     for c, e, o, n in zip(cfgs, engines, b.off, N):
         own = e.forces(c["xyz"], c["q"])
         assert _close(Fb[o:o + n], own) if mode == L.QEM_BATCH_FUSED else np.array_equal(Fb[o:o + n], own)
+
+
+def test_batch_mode_arguments():
+    """Bad modes, k-slice counts, orders and chunk lengths are refused; a
+    fused request for a batch that cannot run fused (FP64 systems) fails at
+    the next batch call and names the reason; the pool request runs."""
+    import torch
+
+    cfgs, engines, N, x, q = _setup(3, "fp64", seed=44)
+    b = Batch(engines, N)
+    for args in ((7, 0, 0, 0), (L.QEM_BATCH_FUSED, -1, 0, 0), (L.QEM_BATCH_FUSED, 0, 2, 0),
+                 (L.QEM_BATCH_FUSED, 0, 0, 100), (L.QEM_BATCH_FUSED, 0, 0, 16)):
+        with pytest.raises(L.QemError) as err:
+            b.set_mode(*args)
+        assert err.value.status == 1, args
+    b.set_mode(L.QEM_BATCH_FUSED)
+    F = torch.empty_like(x)
+    with pytest.raises(L.QemError) as err:
+        b.forces(x, q, F)
+        b.forces(x, q, F)
+    assert "QEM_FP32_FIX" in str(err.value)
+    b.set_mode(L.QEM_BATCH_POOL)
+    Fb = _batch_F(b, x, q)
+    assert b.mode()["mode"] == "pool" and b.mode()["launches"] == -1
+    for c, e, o, n in zip(cfgs, engines, b.off, N):
+        assert np.array_equal(Fb[o:o + n], e.forces(c["xyz"], c["q"]))
