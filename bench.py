@@ -184,7 +184,7 @@ class RefEvaluator:
 
 
 # ----------------------------------------------------------------------------- adjoint
-def backward_timing(lib, local, dev, K=10):
+def backward_timing(lib, local, dev, K=40):
     """qem_backward (FP64) on the differentiation workload -- config 3: N = 2e4,
     |q| ~ U[0.5, 1.5] re-neutralised, Lx = Ly = 450, Lz = 10, gamma_up = 0.8,
     gamma_down = -0.6, P = 500, loss = E + sum_i w_i . F_i with w ~ N(0, 1) --

@@ -780,7 +780,8 @@ __global__ void __launch_bounds__(1024) k_pairs_small(int N, const double4 *__re
 // memory by a bitonic network (ZTILE / 2 threads, two keys each), then runs
 // are merged ZWAY at a time: every key counts, by binary search, the keys
 // that precede it in the other runs of its group.  With distinct keys every
-// step places every key exactly.
+// step places every key exactly.  Above one tile, a single system is ordered
+// by z buckets first (k_zb_*, below), and these passes are its fallback.
 // ---------------------------------------------------------------------------
 constexpr int ZTILE = 2048;
 constexpr int ZT_THREADS = ZTILE / 2;
@@ -823,10 +824,12 @@ __device__ __forceinline__ void bitonic_tile(double *sk, int *si)
 // tile's place (padding, +inf, ranks last and is not written)
 template <bool REV>
 __global__ void __launch_bounds__(ZT_THREADS) k_ztile(int N, const double4 *__restrict__ pos,
-                                                      double *__restrict__ key, int *__restrict__ idx)
+                                                      double *__restrict__ key, int *__restrict__ idx,
+                                                      const int *__restrict__ gate)
 {
     __shared__ double sk[ZTILE];
     __shared__ int si[ZTILE];
+    if (gate && *gate == 0) return;  // the bucket passes placed every key (whole block)
     const int base = blockIdx.x * ZTILE;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -874,10 +877,92 @@ __device__ __forceinline__ void zmerge_one(int p, int N, int width, const double
 
 template <bool REV>
 __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const int *__restrict__ idx,
-                         double *__restrict__ key_out, int *__restrict__ idx_out)
+                         double *__restrict__ key_out, int *__restrict__ idx_out, const int *__restrict__ gate)
 {
+    if (gate && *gate == 0) return;  // the bucket passes placed every key
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < N) zmerge_one<REV>(p, N, width, key, idx, key_out, idx_out);
+}
+
+// ---------------------------------------------------------------------------
+// z order by buckets (one system above one tile).  The slab's z range
+// [0, L_z] is cut into nb equal buckets (about ZB_AVG keys each for a
+// uniform slab; keys outside the range go to the end buckets, and the bucket
+// index never decreases with z).  A count pass (atomics), a one-block scan of
+// the counts, a scatter pass (atomics: arbitrary order inside a bucket) and a
+// rank pass: a warp per bucket ranks each of its keys against every key of
+// the bucket by zless, which restores the exact stable order, since the keys
+// (z, index) are distinct.  Four short launches instead of a tile pass and
+// merge passes, so the long-range chain behind the z order starts while the
+// cell binning still leaves most SMs idle.  A bucket holding more than ZB_CAP
+// keys (z far from uniform, many equal z) sets a flag instead, and the tile
+// and merge passes, launched behind the rank pass, sort everything when that
+// flag is set (and return at once when it is not).
+// ---------------------------------------------------------------------------
+constexpr int ZB_AVG = 32;     // keys per bucket of a uniform slab
+constexpr int ZB_CAP = 256;    // largest bucket the rank pass sorts
+constexpr int ZB_WARPS = 8;    // buckets per block of the rank pass
+
+struct ZBGeom {
+    double z0, scale;  // bucket = floor((z - z0) scale), clamped to [0, nb)
+    int nb;
+};
+
+__device__ __forceinline__ int zbucket(double z, const ZBGeom &g)
+{
+    const double f = (z - g.z0) * g.scale;
+    return f <= 0.0 ? 0 : (f >= (double)(g.nb - 1) ? g.nb - 1 : (int)f);
+}
+
+// count the keys of each bucket; slot[i]: particle i's place inside its bucket
+__global__ void k_zb_count(int N, const double4 *__restrict__ pos, ZBGeom g, int *cnt, int *__restrict__ slot,
+                           int *__restrict__ flag)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *flag = 0;  // read by later launches only
+    if (i < N) slot[i] = atomicAdd(&cnt[zbucket(pos[i].z, g)], 1);
+}
+
+__global__ void k_zb_scatter(int N, const double4 *__restrict__ pos, ZBGeom g, const int *__restrict__ start,
+                             const int *__restrict__ slot, double *__restrict__ key, int *__restrict__ idx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double z = pos[i].z;
+    const int p = start[zbucket(z, g)] + slot[i];
+    key[p] = z;
+    idx[p] = i;
+}
+
+// warp w of the block ranks bucket blockIdx.x ZB_WARPS + w and writes zperm
+template <bool REV>
+__global__ void __launch_bounds__(32 * ZB_WARPS) k_zb_rank(int nb, const int *__restrict__ start,
+                                                           const double *__restrict__ key,
+                                                           const int *__restrict__ idx, int *__restrict__ zperm,
+                                                           int *__restrict__ flag)
+{
+    __shared__ double sk[ZB_WARPS][ZB_CAP];
+    __shared__ int si[ZB_WARPS][ZB_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int b = blockIdx.x * ZB_WARPS + w;
+    if (b >= nb) return;  // whole warp; no block barrier below
+    const int s0 = start[b], n = start[b + 1] - s0;
+    if (n > ZB_CAP) {
+        if (lane == 0) *flag = 1;
+        return;
+    }
+    for (int e = lane; e < n; e += 32) {
+        sk[w][e] = key[s0 + e];
+        si[w][e] = idx[s0 + e];
+    }
+    __syncwarp();
+    for (int e = lane; e < n; e += 32) {
+        const double ze = sk[w][e];
+        const int ie = si[w][e];
+        int r = 0;
+        for (int j = 0; j < n; j++) r += zless<REV>(sk[w][j], si[w][j], ze, ie) ? 1 : 0;
+        zperm[s0 + r] = ie;
+    }
 }
 
 // number of ZWAY-way merge passes after the tile pass for N keys
@@ -1069,7 +1154,13 @@ int qem_scan_f64_launches(int n) { return n <= SCAN_SMALL_MAX ? 1 : 3; }
 
 static int zsort_passes(int N) { return zsort_pass_count(N); }
 
-int qem_zsort_launches(int N) { return N <= 0 ? 0 : 1 + zsort_passes(N); }
+// the bucket passes take over above one tile when the caller gives a flag word and the slab height
+static bool zb_path(int N, const int *zflag, double Lz) { return zflag && Lz > 0.0 && N > ZTILE; }
+static int zb_buckets(int N) { return (int)std::min<int64_t>(((int64_t)N + ZB_AVG - 1) / ZB_AVG, SCAN_SMALL_MAX_INT); }
+int qem_zsort_launches(int N, bool buckets)
+{
+    return N <= 0 ? 0 : 1 + zsort_passes(N) + (buckets && N > ZTILE ? 4 : 0);
+}
 
 cudaError_t qem_scan_i32_to_i64(const int *in, int64_t *out, int n, void *tmp, size_t tmp_bytes, cudaStream_t s)
 {
@@ -1198,18 +1289,35 @@ cudaError_t qem_launch_pair_list(int N, int ncell, const double4 *pos_c, const i
 }
 
 cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
-                             cudaStream_t s, bool rev_ties)
+                             cudaStream_t s, bool rev_ties, int *zflag, double Lz)
 {
     if (N <= 0) return cudaSuccess;
+    const int *gate = nullptr;
+    if (zb_path(N, zflag, Lz)) {
+        // bucket passes; workspace in zkey_tmp (as ints): counts [0, nb),
+        // starts [nb, 2 nb + 1), slots [2 nb + 1, 2 nb + 1 + N) -- within its
+        // 2 N ints since nb <= N / 32 + 1 and N > ZTILE
+        const int nb = zb_buckets(N);
+        int *cnt = reinterpret_cast<int *>(zkey_tmp), *start = cnt + nb, *slot = start + nb + 1;
+        const ZBGeom g{0.0, nb / Lz, nb};
+        cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(int) * nb, s);
+        if (e != cudaSuccess) return e;
+        k_zb_count<<<nblk(N, 256), 256, 0, s>>>(N, pos, g, cnt, slot, zflag);
+        k_scan_small<int, int, SCAN_SMALL_PT_INT><<<1, SCAN_BLOCK, 0, s>>>(cnt, start, nb);
+        k_zb_scatter<<<nblk(N, 256), 256, 0, s>>>(N, pos, g, start, slot, zkey, ztmp);
+        if (rev_ties) k_zb_rank<true><<<nblk(nb, ZB_WARPS), 32 * ZB_WARPS, 0, s>>>(nb, start, zkey, ztmp, zperm, zflag);
+        else k_zb_rank<false><<<nblk(nb, ZB_WARPS), 32 * ZB_WARPS, 0, s>>>(nb, start, zkey, ztmp, zperm, zflag);
+        gate = zflag;  // the tile and merge passes below run only for a bucket over ZB_CAP
+    }
     // ping-pong so that the last pass writes (zkey, zperm)
     const int passes = zsort_passes(N);
     double *ka = (passes & 1) ? zkey_tmp : zkey, *kb = (passes & 1) ? zkey : zkey_tmp;
     int *ia = (passes & 1) ? ztmp : zperm, *ib = (passes & 1) ? zperm : ztmp;
-    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia);
-    else k_ztile<false><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia);
+    if (rev_ties) k_ztile<true><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia, gate);
+    else k_ztile<false><<<nblk(N, ZTILE), ZT_THREADS, 0, s>>>(N, pos, ka, ia, gate);
     for (int64_t w = ZTILE; w < N; w *= ZWAY) {
-        if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);
-        else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib);
+        if (rev_ties) k_zmerge<true><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib, gate);
+        else k_zmerge<false><<<nblk(N, 256), 256, 0, s>>>(N, (int)w, ka, ia, kb, ib, gate);
         double *tk = ka; ka = kb; kb = tk;
         int *ti = ia; ia = ib; ib = ti;
     }

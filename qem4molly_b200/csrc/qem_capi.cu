@@ -462,7 +462,7 @@ static qem_status long_buffers(qem_handle *h, int N, int Pk, int nch, int ks, do
     CU(grow(h->kin, sizeof(double) * 3 * std::max(Pk, 1)));
     CU(grow(h->kw, sizeof(double) * std::max(Pk, 1)));
     CU(grow(h->zperm, sizeof(int) * N));
-    CU(grow(h->ztmp, sizeof(int) * N));
+    CU(grow(h->ztmp, sizeof(int) * (N + 1)));  // + the z-bucket flag word at ztmp[N]
     CU(grow(h->zkey, sizeof(double) * N));
     CU(grow(h->zkey2, sizeof(double) * N));
     CU(grow(h->zx, sizeof(double) * N));
@@ -711,7 +711,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         double *FL = concurrent ? ptr<double>(h->Flong) : F_d;
         CU(cudaMemsetAsync(FL, 0, sizeof(double) * 3 * N, sl));
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
-                            ptr<double>(h->zkey2), sl));
+                            ptr<double>(h->zkey2), sl, false, ptr<int>(h->ztmp) + N, h->p.Lz));
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 0));
         mk_lprep = h->prof.mark(sl);
@@ -719,7 +719,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
                            h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, sl, 1));
         // z sort, zgather + q scan + k = 0 term, per-k constants + totals + scan, force pass + final
         auto long_launches = [&](bool energy_pass) {
-            return qem_zsort_launches(N) +
+            return qem_zsort_launches(N, true) +
                    (!energy_pass && N <= 8192 ? 1 + (Pk > 0 ? 2 : 0) : 2 + qem_scan_f64_launches(N) + (Pk > 0 ? 3 : 0)) +
                    2;
         };
@@ -732,7 +732,8 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
             // below nor above each other.  The energy does not depend on the
             // order of ties and comes from the first pass.
             CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
-                                ptr<double>(h->zkey), ptr<double>(h->zkey2), sl, true));
+                                ptr<double>(h->zkey), ptr<double>(h->zkey2), sl, true, ptr<int>(h->ztmp) + N,
+                                h->p.Lz));
             b.draw_ctr = nullptr;  // the second pass reuses the rows the first one drew
             for (int stage = 0; stage < 2; stage++)
                 CU(qem_launch_long(prec, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
@@ -1538,7 +1539,7 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
                 CU(cudaStreamWaitEvent(sl, h->ev_fork, 0));
             }
             CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
-                                ptr<double>(h->zkey2), sl));
+                                ptr<double>(h->zkey2), sl, false, ptr<int>(h->ztmp) + N, h->p.Lz));
             CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
                                h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch, st, sl, 0));
             const size_t P1 = std::max(Pk, 1);
@@ -1581,7 +1582,8 @@ static qem_status backward_once(qem_handle *h, int N, const double *xyz, const d
                 CU(qem_launch_long_adj(N, Pk, ptr<int>(h->zperm), b, a, h->p.Lx, h->p.Ly, h->p.Lz, h->p.gamma_down,
                                        h->p.gamma_up, h->p.eps_0, gFh, 0.5 * gE, gx_d, gq_d, nch, ks, s));
                 CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp),
-                                    ptr<double>(h->zkey), ptr<double>(h->zkey2), s, true));
+                                    ptr<double>(h->zkey), ptr<double>(h->zkey2), s, true, ptr<int>(h->ztmp) + N,
+                                    h->p.Lz));
                 CU(qem_launch_long(QEM_FP64, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
                                    h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, h->sum_K, nullptr, nch,
                                    st, s, 0));

@@ -325,7 +325,8 @@ int qem_scan_launches(int n);
 int qem_scan_f64_launches(int n);
 // whether the cell build of N particles in ncell cells runs as one one-block kernel
 bool qem_cells_small(int N, int ncell);
-int qem_zsort_launches(int N);
+// kernels of one z order of N particles (buckets: the bucket passes of qem_launch_zsort in use)
+int qem_zsort_launches(int N, bool buckets = false);
 
 // np: device pointer to the pair count; cap: capacity of pairs / R / Upair
 cudaError_t qem_launch_short_pairs(int precision, bool energy, const int64_t *np, int64_t cap, const int2 *pairs,
@@ -337,9 +338,13 @@ cudaError_t qem_launch_short_gather(int precision, bool energy, bool do_short, b
                                     const ShortConsts &c, double *F3, double *Epart, unsigned *status,
                                     cudaStream_t s, const double *Fadd = nullptr);
 
-// stable z order (equal z by ascending index; by descending index with rev_ties)
+// stable z order (equal z by ascending index; by descending index with rev_ties).
+// Scratch: ztmp N ints, zkey and zkey_tmp N doubles each.  With a device flag
+// word zflag (not inside that scratch) and the slab height Lz > 0, more than
+// one tile of particles is ordered by z buckets (four short passes), with the
+// tile and merge passes as the fallback for a bucket that is too full.
 cudaError_t qem_launch_zsort(int N, const double4 *pos, int *zperm, int *ztmp, double *zkey, double *zkey_tmp,
-                             cudaStream_t s, bool rev_ties = false);
+                             cudaStream_t s, bool rev_ties = false, int *zflag = nullptr, double Lz = 0.0);
 // y = a x (y may be x)
 cudaError_t qem_launch_scale(int n, double a, const double *x, double *y, cudaStream_t s);
 struct LongBuffers {

@@ -78,12 +78,20 @@ def test_cell_index_matches_definition():
     assert np.array_equal(np.diff(start), np.bincount(cell, minlength=ncx * ncy))
 
 
-@pytest.mark.parametrize("N,ties", [(1, False), (1000, False), (5000, True), (70_000, True)])
-def test_z_order_is_sortperm(N, ties):
-    """QEM_long.jl:39-40 sortperm: stable ascending, ties in index order."""
+@pytest.mark.parametrize("N,kind", [(1, "uniform"), (1000, "uniform"), (5000, "ties"), (70_000, "ties"),
+                                    (100_000, "uniform"), (30_000, "outside")])
+def test_z_order_is_sortperm(N, kind):
+    """QEM_long.jl:39-40 sortperm: stable ascending, ties in index order.  Up
+    to 2048 particles one tile pass; above, the z-bucket passes (uniform z,
+    ties of about 135 particles per z value, particles outside [0, L_z]),
+    or the tile and merge passes behind them when a bucket overflows (ties of
+    about 1900 particles per z value at N = 7e4)."""
     xyz, _ = slab(N, (300.0, 300.0, 10.0), 13)
-    if ties:
+    if kind == "ties":
         xyz[:, 2] = np.round(xyz[:, 2] * 4) / 4
+    if kind == "outside":
+        xyz[:50, 2] = -3.0
+        xyz[50:100, 2] = 14.0
     e = Engine(L_box=(300.0, 300.0, 10.0), alpha=0.1, r_cutoff=10.0, rbe_p=0)
     assert np.array_equal(e.z_order(xyz), np.argsort(xyz[:, 2], kind="stable"))
     assert np.array_equal(e.z_order(xyz), O.sortperm_z(xyz))

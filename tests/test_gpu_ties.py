@@ -54,9 +54,13 @@ def _tied_slab(N=2000, levels=20, seed=3):
     return cfg
 
 
+@pytest.mark.parametrize("N,levels", [(2000, 20), (6000, 60), (6000, 12)])
 @pytest.mark.parametrize("prec,ftol", [("fp64", 1e-9), ("fp32", 1e-5)])
-def test_ties_vs_oracle_and_energy(prec, ftol):
-    cfg = _tied_slab()
+def test_ties_vs_oracle_and_energy(prec, ftol, N, levels):
+    """N = 2000: one z tile; N = 6000: z buckets with about 100 tied particles
+    per z value (both tie orders on the bucket path), or with 500 per value
+    (a bucket overflows: tile and merge passes)."""
+    cfg = _tied_slab(N=N, levels=levels)
     e = W.engine_for(cfg, prec, mode_flags=L.QEM_EQUAL_Z_TIES)
     k3, sK = e.get_kset()
     F, E = e.forces(cfg["xyz"], cfg["q"], terms=L.QEM_TERM_LONG, energy=True)
