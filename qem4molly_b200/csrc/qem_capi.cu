@@ -161,7 +161,8 @@ struct qem_handle {
     // adjoint pass
     DevBuf gF, gxyz, gq, RA, gam, gout, zgx, zgy, zgz, w1, w2, ws1, ws2, atot, aoff, lam, ggk, Gpart, gFh, normxw;
     cudaStream_t s2 = nullptr;  // side stream of the long range
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t s3 = nullptr;  // per-k constants (and the batch draw) beside the z order
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_kfork = nullptr, ev_kdone = nullptr;
     unsigned *h_status = nullptr;
     double *h_E = nullptr;
     int64_t *h_np = nullptr;
@@ -710,6 +711,16 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
         }
         double *FL = concurrent ? ptr<double>(h->Flong) : F_d;
         CU(cudaMemsetAsync(FL, 0, sizeof(double) * 3 * N, sl));
+        if (concurrent && Pk > 0 && !qem_long_prep_is_small(N, want_E)) {
+            // the per-k constants (with a per-call batch, its draw) on a third
+            // stream while the z order runs; the chunk totals wait for them
+            CU(cudaEventRecord(h->ev_kfork, sl));
+            CU(cudaStreamWaitEvent(h->s3, h->ev_kfork, 0));
+            CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
+                               h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch, st, h->s3, 2));
+            CU(cudaEventRecord(h->ev_kdone, h->s3));
+            b.kconst_done = h->ev_kdone;
+        }
         CU(qem_launch_zsort(N, ptr<double4>(h->pos), ptr<int>(h->zperm), ptr<int>(h->ztmp), ptr<double>(h->zkey),
                             ptr<double>(h->zkey2), sl, false, ptr<int>(h->ztmp) + N, h->p.Lz));
         CU(qem_launch_long(prec, want_E, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx, h->p.Ly,
@@ -735,6 +746,7 @@ static qem_status run_once(qem_handle *h, int N, const double *xyz, const double
                                 ptr<double>(h->zkey), ptr<double>(h->zkey2), sl, true, ptr<int>(h->ztmp) + N,
                                 h->p.Lz));
             b.draw_ctr = nullptr;  // the second pass reuses the rows the first one drew
+            b.kconst_done = nullptr;
             for (int stage = 0; stage < 2; stage++)
                 CU(qem_launch_long(prec, false, N, Pk, ptr<double4>(h->pos), ptr<int>(h->zperm), b, h->p.Lx,
                                    h->p.Ly, h->p.Lz, h->p.gamma_down, h->p.gamma_up, h->p.eps_0, sumK_eff, FL, nch,
@@ -1068,9 +1080,11 @@ qem_status qem_create(const qem_params *p, qem_handle **out)
     if (cudaMallocHost(&h->h_status, sizeof(unsigned)) != cudaSuccess ||
         cudaMallocHost(&h->h_E, sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&h->h_np, sizeof(int64_t)) != cudaSuccess ||
-        create_side_stream(&h->s2) != cudaSuccess ||
+        create_side_stream(&h->s2) != cudaSuccess || create_side_stream(&h->s3) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_kfork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_kdone, cudaEventDisableTiming) != cudaSuccess) {
         qem_destroy(h);
         return QEM_ERR_CUDA;
     }
@@ -1109,8 +1123,14 @@ void qem_destroy(qem_handle *h)
         cudaStreamSynchronize(h->s2);
         cudaStreamDestroy(h->s2);
     }
+    if (h->s3) {
+        cudaStreamSynchronize(h->s3);
+        cudaStreamDestroy(h->s3);
+    }
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_kfork) cudaEventDestroy(h->ev_kfork);
+    if (h->ev_kdone) cudaEventDestroy(h->ev_kdone);
     if (h->h_status) cudaFreeHost(h->h_status);
     if (h->h_E) cudaFreeHost(h->h_E);
     if (h->h_np) cudaFreeHost(h->h_np);

@@ -377,6 +377,9 @@ struct LongBuffers {
     // of this call), and the last kernel of the pass advances *draw_ctr
     unsigned long long *draw_ctr = nullptr;
     KSampler sampler{};
+    // set: the per-k constants were launched on another stream (stage 2) and
+    // recorded in this event, which stage 0 waits for before the chunk totals
+    cudaEvent_t kconst_done = nullptr;
 };
 // zlim of the FP32 k-space path for a k-set whose largest |k| is kmax:
 // e^{+-k (z - Lz/2)} <= e^{60}, so that sums over many particles stay finite
@@ -387,7 +390,10 @@ inline double qem_fp32_zlim(double kmax) { return kmax > 0 ? 60.0 / kmax : 0.0; 
 int qem_long_ksplit(int nch, int P, int max_ks, int precision);
 constexpr int QEM_LONG_MAX_KS = 64;
 // stage 0: z-ordered gather, k = 0 term, per-k constants, chunk totals and
-// their scan; stage 1: the k-sliced force pass, added into F3.
+// their scan; stage 1: the k-sliced force pass, added into F3; stage 2: the
+// per-k constants alone (for a stream beside the z order; not for the
+// one-block preparation, qem_long_prep_is_small).
+bool qem_long_prep_is_small(int N, bool energy);
 cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const double4 *pos, const int *zperm,
                             const LongBuffers &b, double Lx, double Ly, double Lz, double g1, double g2, double eps0,
                             double sum_K, double *F3, int nch, unsigned *status, cudaStream_t s, int stage);

@@ -1321,7 +1321,18 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
     if (N <= 0) return cudaSuccess;
     const double zlim = precision == QEM_FP64 ? 0.0 : b.zlim;
     uint4 *zP = precision == QEM_FP64 ? nullptr : b.zP;
-    if (stage == 0 && !energy && N <= LONG_PREP_SMALL) {
+    auto kconst = [&]() {
+        const double wk = (sum_K / P) / (Lx * Ly * eps0);
+        const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
+        k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
+                                              2.0 * eps0 * Lx * Ly, b.sampler, b.draw_ctr, Lx / (2.0 * QEM_PI),
+                                              Ly / (2.0 * QEM_PI));
+    };
+    if (stage == 2) {
+        if (P > 0) kconst();
+        return cudaGetLastError();
+    }
+    if (stage == 0 && qem_long_prep_is_small(N, energy)) {
         const double h = 0.5 * Lz;
         const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
         const double wk = P > 0 ? (sum_K / P) / (Lx * Ly * eps0) : 0.0;
@@ -1349,23 +1360,35 @@ cudaError_t qem_launch_long(int precision, bool energy, int N, int P, const doub
         const double h = 0.5 * Lz;
         k_zgather<<<nblk(N, 256), 256, 0, s>>>(N, pos, zperm, h, b.zx, b.zy, b.zhd, b.qd, zlim, status, zP,
                                                1.0 / Lx, 1.0 / Ly);
-        cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
-        if (e != cudaSuccess) return e;
-        const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
-        const double escale = b.skip_k0 ? 0.0 : -1.0 / (4.0 * eps0 * Lx * Ly);
-        k_k0<<<nblk(N, 256), 256, 0, s>>>(N, b.qd, b.zhd, h, b.qscan, fscale, escale, b.k0, b.Epart + b.ks * nch,
-                                          energy ? 1 : 0);
+        // the k = 0 term (charge scan in z order) is read only by the final
+        // pass: it follows the chunk totals, which then start sooner
+        auto k0_term = [&]() -> cudaError_t {
+            cudaError_t e = qem_scan_f64_excl(b.qd, b.qscan, N, b.stmp, b.stmp_bytes, s);
+            if (e != cudaSuccess) return e;
+            const double fscale = b.skip_k0 ? 0.0 : 1.0 / (2.0 * Lx * Ly * eps0);
+            const double escale = b.skip_k0 ? 0.0 : -1.0 / (4.0 * eps0 * Lx * Ly);
+            k_k0<<<nblk(N, 256), 256, 0, s>>>(N, b.qd, b.zhd, h, b.qscan, fscale, escale, b.k0,
+                                              b.Epart + b.ks * nch, energy ? 1 : 0);
+            return cudaSuccess;
+        };
+        if (P <= 0) {
+            const cudaError_t e = k0_term();
+            if (e != cudaSuccess) return e;
+        }
         if (P > 0) {
-            const double wk = (sum_K / P) / (Lx * Ly * eps0);
-            const double esc = -(sum_K / P) / (2.0 * eps0 * Lx * Ly);
-            k_kconst<<<nblk(P, 128), 128, 0, s>>>(P, b.kin, b.kc, Lz, g1 * g2, wk, esc, b.kwt, Lx * Ly * eps0,
-                                                  2.0 * eps0 * Lx * Ly, b.sampler, b.draw_ctr, Lx / (2.0 * QEM_PI),
-                                                  Ly / (2.0 * QEM_PI));
+            if (b.kconst_done) {
+                const cudaError_t e = cudaStreamWaitEvent(s, b.kconst_done, 0);
+                if (e != cudaSuccess) return e;
+            } else {
+                kconst();
+            }
             dim3 gt(nch, nblk(P, KPB));
             if (precision == QEM_FP64)
                 k_ltot<double><<<gt, LT, 0, s>>>(N, P, nch, b.zx, b.zy, b.zhd, b.qd, b.kc, b.tot);
             else
                 k_ltot_lk<<<dim3(nch, nblk(P, KTT)), KTT, 0, s>>>(N, P, nch, b.zP, b.kc, b.tot);
+            const cudaError_t e = k0_term();
+            if (e != cudaSuccess) return e;
             if (precision == QEM_FP64)
                 k_lscan<double><<<nblk(P, 4), 128, 0, s>>>(P, nch, b.tot, b.off, b.Utot, b.kc, g1, g2, b.Eks,
                                                            (KForce<double> *)b.kf);
@@ -1402,6 +1425,8 @@ __global__ void k_scale_vec(int n, double a, const double *x, double *y)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] = a * x[i];
 }
+
+bool qem_long_prep_is_small(int N, bool energy) { return !energy && N <= LONG_PREP_SMALL; }
 
 int qem_batch_particle_tile(void) { return BATCH_PTILE; }
 int qem_batch_ltot_tile(void) { return KTT; }
