@@ -187,3 +187,36 @@ def test_forces_substrate_lj(cfg):
         assert np.allclose(F, Fo, rtol=1e-13, atol=1e-14 * max(np.abs(Fo).max(), 1e-300))
     with pytest.raises(TypeError):
         api.potential_energy(api.Substrate_LJ(), sys_)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_resampling_with_the_constants_on_their_own_stream(precision):
+    """Above 8192 particles (and whenever the energy is asked for) the per-k
+    constants, and with per-call batches the draw of the batch, run on a
+    stream of their own beside the z order, and the chunk totals wait for
+    them.  On a 2e4-particle slab, call n must still use batch n of the seed,
+    through the recorded graph and through an ordinary call with the energy,
+    and give the forces (and energy) of a handle fed batch n explicitly."""
+    import torch
+
+    cfg = W.config2(N=20_000, seed=11)
+    e = W.engine_for(cfg, precision, mode_flags=L.QEM_RESAMPLE_KSET, seed=31)
+    ref = W.engine_for(cfg, precision)
+    x = torch.tensor(cfg["xyz"], dtype=torch.float64, device="cuda")
+    q = torch.tensor(cfg["q"], dtype=torch.float64, device="cuda")
+    F = torch.empty_like(x)
+    for n in range(5):
+        e.forces_device(x, q, F)
+        torch.cuda.synchronize()
+        rows, sK = draw_rows(e.params, 31, n, cfg["P"])
+        np.testing.assert_array_equal(e.get_kset()[0], rows)
+        ref.set_kset(rows, sK)
+        assert W.rel_err(F.cpu().numpy(), ref.forces(cfg["xyz"], cfg["q"]))[0] <= 1e-13, n
+    Fe, E = e.forces(cfg["xyz"], cfg["q"], energy=True)
+    rows, sK = draw_rows(e.params, 31, 5, cfg["P"])
+    np.testing.assert_array_equal(e.get_kset()[0], rows)
+    ref.set_kset(rows, sK)
+    Fr, Er = ref.forces(cfg["xyz"], cfg["q"], energy=True)
+    assert W.rel_err(Fe, Fr)[0] <= 1e-13 and abs(E - Er) <= 1e-13 * abs(Er)
+    e.close()
+    ref.close()
