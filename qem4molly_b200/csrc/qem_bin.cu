@@ -902,6 +902,11 @@ __global__ void k_zmerge(int N, int width, const double *__restrict__ key, const
 constexpr int ZB_AVG = 32;     // keys per bucket of a uniform slab
 constexpr int ZB_CAP = 256;    // largest bucket the rank pass sorts
 constexpr int ZB_WARPS = 8;    // buckets per block of the rank pass
+// the workspace (counts nb, starts nb + 1, places N ints) fits the 2 N ints of
+// zkey_tmp from the smallest system on the bucket path (N = ZTILE + 1) up,
+// since nb <= N / ZB_AVG + 1 grows more slowly than N
+static_assert(2 * ((ZTILE + ZB_AVG) / ZB_AVG) + 1 <= ZTILE + 1, "z-bucket workspace exceeds its scratch");
+static_assert(ZB_CAP % 32 == 0 && ZB_CAP >= 2 * ZB_AVG, "rank-pass bucket capacity");
 
 struct ZBGeom {
     double z0, scale;  // bucket = floor((z - z0) scale), clamped to [0, nb)
